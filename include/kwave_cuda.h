@@ -1,0 +1,271 @@
+/*
+ * kwave_cuda.h — C ABI of the B200 (sm_100a) k-space pseudospectral fluid solver.
+ *
+ * This is the drop-in boundary for k-wave-swift's
+ *   kspaceFirstOrder(grid:medium:source:sensor:options:) -> SimulationOutput
+ * (Sources/KWave/Solver/KSpaceFirstOrder.swift:79-107). A Swift `.systemLibrary` target
+ * (modelled on Sources/CHDF5/module.modulemap:1-5) links this library; the Swift adapter
+ * flattens its KWaveGrid / KWaveMedium / KWaveSource / KWaveSensor / SimulationOptions values
+ * into one kw_sim_desc of plain host pointers, calls kw_sim_create + kw_sim_run, and copies the
+ * SimulationOutput fields back with kw_sim_get_output.
+ *
+ * Conventions
+ *   - Every function returns a kw_status (0 = KW_OK) and never aborts the process. The text of the
+ *     last error of a context is kw_last_error_message(ctx). The reference traps on the same
+ *     conditions (precondition/fatalError, KSpaceFirstOrder.swift:105,210-212,358-360,369-370;
+ *     Recording.swift:76-77); here they come back as KW_ERR_INVALID.
+ *   - All arrays are row-major (C order) float32 host arrays, last axis contiguous, exactly the
+ *     memory order of an MLXArray of shape [nx], [nx, ny] or [nx, ny, nz]. The library copies
+ *     every input during kw_sim_create; the caller keeps ownership of its buffers.
+ *   - One kw_context per host thread; a context (and the sims/batches made from it) must not be
+ *     used by two threads at once without external locking.
+ *   - All device work of a context runs on one CUDA stream (its own, or the caller's stream set
+ *     with kw_context_set_stream).
+ */
+#ifndef KWAVE_CUDA_H
+#define KWAVE_CUDA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define KW_ABI_VERSION 1
+
+/* ---- status codes ------------------------------------------------------------------------ */
+typedef enum kw_status {
+    KW_OK = 0,
+    KW_ERR_INVALID = 1,     /* a descriptor or argument the reference would reject (precondition) */
+    KW_ERR_OOM = 2,         /* device or host allocation failed */
+    KW_ERR_CUDA = 3,        /* a CUDA runtime call failed (message has the CUDA error string) */
+    KW_ERR_NONFINITE = 4,   /* the pressure field became NaN/Inf (checked every few steps) */
+    KW_ERR_TIMEOUT = 5,     /* a bounded device-side wait ran out */
+    KW_ERR_UNSUPPORTED = 6, /* a size or mode this build does not implement (e.g. FFT length) */
+    KW_ERR_STATE = 7        /* call out of order (e.g. output requested before kw_sim_run) */
+} kw_status;
+
+/* ---- enums mirroring the reference types ------------------------------------------------ */
+
+/* SourceMode (Sources/KWave/Source/KWaveSource.swift:4-8). */
+typedef enum kw_source_mode {
+    KW_SOURCE_DIRICHLET = 0,
+    KW_SOURCE_ADDITIVE = 1,               /* default in the reference */
+    KW_SOURCE_ADDITIVE_NO_CORRECTION = 2
+} kw_source_mode;
+
+/* AbsorptionMode (Sources/KWave/Medium/KWaveMedium.swift:8-17). */
+typedef enum kw_absorption_mode {
+    KW_ABSORPTION_NONE = 0,               /* .noAbsorption (default) */
+    KW_ABSORPTION_POWER_LAW = 1,          /* .powerLaw */
+    KW_ABSORPTION_NO_DISPERSION = 2,      /* .noDispersion */
+    KW_ABSORPTION_STOKES = 3              /* .stokes */
+} kw_absorption_mode;
+
+/* DirectivityPattern (Sources/KWave/Sensor/KWaveSensor.swift:24-29). */
+typedef enum kw_directivity_pattern {
+    KW_DIRECTIVITY_PRESSURE = 0,
+    KW_DIRECTIVITY_GRADIENT = 1
+} kw_directivity_pattern;
+
+/* RecordField bit values, identical to Sources/KWave/Sensor/KWaveSensor.swift:4-21. */
+#define KW_RECORD_P        (1u << 0)
+#define KW_RECORD_P_MAX    (1u << 1)
+#define KW_RECORD_P_MIN    (1u << 2)
+#define KW_RECORD_P_RMS    (1u << 3)
+#define KW_RECORD_P_FINAL  (1u << 4)
+#define KW_RECORD_UX       (1u << 5)
+#define KW_RECORD_UY       (1u << 6)
+#define KW_RECORD_UZ       (1u << 7)
+#define KW_RECORD_U_MAX    (1u << 8)
+#define KW_RECORD_U_RMS    (1u << 9)
+#define KW_RECORD_U_FINAL  (1u << 10)
+#define KW_RECORD_I_AVG    (1u << 11)
+#define KW_RECORD_I_MAX    (1u << 12)
+
+/* Sensor mask kinds. The reference decides by shape (Recording.swift:50-56): a mask of shape
+ * [dim, nPoints] is Cartesian, anything else is a binary grid mask. The caller passes the
+ * decision explicitly. */
+typedef enum kw_sensor_kind {
+    KW_SENSOR_NONE = 0,
+    KW_SENSOR_BINARY = 1,      /* grid-shaped mask, nonzero = sensor point */
+    KW_SENSOR_CARTESIAN = 2    /* [dim][n_points] coordinates in metres, grid centre at n/2 */
+} kw_sensor_kind;
+
+/* SimulationOutput fields (KSpaceFirstOrder.swift:47-73). */
+typedef enum kw_field {
+    KW_FIELD_P = 0,          /* [nSensor, nt] */
+    KW_FIELD_P_MAX,          /* [nSensor] */
+    KW_FIELD_P_MIN,
+    KW_FIELD_P_RMS,
+    KW_FIELD_P_FINAL,        /* grid shape, always present */
+    KW_FIELD_UX,             /* [nSensor, nt], collocated to the pressure grid */
+    KW_FIELD_UY,
+    KW_FIELD_UZ,
+    KW_FIELD_UX_MAX,         /* [nSensor] */
+    KW_FIELD_UY_MAX,
+    KW_FIELD_UZ_MAX,
+    KW_FIELD_UX_RMS,
+    KW_FIELD_UY_RMS,
+    KW_FIELD_UZ_RMS,
+    KW_FIELD_UX_FINAL,       /* grid shape, staggered grid */
+    KW_FIELD_UY_FINAL,
+    KW_FIELD_UZ_FINAL,
+    KW_FIELD_IX_AVG,         /* [nSensor] */
+    KW_FIELD_IY_AVG,
+    KW_FIELD_IZ_AVG,
+    KW_FIELD_COUNT
+} kw_field;
+
+/* ---- descriptor ---------------------------------------------------------------------------- */
+
+/* A float32 host array that is either a scalar (len == 1) or grid-shaped (len == nx*ny*nz).
+ * data == NULL means "absent" (only meaningful for optional medium properties). */
+typedef struct kw_array {
+    const float* data;
+    size_t len;
+} kw_array;
+
+/* A source signal: one broadcast row (rows == 1) or one row per source point (rows == nSrc,
+ * in ascending flat mask order), each `len` samples long, row-major. data == NULL: absent. */
+typedef struct kw_signal {
+    const float* data;
+    int rows;
+    int len;
+} kw_signal;
+
+/* One simulation: the reference's grid, medium, source, sensor and options flattened.
+ * Source line references are Sources/KWave/... paths of k-wave-swift. */
+typedef struct kw_sim_desc {
+    int abi_version;                 /* must be KW_ABI_VERSION */
+
+    /* KWaveGrid (Grid/KWaveGrid.swift:9-101); unused sizes are 1. */
+    int dim;                         /* 1, 2 or 3 */
+    int nx, ny, nz;
+    double dx, dy, dz;
+    double dt;                       /* from makeTime / setTime (KWaveGrid.swift:112-142) */
+    int nt;
+
+    /* SimulationOptions (Solver/KSpaceFirstOrder.swift:17-40). dtype, device, pmlInside,
+     * plotSim and saveToDisk are not read by the reference solver and have no field here. */
+    int pml_size;                    /* PMLSize.uniform(n); the PML is inside the grid */
+    double pml_alpha;                /* default 2.0 */
+    int smooth_p0;                   /* default 1 */
+    int smooth_c0;                   /* default 0 */
+    int smooth_rho0;                 /* default 0 */
+    double c_ref;                    /* NaN (default): max(c0) after smoothing, as the reference;
+                                        otherwise this value (used by the adjoint, where cRef is
+                                        held fixed) */
+
+    /* KWaveMedium (Medium/KWaveMedium.swift:21-76). */
+    kw_array sound_speed;            /* required */
+    kw_array density;                /* required */
+    kw_array alpha_coeff;            /* dB/(MHz^y cm); data == NULL: lossless */
+    double alpha_power;              /* NaN: absent (the reference then uses 1.5) */
+    int alpha_mode;                  /* kw_absorption_mode */
+    kw_array b_on_a;                 /* data == NULL: linear */
+
+    /* KWaveSource (Source/KWaveSource.swift:11-71). Elastic stress fields are not part of the
+     * fluid solver and are not carried. */
+    const float* p0;                 /* grid-shaped initial pressure or NULL */
+    const float* p_mask;             /* grid-shaped or NULL */
+    kw_signal p;
+    int p_mode;                      /* kw_source_mode */
+    const float* u_mask;             /* grid-shaped or NULL */
+    kw_signal ux, uy, uz;
+    int u_mode;                      /* kw_source_mode */
+
+    /* KWaveSensor (Sensor/KWaveSensor.swift:32-62). */
+    int sensor_kind;                 /* kw_sensor_kind */
+    const float* sensor_mask;        /* grid-shaped (binary) or [dim][sensor_points] (Cartesian) */
+    int sensor_points;               /* Cartesian point count (ignored for binary masks) */
+    unsigned record;                 /* KW_RECORD_* bits; default KW_RECORD_P */
+    const float* directivity_angle;  /* 2D binary sensors only: grid-shaped angles (rad) or NULL */
+    double directivity_size;         /* NaN: 10*max(dx, dy) */
+    int directivity_pattern;         /* kw_directivity_pattern */
+} kw_sim_desc;
+
+/* Fill a descriptor with the reference's defaults (SimulationOptions(), KWaveSource(),
+ * KWaveSensor()): pml 20, alpha 2, smoothP0 on, additive sources, record = KW_RECORD_P. */
+void kw_sim_desc_init(kw_sim_desc* desc);
+
+/* ---- callbacks ----------------------------------------------------------------------------- */
+
+/* progress(t, nt): SimulationOptions.progress, called once per time step after the step has
+ * been issued (KSpaceFirstOrder.swift:30-31,544). */
+typedef void (*kw_progress_fn)(int t, int nt, void* user);
+/* monitor(t, p, count): SimulationOptions.fieldMonitor, called every `monitor_interval` steps
+ * with a host copy of the whole pressure field (KSpaceFirstOrder.swift:32-37,541-543). */
+typedef void (*kw_monitor_fn)(int t, const float* p, size_t count, void* user);
+
+typedef struct kw_callbacks {
+    kw_progress_fn progress;
+    kw_monitor_fn monitor;
+    int monitor_interval;            /* <= 0 is treated as 1, like max(interval, 1) */
+    void* user;
+} kw_callbacks;
+
+/* ---- opaque handles ------------------------------------------------------------------------ */
+typedef struct kw_context kw_context;
+typedef struct kw_sim kw_sim;
+typedef struct kw_batch kw_batch;
+
+/* ---- library / context --------------------------------------------------------------------- */
+const char* kw_version(void);
+int kw_abi_version(void);
+
+/* Create a context on CUDA device `device` with its own non-blocking stream. */
+int kw_context_create(int device, kw_context** out);
+/* Run all further work of this context on `cuda_stream` (a cudaStream_t; NULL restores the
+ * context's own stream). */
+int kw_context_set_stream(kw_context* ctx, void* cuda_stream);
+void kw_context_destroy(kw_context* ctx);
+const char* kw_last_error_message(const kw_context* ctx);
+
+/* ---- one simulation: kspaceFirstOrder ------------------------------------------------------ */
+
+/* Validate the descriptor, run the once-per-run setup (smoothing, operators, PML, source and
+ * sensor plans; KSpaceFirstOrder.swift:351-490) and upload everything to the device. */
+int kw_sim_create(kw_context* ctx, const kw_sim_desc* desc, kw_sim** out);
+/* Run all nt time steps from t = 0 (resets the state first) and finalise the recording
+ * (KSpaceFirstOrder.swift:492-554). `cb` may be NULL. */
+int kw_sim_run(kw_sim* sim, const kw_callbacks* cb);
+/* Reset the state to t = 0 without running. */
+int kw_sim_reset(kw_sim* sim);
+/* Advance `nsteps` further time steps (clamped to nt) without callbacks; asynchronous on the
+ * context's stream. Used for incremental runs and timing. */
+int kw_sim_step(kw_sim* sim, int nsteps);
+/* Block until all issued work has finished; reports KW_ERR_NONFINITE if p became non-finite. */
+int kw_sim_synchronize(kw_sim* sim);
+/* Current time index (number of steps taken since the last reset). */
+int kw_sim_current_step(const kw_sim* sim, int* t);
+int kw_sim_num_sensor_points(const kw_sim* sim, int* count);
+/* Element count of an output field (0 when the field was not requested / does not apply). */
+int kw_sim_output_size(const kw_sim* sim, int field, size_t* count);
+/* Copy an output field into `dst` (count must equal kw_sim_output_size). Series are
+ * [nSensor, nt] row-major over the steps taken so far. */
+int kw_sim_get_output(kw_sim* sim, int field, float* dst, size_t count);
+/* Device pointer of a live state field (KW_FIELD_P_FINAL = p, KW_FIELD_U?_FINAL = u) for
+ * zero-copy consumers such as a field monitor; valid until the next step. */
+int kw_sim_device_field(kw_sim* sim, int field, const float** dptr, size_t* count);
+void kw_sim_destroy(kw_sim* sim);
+
+/* ---- many independent simulations in one launch sequence -----------------------------------
+ * Simulations of the same dimensionality (any sizes, any nt) step together: every kernel of a
+ * step covers the tiles of all simulations that are still running, so small grids fill the GPU.
+ * Each member behaves exactly as kw_sim_run would for its own descriptor. */
+int kw_batch_create(kw_context* ctx, const kw_sim_desc* descs, int count, kw_batch** out);
+int kw_batch_run(kw_batch* batch, const kw_callbacks* cb);
+int kw_batch_reset(kw_batch* batch);
+int kw_batch_step(kw_batch* batch, int nsteps);
+int kw_batch_synchronize(kw_batch* batch);
+int kw_batch_output_size(const kw_batch* batch, int index, int field, size_t* count);
+int kw_batch_get_output(kw_batch* batch, int index, int field, float* dst, size_t count);
+void kw_batch_destroy(kw_batch* batch);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* KWAVE_CUDA_H */
