@@ -1,0 +1,303 @@
+#!/usr/bin/env python
+"""Benchmark of the k-space pseudospectral time step on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload NAME]
+
+Default workload: hetero3d_256 — 256^3 heterogeneous (12 spheres) nonlinear (B/A 6) power-law
+absorbing (alpha 0.75, y 1.5) forward with an additive 1 MPa tone-burst plane source and a full
+xy sensor plane recording p and pMax, FP32 on the device. A "step" is one time step of that
+simulation. The metric is grid-point-steps per second over the whole job.
+
+`value`   device throughput: K time steps timed with CUDA events on the library's stream, inputs
+          resident in HBM (every field is 67 MB, far above the 126 MB L2 in aggregate).
+`e2e`     the same metric through the public C ABI from host buffers: kw_sim_create (host->device
+          copies and setup) + K steps + copy-out of p, pMax and pFinal, host wall clock.
+`roofline` the dominant pass kernel of a step: algorithmic HBM bytes per launch / mean CUDA-event
+          duration per launch, against the measured HBM copy bandwidth of this pool.
+`cpu_baseline` the FP64 oracle (a restatement of the reference's update equations; the Swift/MLX
+          reference cannot run here) on this host's cores for a bounded sample of the workload.
+With --gpus N > 1 (torchrun), every rank runs an independent replica (no collective on the data
+path): "scaling": "weak", value = all ranks' grid-point-steps / max-over-ranks time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "k-wave-swift_b200"))
+
+METRIC = "grid-pt-steps/s"
+UNIT = "grid-pt-steps/s"
+
+
+def measured_peak_gbs() -> tuple[float, str]:
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi sampling of SM clocks and throttle reasons during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_id: str):
+        self.gpu_id = gpu_id
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(prefix="clk", suffix=".csv")
+        os.close(fd)
+        try:
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                                          "-lms", "100", "-i", self.gpu_id], stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *exc):
+        time.sleep(0.25)
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+            self.f.close()
+
+    def summary(self) -> dict:
+        rows = []
+        try:
+            for line in open(self.path):
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+        except Exception:
+            pass
+        finally:
+            try:
+                os.remove(self.path)
+            except Exception:
+                pass
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def workload(name: str, steps_needed: int):
+    from kwave import workloads
+    if name == "hetero3d_256":
+        b = workloads.hetero3d(256)
+    elif name == "hetero3d_128":
+        b = workloads.hetero3d(128)
+    elif name == "ivp2d_128":
+        b = workloads.ivp2d_128()
+    else:
+        raise SystemExit(f"unknown workload {name}")
+    if b.grid.nt < steps_needed:
+        raise SystemExit(f"workload has nt={b.grid.nt} < warmup+steps={steps_needed}")
+    return b
+
+
+def cpu_sample(builder, steps: int, threads: int) -> dict:
+    """Time the FP64 oracle on this host for `steps` time steps (time loop only)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    _, loop_s = oracle.run(builder, nthreads=threads, max_steps=steps)
+    n = builder.grid.totalGridPoints
+    return {"value": n * steps / loop_s, "unit": UNIT, "cores": threads, "kind": "port",
+            "seconds": loop_s, "steps": steps}
+
+
+def run_reference(args) -> None:
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    threads = os.cpu_count() or 1
+    b = workload(args.workload, 1)
+    steps = max(1, min(args.steps, args.ref_steps))
+    r = cpu_sample(b, steps, threads)
+    sample = (f"{args.workload}: first {steps} time step(s) of the workload (additive source active, "
+              f"power law + B/A) in FP64 on {threads} threads; time loop only")
+    line = {
+        "impl": "reference", "metric": METRIC, "value": r["value"], "unit": UNIT, "n_gpus": args.gpus,
+        "steps": steps, "warmup": 0, "ms_per_step": 1e3 * r["seconds"] / steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": args.workload, "grid": list(b.grid.shape), "nt": b.grid.nt,
+                   "l2": "inputs larger than L2"},
+        "cpu_baseline": {"value": r["value"], "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
+        "e2e": {"value": r["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args) -> None:
+    import numpy as np
+    import torch
+
+    from kwave.runtime import Context
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    K, W = args.steps, args.warmup
+    b = workload(args.workload, K + W + 4)
+    npts = b.grid.totalGridPoints
+
+    ctx = Context(local)
+    # a dedicated (non-default) stream shared by the library and the CUDA events below
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    ctx.set_stream(stream.cuda_stream)
+    sim = ctx.create_sim(b)
+    sim.step(W)
+    torch.cuda.synchronize()
+    try:
+        gpu_id = "GPU-" + str(torch.cuda.get_device_properties(local).uuid)
+    except Exception:
+        gpu_id = str(local)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(gpu_id) as clk:
+        e0.record(stream)
+        sim.step(K)
+        e1.record(stream)
+        torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    if dist:
+        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    value = npts * K * world / (ms / 1e3)
+
+    # per-launch device profile of one step (advances a few steps; not part of `value`)
+    prof = sim.profile_step(3)
+    launches_per_step = len(prof)
+    groups: dict[str, dict] = {}
+    for k in prof:
+        kern = k["name"].split(":")[0]
+        g = groups.setdefault(kern, {"ms": 0.0, "bytes": 0.0, "launches": 0})
+        g["ms"] += k["ms"]
+        g["bytes"] += k["bytes"]
+        g["launches"] += 1
+    dom_name, dom = max(groups.items(), key=lambda kv: kv[1]["ms"])
+    peak, peak_kind = measured_peak_gbs()
+    achieved = dom["bytes"] / (dom["ms"] / 1e3) / 1e9 if dom["ms"] > 0 else 0.0
+    step_bytes = sum(k["bytes"] for k in prof)
+    step_ms = sum(k["ms"] for k in prof)
+    traffic = None
+    tfile = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tfile):
+        try:
+            traffic = json.load(open(tfile)).get(args.workload, {}).get(dom_name)
+        except Exception:
+            traffic = None
+    sim.close()
+
+    # end to end through the public ABI from host buffers (setup + K steps + outputs)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    sim2 = ctx.create_sim(b)
+    sim2.step(K)
+    outs = {k: sim2.output(k) for k in ("p", "pMax", "pFinal")}
+    torch.cuda.synchronize()
+    t1 = time.perf_counter()
+    h2d = sum(a.nbytes for a in b.keep)
+    d2h = sum(v.nbytes for v in outs.values() if v is not None)
+    sim2.close()
+    e2e_val = npts * K * world / (t1 - t0)
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        steps = args.cpu_steps
+        r = cpu_sample(b, steps, threads)
+        cpu = {"value": r["value"], "unit": UNIT, "cores": threads, "kind": "port",
+               "sample": f"{args.workload}: first {steps} time step(s) in FP64 (oracle restatement) on "
+                         f"{threads} threads, time loop only ({r['seconds']:.1f} s)"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,
+            "ms_per_step": ms / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32", "data": "synthetic",
+            "config": {"workload": args.workload, "grid": list(b.grid.shape), "nt": b.grid.nt,
+                       "physics": "heterogeneous c0/rho0, power law y=1.5 with dispersion, B/A=6, additive p source"
+                       if args.workload.startswith("hetero") else "homogeneous IVP",
+                       "l2": "inputs larger than L2 (every field >= 67 MB)" if npts >= 2 ** 24 else "small grid",
+                       "parallelism": f"replicas{world}"},
+            "roofline": {"bound": "hbm", "kernel": dom_name, "achieved": achieved, "peak": peak,
+                         "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
+                         "peak_source": peak_kind,
+                         "step_achieved": step_bytes / (ms / K / 1e3) / 1e9,
+                         "step_bytes_per_pt": step_bytes / npts,
+                         "kernel_share": dom["ms"] / step_ms if step_ms else None},
+            "cpu_baseline": cpu,
+            "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": h2d / K, "d2h_bytes_per_step": d2h / K,
+                    "seconds": t1 - t0},
+            "gpu_launches": launches_per_step * K,
+            "clocks": clk.summary(),
+            "kernels": {k: {"ms": round(v["ms"], 4), "GBps": round(v["bytes"] / (v["ms"] / 1e3) / 1e9, 1) if v["ms"] > 0 else 0,
+                            "launches": v["launches"]} for k, v in groups.items()},
+        }
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=300)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="hetero3d_256")
+    ap.add_argument("--cpu-steps", type=int, default=1)
+    ap.add_argument("--ref-steps", type=int, default=2)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

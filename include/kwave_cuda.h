@@ -34,6 +34,12 @@ extern "C" {
 
 #define KW_ABI_VERSION 1
 
+#if defined(__GNUC__)
+#define KW_API __attribute__((visibility("default")))
+#else
+#define KW_API
+#endif
+
 /* ---- status codes ------------------------------------------------------------------------ */
 typedef enum kw_status {
     KW_OK = 0,
@@ -188,7 +194,7 @@ typedef struct kw_sim_desc {
 
 /* Fill a descriptor with the reference's defaults (SimulationOptions(), KWaveSource(),
  * KWaveSensor()): pml 20, alpha 2, smoothP0 on, additive sources, record = KW_RECORD_P. */
-void kw_sim_desc_init(kw_sim_desc* desc);
+KW_API void kw_sim_desc_init(kw_sim_desc* desc);
 
 /* ---- callbacks ----------------------------------------------------------------------------- */
 
@@ -212,57 +218,69 @@ typedef struct kw_sim kw_sim;
 typedef struct kw_batch kw_batch;
 
 /* ---- library / context --------------------------------------------------------------------- */
-const char* kw_version(void);
-int kw_abi_version(void);
+KW_API const char* kw_version(void);
+KW_API int kw_abi_version(void);
 
 /* Create a context on CUDA device `device` with its own non-blocking stream. */
-int kw_context_create(int device, kw_context** out);
+KW_API int kw_context_create(int device, kw_context** out);
 /* Run all further work of this context on `cuda_stream` (a cudaStream_t; NULL restores the
  * context's own stream). */
-int kw_context_set_stream(kw_context* ctx, void* cuda_stream);
-void kw_context_destroy(kw_context* ctx);
-const char* kw_last_error_message(const kw_context* ctx);
+KW_API int kw_context_set_stream(kw_context* ctx, void* cuda_stream);
+KW_API void kw_context_destroy(kw_context* ctx);
+KW_API const char* kw_last_error_message(const kw_context* ctx);
 
 /* ---- one simulation: kspaceFirstOrder ------------------------------------------------------ */
 
 /* Validate the descriptor, run the once-per-run setup (smoothing, operators, PML, source and
  * sensor plans; KSpaceFirstOrder.swift:351-490) and upload everything to the device. */
-int kw_sim_create(kw_context* ctx, const kw_sim_desc* desc, kw_sim** out);
+KW_API int kw_sim_create(kw_context* ctx, const kw_sim_desc* desc, kw_sim** out);
 /* Run all nt time steps from t = 0 (resets the state first) and finalise the recording
  * (KSpaceFirstOrder.swift:492-554). `cb` may be NULL. */
-int kw_sim_run(kw_sim* sim, const kw_callbacks* cb);
+KW_API int kw_sim_run(kw_sim* sim, const kw_callbacks* cb);
 /* Reset the state to t = 0 without running. */
-int kw_sim_reset(kw_sim* sim);
+KW_API int kw_sim_reset(kw_sim* sim);
 /* Advance `nsteps` further time steps (clamped to nt) without callbacks; asynchronous on the
  * context's stream. Used for incremental runs and timing. */
-int kw_sim_step(kw_sim* sim, int nsteps);
+KW_API int kw_sim_step(kw_sim* sim, int nsteps);
 /* Block until all issued work has finished; reports KW_ERR_NONFINITE if p became non-finite. */
-int kw_sim_synchronize(kw_sim* sim);
+KW_API int kw_sim_synchronize(kw_sim* sim);
 /* Current time index (number of steps taken since the last reset). */
-int kw_sim_current_step(const kw_sim* sim, int* t);
-int kw_sim_num_sensor_points(const kw_sim* sim, int* count);
+KW_API int kw_sim_current_step(const kw_sim* sim, int* t);
+KW_API int kw_sim_num_sensor_points(const kw_sim* sim, int* count);
 /* Element count of an output field (0 when the field was not requested / does not apply). */
-int kw_sim_output_size(const kw_sim* sim, int field, size_t* count);
+KW_API int kw_sim_output_size(const kw_sim* sim, int field, size_t* count);
 /* Copy an output field into `dst` (count must equal kw_sim_output_size). Series are
  * [nSensor, nt] row-major over the steps taken so far. */
-int kw_sim_get_output(kw_sim* sim, int field, float* dst, size_t count);
+KW_API int kw_sim_get_output(kw_sim* sim, int field, float* dst, size_t count);
 /* Device pointer of a live state field (KW_FIELD_P_FINAL = p, KW_FIELD_U?_FINAL = u) for
  * zero-copy consumers such as a field monitor; valid until the next step. */
-int kw_sim_device_field(kw_sim* sim, int field, const float** dptr, size_t* count);
-void kw_sim_destroy(kw_sim* sim);
+KW_API int kw_sim_device_field(kw_sim* sim, int field, const float** dptr, size_t* count);
+KW_API void kw_sim_destroy(kw_sim* sim);
+
+/* ---- measurement ---------------------------------------------------------------------------
+ * The reference has no profiler (its bench wall-clocks whole runs, Sources/KWaveBench/main.swift:
+ * 50-57). This entry point runs `reps` further time steps launch by launch with CUDA events around
+ * every launch and reports, for each launch of one step in issue order, its mean device time and
+ * its algorithmic HBM bytes (the compulsory reads + writes of that pass). */
+typedef struct kw_kernel_timing {
+    char name[48];       /* "<pass>:<job>", e.g. "colA_op:vel", "c2r:den" */
+    double ms;           /* mean device time per launch */
+    double bytes;        /* algorithmic HBM bytes per launch */
+} kw_kernel_timing;
+KW_API int kw_sim_profile_step(kw_sim* sim, int reps, kw_kernel_timing* out, int max_entries, int* n_entries);
 
 /* ---- many independent simulations in one launch sequence -----------------------------------
  * Simulations of the same dimensionality (any sizes, any nt) step together: every kernel of a
  * step covers the tiles of all simulations that are still running, so small grids fill the GPU.
  * Each member behaves exactly as kw_sim_run would for its own descriptor. */
-int kw_batch_create(kw_context* ctx, const kw_sim_desc* descs, int count, kw_batch** out);
-int kw_batch_run(kw_batch* batch, const kw_callbacks* cb);
-int kw_batch_reset(kw_batch* batch);
-int kw_batch_step(kw_batch* batch, int nsteps);
-int kw_batch_synchronize(kw_batch* batch);
-int kw_batch_output_size(const kw_batch* batch, int index, int field, size_t* count);
-int kw_batch_get_output(kw_batch* batch, int index, int field, float* dst, size_t count);
-void kw_batch_destroy(kw_batch* batch);
+KW_API int kw_batch_create(kw_context* ctx, const kw_sim_desc* descs, int count, kw_batch** out);
+KW_API int kw_batch_run(kw_batch* batch, const kw_callbacks* cb);
+KW_API int kw_batch_reset(kw_batch* batch);
+KW_API int kw_batch_step(kw_batch* batch, int nsteps);
+KW_API int kw_batch_synchronize(kw_batch* batch);
+KW_API int kw_batch_output_size(const kw_batch* batch, int index, int field, size_t* count);
+KW_API int kw_batch_get_output(kw_batch* batch, int index, int field, float* dst, size_t count);
+KW_API void kw_batch_destroy(kw_batch* batch);
 
 #ifdef __cplusplus
 }

@@ -1,0 +1,147 @@
+// kw_common.h — structures shared by the host engine and the sm_100a kernels.
+//
+// Layout. Every simulation stores its real fields as [A][B][C] float32 with C contiguous:
+//   1D (nx):        A = 1,  B = 1,  C = nx
+//   2D (nx, ny):    A = 1,  B = nx, C = ny
+//   3D (nx,ny,nz):  A = nx, B = ny, C = nz
+// i.e. exactly the row-major order of the reference's MLXArray fields. Spectra are the
+// half-spectrum of a real transform along C: [A][B][Cp] float2 with Ch = C/2 + 1 bins per row,
+// padded to Cp = Ch rounded up to even so that every spectrum row starts 16-byte aligned.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace kw {
+
+constexpr int kMaxStages = 16;
+constexpr int kMaxComp = 3;
+
+// FFT plan of one complex transform length n (a Stockham sequence of radix stages).
+struct FFTPlanDev {
+    int n;
+    int nstages;
+    int radix[kMaxStages];
+    int tw_off[kMaxStages];   // offset of stage s in `tw` (Ns*(R-1) entries, forward sign)
+    const float2* tw;         // exp(-2 pi i r k / (Ns R)), k in [0, Ns), r in [1, R)
+    const float2* gen;        // for generic-prime stages: exp(-2 pi i m / R) at tw_off-independent offsets
+    int gen_off[kMaxStages];
+};
+
+// Per-axis operator vectors in FFT order (length n of that axis). Each is already made
+// Hermitian (real part at the Nyquist bin), so Re(ifft(H * fft(x))) == C2R(H * R2C(x)).
+struct AxisDev {
+    int n;
+    const float2* dpos;     // i k exp(+i k d/2)
+    const float2* dneg;     // i k exp(-i k d/2)
+    const float2* colloc;   // exp(-i k d/2)
+    const float* pml;       // collocated PML profile
+    const float* pml_sg;    // staggered PML profile
+    float inv_d;            // 1 / spacing
+};
+
+// A float32 quantity that is either one value or a full [A][B][C] field.
+struct FieldOrScalar {
+    const float* ptr;       // nullptr: use `s`
+    float s;
+    __host__ __device__ float at(long long i) const { return ptr ? ptr[i] : s; }
+};
+
+// Radial (|k|-only) operator tables over the half-spectrum [A][B][Cp], precomputed in FP64.
+enum RadialTable { RT_NONE = 0, RT_KAPPA, RT_SKAPPA, RT_NU1, RT_NU2, RT_WINDOW, RT_COUNT };
+// Per-axis factor selector.
+enum AxisOp { AO_NONE = 0, AO_DPOS, AO_DNEG, AO_COLLOC };
+
+struct OpSpec {
+    int8_t axis_op;   // AxisOp
+    int8_t axis;      // reference axis (0 = x) the per-axis factor applies to
+    int8_t radial;    // RadialTable
+    int8_t src;       // input component this output reads
+};
+
+// Epilogues of the inverse row pass (C2R), i.e. what happens to the inverse-transformed
+// values d_o of the job's outputs o at each grid point.
+enum Epilogue {
+    EPI_STORE = 0,       // out_field[o][i] = d_o
+    EPI_VEL,             // u_a = pml_sg_a (pml_sg_a u_a - dtor_a d_a)             (velStep)
+    EPI_VEL_INIT,        // u_a = 0.5 dtor_a d_a                                    (t = 0 override)
+    EPI_DEN,             // nl; rho_a = pml_a (pml_a rho_a - dtrho0 d_a nl); rho_sum; div; EoS
+    EPI_ADD_U,           // u_{comp(o)} += d_o                                       (additive u source)
+    EPI_ADD_RHO,         // rho_a += d_0 / d_a; rho_sum; EoS                          (additive p source)
+    EPI_EOS_ABS,         // p = c2 (rho_sum + tau d_0 - eta d_1 + nonlinear)          (power law)
+};
+
+// Source operator of one field variable (SourceOp, KSpaceFirstOrder.swift:129-175).
+struct SourceDev {
+    int nsrc;
+    int rows;              // 1 (broadcast) or nsrc
+    int len;               // samples
+    int mode;              // kw_source_mode
+    const int* idx;        // [nsrc] flat indices, ascending
+    const float* signal;   // [rows][len]
+    const float* scale[kMaxComp];  // per-axis (p) or per-component (u) per-point scale, [nsrc]
+};
+
+struct SensorDev {
+    int kind;              // 0 none, 1 binary, 2 cartesian
+    int npts;
+    int ncorners;
+    const int* idx;        // [npts * ncorners]
+    const float* w;        // [npts * ncorners] (cartesian)
+    int record_p_series;   // keep p[t][q]
+    int record_u_series;   // keep u[a][t][q]
+    int record_p_agg;      // running max/min/sum-of-squares of p
+    int record_u_agg;
+    float* p_series;       // [nt][npts]
+    float* u_series[kMaxComp];
+    float* p_max; float* p_min; float* p_ss; float* p_ssc;   // running aggregates (Kahan)
+    float* u_max[kMaxComp]; float* u_ss[kMaxComp]; float* u_ssc[kMaxComp];
+};
+
+struct SimDev {
+    int dim;
+    int A, B, C, Ch, Cp;
+    long long N;           // real points A*B*C
+    long long Ns;          // spectrum elements A*B*Cp
+    int nt;
+    int axis_of_layout[3]; // reference axis of layout axis A, B, C (-1 when the layout axis is 1)
+    AxisDev ax[3];         // reference axes
+    FFTPlanDev plan_row;   // complex plan of the row transform (length C/2 for even C, C for odd)
+    const float2* row_tw;  // exp(-2 pi i k / C), k in [0, C/2]
+    FFTPlanDev plan_b;     // column plan along B (length B)
+    FFTPlanDev plan_a;     // column plan along A (length A)
+    float inv_n;           // 1 / N
+    const float* radial[RT_COUNT];   // [A][B][Cp] tables (nullptr when unused)
+
+    // state
+    float* p;
+    float* u[kMaxComp];
+    float* rho[kMaxComp];
+    float* rho_sum;
+    float* div_term;       // rho0 * sum_a d_a (power law input) or sum_a d_a * tau * rho0 (Stokes)
+    float* src_buf[kMaxComp];   // sparse scratch fields for additive sources (zero off-mask)
+    float* tmp[kMaxComp];       // real scratch fields (collocated velocity etc.)
+    float2* spec[4];
+
+    // medium
+    FieldOrScalar c2, dtrho0, rho0, tau, eta, bona;
+    FieldOrScalar dtor[kMaxComp];
+    int nonlinear;
+    int absorb;            // 0 none, 1 Stokes, 2 power law without dispersion, 3 with dispersion
+    int eos_pointwise;     // EoS evaluated in the density epilogue / source kernels
+
+    SourceDev psrc, usrc[kMaxComp];
+    int has_p, has_u[kMaxComp];
+    int has_p0;
+    SensorDev sensor;
+    int* nonfinite;        // device flag
+};
+
+// One entry of a launch's block map: which simulation, which component, which tile.
+struct BlockWork {
+    int sim;
+    int comp;
+    int tile;
+};
+
+}  // namespace kw

@@ -1,0 +1,1206 @@
+// kw_engine.cpp — host side of the solver: validation, FP64 precompute, device buffers, the
+// per-step launch sequence (captured as a CUDA graph), recording and output copy-out.
+//
+// Reference: k-wave-swift Sources/KWave/Solver/KSpaceFirstOrder.swift (KSFO) and
+// Sources/KWave/Sensor/Recording.swift (REC). The per-step order of operations follows
+// KSFO:492-546: velocity update, velocity sources, density update, pressure sources, equation of
+// state, t = 0 initial-pressure override, sensor sampling.
+#include "kw_engine.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <limits>
+
+namespace kw {
+
+static constexpr size_t kSmemBudget = 100 * 1024;  // per CTA: two CTAs per SM
+
+static KwError err(int code, const std::string& m) { return KwError{code, m}; }
+
+void Engine::check(cudaError_t e, const char* what) {
+    if (e != cudaSuccess) throw err(KW_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+void* Engine::dalloc(size_t bytes) {
+    if (bytes == 0) bytes = 16;
+    void* p = nullptr;
+    cudaError_t e = cudaMalloc(&p, bytes);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        throw err(KW_ERR_OOM, "device allocation of " + std::to_string(bytes) + " bytes failed: " + cudaGetErrorString(e));
+    }
+    allocs_.push_back(p);
+    check(cudaMemsetAsync(p, 0, bytes, st()), "memset");
+    return p;
+}
+
+Engine::~Engine() {
+    if (graph_exec_) cudaGraphExecDestroy(graph_exec_);
+    if (graph_) cudaGraphDestroy(graph_);
+    cudaStreamSynchronize(ctx_->stream);
+    for (void* p : allocs_) cudaFree(p);
+}
+
+// ------------------------------------------------------------------------------------------
+// FP64 helpers (restated from the reference's host setup)
+// ------------------------------------------------------------------------------------------
+
+// 2 pi fftfreq(n, d)   (Internal/Support.swift:6-19)
+static std::vector<double> wavenumbers(int n, double d) {
+    std::vector<double> r(n);
+    const double val = 1.0 / ((double)n * d);
+    const int cutoff = (n - 1) / 2 + 1;
+    for (int i = 0; i < cutoff; ++i) r[i] = (double)i * val;
+    int j = -(n / 2);
+    for (int i = cutoff; i < n; ++i) r[i] = (double)(j++) * val;
+    for (auto& v : r) v *= 2.0 * M_PI;
+    return r;
+}
+
+// pmlProfile (PML/PML.swift:17-43)
+static std::vector<double> pml_profile(int n, double dx, double dt, double c, int m, double alpha, bool staggered) {
+    const double a = alpha * (c / dx);
+    const double md = (double)m;
+    std::vector<double> pml(n, 1.0);
+    for (int k = 0; k < std::min(m, n); ++k) {
+        const double x = (double)(k + 1);
+        const double pl = staggered ? (md + 0.5 - x) / md : (md + 1.0 - x) / md;
+        const double pr = staggered ? (x + 0.5) / md : x / md;
+        pml[k] = std::exp(-a * dt / 2.0 * std::pow(pl, 4.0));
+        pml[n - m + k] = std::exp(-a * dt / 2.0 * std::pow(pr, 4.0));
+    }
+    return pml;
+}
+
+static double db2neper(double alpha, double y) {  // Material/Conversion.swift:6-8
+    return 100.0 * alpha * std::pow(1e-6 / (2.0 * M_PI), y) / (20.0 * std::log10(M_E));
+}
+
+static std::vector<float> to_f32(const std::vector<double>& v) {
+    std::vector<float> r(v.size());
+    for (size_t i = 0; i < v.size(); ++i) r[i] = (float)v[i];
+    return r;
+}
+
+// ------------------------------------------------------------------------------------------
+// FFT plans: Stockham radix sequence + FP64 twiddles rounded to FP32
+// ------------------------------------------------------------------------------------------
+void Engine::build_plan(FFTPlanDev& pl, int n) {
+    std::memset(&pl, 0, sizeof(pl));
+    pl.n = n;
+    std::vector<int> rad;
+    int m = n;
+    for (int r : {16, 8, 4, 2, 3, 5}) {
+        while (m % r == 0) { rad.push_back(r); m /= r; }
+    }
+    for (int p = 7; m > 1; p += 2) {
+        while (m % p == 0) { rad.push_back(p); m /= p; }
+        if ((long long)p * p > m && m > 1) { rad.push_back(m); m = 1; }
+    }
+    if ((int)rad.size() > kMaxStages) throw err(KW_ERR_UNSUPPORTED, "FFT length " + std::to_string(n) + " has too many factors");
+    for (int r : rad)
+        if (r > 64) throw err(KW_ERR_UNSUPPORTED, "FFT length " + std::to_string(n) + " has a prime factor above 64");
+    pl.nstages = (int)rad.size();
+    std::vector<float2> tw, gen;
+    int Ns = 1;
+    for (int s = 0; s < pl.nstages; ++s) {
+        const int R = rad[s];
+        pl.radix[s] = R;
+        pl.tw_off[s] = (int)tw.size();
+        for (int k = 0; k < Ns; ++k)
+            for (int r = 1; r < R; ++r) {
+                const double a = -2.0 * M_PI * (double)r * (double)k / (double)(Ns * R);
+                tw.push_back(make_float2((float)std::cos(a), (float)std::sin(a)));
+            }
+        pl.gen_off[s] = (int)gen.size();
+        if (R != 2 && R != 3 && R != 4 && R != 5 && R != 8 && R != 16)
+            for (int q = 0; q < R; ++q) {
+                const double a = -2.0 * M_PI * (double)q / (double)R;
+                gen.push_back(make_float2((float)std::cos(a), (float)std::sin(a)));
+            }
+        Ns *= R;
+    }
+    if (tw.empty()) tw.push_back(make_float2(1.f, 0.f));
+    if (gen.empty()) gen.push_back(make_float2(1.f, 0.f));
+    pl.tw = upload(tw);
+    pl.gen = upload(gen);
+}
+
+// ------------------------------------------------------------------------------------------
+// block maps
+// ------------------------------------------------------------------------------------------
+const Engine::Map& Engine::map_rows(int rpc, int ncomp, int sim_only) {
+    auto key = std::make_tuple(0, rpc, ncomp, sim_only, 0);
+    auto it = maps_.find(key);
+    if (it != maps_.end()) return it->second;
+    std::vector<BlockWork> v;
+    for (int s = 0; s < count(); ++s) {
+        if (sim_only >= 0 && s != sim_only) continue;
+        const int rows = sims_[s].A * sims_[s].B;
+        const int tiles = (rows + rpc - 1) / rpc;
+        for (int c = 0; c < ncomp; ++c)
+            for (int tI = 0; tI < tiles; ++tI) v.push_back(BlockWork{s, c, tI});
+    }
+    Map m;
+    m.d = upload(v);
+    m.n = (int)v.size();
+    return maps_[key] = m;
+}
+
+const Engine::Map& Engine::map_cols(int axis, int tw, int ncomp, int sim_only) {
+    auto key = std::make_tuple(1 + axis, tw, ncomp, sim_only, 0);
+    auto it = maps_.find(key);
+    if (it != maps_.end()) return it->second;
+    std::vector<BlockWork> v;
+    for (int s = 0; s < count(); ++s) {
+        if (sim_only >= 0 && s != sim_only) continue;
+        const SimHost& h = sims_[s];
+        const int inner = axis == 0 ? h.B * h.Cp : h.Cp;
+        const int outer = axis == 0 ? 1 : h.A;
+        const int tiles = outer * ((inner + tw - 1) / tw);
+        for (int c = 0; c < ncomp; ++c)
+            for (int tI = 0; tI < tiles; ++tI) v.push_back(BlockWork{s, c, tI});
+    }
+    Map m;
+    m.d = upload(v);
+    m.n = (int)v.size();
+    return maps_[key] = m;
+}
+
+const Engine::Map& Engine::map_elems(int sim_only) {
+    auto key = std::make_tuple(9, 0, 0, sim_only, 0);
+    auto it = maps_.find(key);
+    if (it != maps_.end()) return it->second;
+    std::vector<BlockWork> v;
+    for (int s = 0; s < count(); ++s) {
+        if (sim_only >= 0 && s != sim_only) continue;
+        const long long tiles = (sims_[s].N + 255) / 256;
+        for (long long tI = 0; tI < tiles; ++tI) v.push_back(BlockWork{s, 0, (int)tI});
+    }
+    Map m;
+    m.d = upload(v);
+    m.n = (int)v.size();
+    return maps_[key] = m;
+}
+
+// ------------------------------------------------------------------------------------------
+// spectral job: R2C rows -> column passes (operator fused in the last) -> C2R rows + epilogue
+// ------------------------------------------------------------------------------------------
+void Engine::issue_job(const SpecJob& job, int sim_only) {
+    const int comps_in = job.fanout ? 1 : job.nin;
+    const int M = max_M_;
+    // rows per CTA for the forward row pass
+    int rpc = 16;
+    while (rpc > 1 && (size_t)2 * M * (rpc + 1) * sizeof(float2) > kSmemBudget) rpc /= 2;
+    long long total_rows = 0;
+    for (int s = 0; s < count(); ++s)
+        if (sim_only < 0 || s == sim_only) total_rows += (long long)sims_[s].A * sims_[s].B;
+    while (rpc > 1 && total_rows * comps_in / rpc < 2 * 148) rpc /= 2;
+
+    RowR2CJob rj{};
+    rj.in_field = job.in_field;
+    rj.spec_out = job.spec_in;
+    rj.apply_op = dim_ == 1 ? 1 : 0;
+    for (int c = 0; c < kMaxComp; ++c) rj.op[c] = job.op[c];
+    rj.rows_per_cta = rpc;
+    rj.gate = job.gate;
+    // algorithmic bytes per launch (compulsory HBM reads + writes of the open simulations)
+    auto sum_sims = [&](auto per_sim) {
+        double b = 0;
+        for (int s = 0; s < count(); ++s)
+            if ((sim_only < 0 || s == sim_only) && t_ < sims_[s].nt) b += per_sim(sims_[s]);
+        return b;
+    };
+    auto spec_bytes = [](const SimHost& h) { return (double)h.A * h.B * h.Ch * sizeof(float2); };
+    auto open_comps = [&](const SimHost& h, int ncomp) {
+        int n = 0;
+        for (int c = 0; c < ncomp; ++c) n += host_gate(h, job.gate, c) ? 1 : 0;
+        return n;
+    };
+    {
+        const Map& m = map_rows(rpc, comps_in, sim_only);
+        const double bytes = sum_sims([&](const SimHost& h) { return open_comps(h, comps_in) * ((double)h.N * 4 + spec_bytes(h)); });
+        timed(std::string("r2c:") + job.name, bytes, [&] {
+            launch_row_r2c(st(), d_sims_, d_t_, m.d, m.n, rj, (size_t)2 * M * (rpc + 1) * sizeof(float2));
+        });
+    }
+
+    auto col_tw = [&](int n, int bufs, long long lines_total) {
+        int tw = 16;
+        while (tw > 1 && (size_t)bufs * n * tw * sizeof(float2) > kSmemBudget) tw /= 2;
+        while (tw > 2 && lines_total / tw < 2 * 148) tw /= 2;
+        return tw;
+    };
+    auto lines_of = [&](int axis) {
+        long long L = 0;
+        for (int s = 0; s < count(); ++s)
+            if (sim_only < 0 || s == sim_only) {
+                const SimHost& h = sims_[s];
+                L += axis == 0 ? (long long)h.B * h.Cp : (long long)h.A * h.Cp;
+            }
+        return L;
+    };
+
+    int spec_final = job.spec_in;
+    if (dim_ >= 2) {
+        if (dim_ == 3) {
+            ColJob cj{};
+            cj.layout_axis = 1;
+            cj.mode = COL_FWD;
+            cj.spec_in = job.spec_in;
+            cj.tw_cols = col_tw(max_B_, 2, lines_of(1) * comps_in);
+            cj.gate = job.gate;
+            const Map& m = map_cols(1, cj.tw_cols, comps_in, sim_only);
+            const double bytes = sum_sims([&](const SimHost& h) { return open_comps(h, comps_in) * 2 * spec_bytes(h); });
+            timed(std::string("colB_fwd:") + job.name, bytes, [&] {
+                launch_col(st(), d_sims_, d_t_, m.d, m.n, cj, (size_t)2 * max_B_ * cj.tw_cols * sizeof(float2));
+            });
+        }
+        const int last = dim_ == 3 ? 0 : 1;
+        const int nlast = last == 0 ? max_A_ : max_B_;
+        ColJob cj{};
+        cj.layout_axis = last;
+        cj.mode = COL_FWD_OP_INV;
+        cj.spec_in = job.spec_in;
+        cj.spec_out = job.spec_out;
+        cj.nout = job.nout;
+        cj.fanout = job.fanout;
+        for (int c = 0; c < kMaxComp; ++c) cj.op[c] = job.op[c];
+        cj.tw_cols = col_tw(nlast, 3, lines_of(last) * (job.fanout ? 1 : job.nout));
+        cj.gate = job.gate;
+        {
+            const Map& m = map_cols(last, cj.tw_cols, job.fanout ? 1 : job.nout, sim_only);
+            const double bytes = sum_sims([&](const SimHost& h) {
+                const int no = open_comps(h, job.fanout ? 1 : job.nout);
+                if (no == 0) return 0.0;
+                const double tables = job.op[0].radial != RT_NONE ? (double)h.A * h.B * h.Ch * 4 : 0.0;
+                return job.fanout ? spec_bytes(h) * (1 + job.nout) + tables : no * (2 * spec_bytes(h) + tables);
+            });
+            timed(std::string(last == 0 ? "colA_op:" : "colB_op:") + job.name, bytes, [&] {
+                launch_col(st(), d_sims_, d_t_, m.d, m.n, cj, (size_t)3 * nlast * cj.tw_cols * sizeof(float2));
+            });
+        }
+        spec_final = job.spec_out;
+        if (dim_ == 3) {
+            ColJob ci{};
+            ci.layout_axis = 1;
+            ci.mode = COL_INV;
+            ci.spec_in = job.spec_out;
+            ci.tw_cols = col_tw(max_B_, 2, lines_of(1) * job.nout);
+            ci.gate = job.gate;
+            const Map& m = map_cols(1, ci.tw_cols, job.nout, sim_only);
+            const double bytes = sum_sims([&](const SimHost& h) {
+                return (job.fanout ? (open_comps(h, 1) ? job.nout : 0) : open_comps(h, job.nout)) * 2 * spec_bytes(h);
+            });
+            timed(std::string("colB_inv:") + job.name, bytes, [&] {
+                launch_col(st(), d_sims_, d_t_, m.d, m.n, ci, (size_t)2 * max_B_ * ci.tw_cols * sizeof(float2));
+            });
+        }
+    }
+
+    const int ncta = job.coupled ? job.nout : 1;
+    int rpc2 = 16;
+    while (rpc2 > 1 && (size_t)2 * M * (ncta * rpc2 + 1) * sizeof(float2) > kSmemBudget) rpc2 /= 2;
+    while (rpc2 > 1 && total_rows * (job.coupled ? 1 : job.nout) / rpc2 < 2 * 148) rpc2 /= 2;
+    RowC2RJob cj{};
+    cj.spec_in = spec_final;
+    cj.ncomp = ncta;
+    cj.epi = job.epi;
+    cj.out_field = job.out_field;
+    cj.rows_per_cta = rpc2;
+    cj.gate = job.gate;
+    const Map& m = map_rows(rpc2, job.coupled ? 1 : job.nout, sim_only);
+    const double bytes = sum_sims([&](const SimHost& h) {
+        int no = job.coupled ? (open_comps(h, 1) ? job.nout : 0) : open_comps(h, job.nout);
+        if (job.epi == EPI_EOS_ABS && no) no = h.dev.absorb == 3 ? 2 : 1;
+        if (no == 0) return 0.0;
+        return no * spec_bytes(h) + (double)h.N * epi_bytes(h, job.epi, job.coupled ? 1 : no);
+    });
+    timed(std::string("c2r:") + job.name, bytes, [&] {
+        launch_row_c2r(st(), d_sims_, d_t_, m.d, m.n, cj, (size_t)2 * M * (ncta * rpc2 + 1) * sizeof(float2));
+    });
+}
+
+// ------------------------------------------------------------------------------------------
+// one time step (KSFO:492-546)
+// ------------------------------------------------------------------------------------------
+void Engine::issue_step(bool first) {
+    const int D = dim_;
+    const int sp1 = D == 1 ? 0 : 1;   // first output spectrum
+
+    // velocity update: u_a = pml_sg (pml_sg u_a - dt/rho_sg Re F^-1(ddPos_a kappa F(p)))
+    SpecJob vel;
+    vel.in_field = FS_P;
+    vel.nin = 1;
+    vel.fanout = 1;
+    vel.nout = D;
+    for (int a = 0; a < D; ++a) vel.op[a] = OpSpec{AO_DPOS, (int8_t)a, RT_KAPPA, 0};
+    vel.spec_in = 0;
+    vel.spec_out = sp1;
+    vel.epi = EPI_VEL;
+    vel.name = "vel";
+    issue_job(vel, -1);
+
+    // velocity sources
+    if (any_u_direct_) timed("src_u", 0, [&] { launch_src_u(st(), d_sims_, d_t_, count(), max_usrc_, 0); });
+    if (any_u_add_) {
+        timed("src_u_scatter", 0, [&] { launch_src_u(st(), d_sims_, d_t_, count(), max_usrc_, 1); });
+        SpecJob us;
+        us.in_field = FS_SRCBUF;
+        us.nin = D;
+        us.nout = D;
+        for (int a = 0; a < D; ++a) us.op[a] = OpSpec{AO_NONE, (int8_t)a, RT_SKAPPA, (int8_t)a};
+        us.spec_in = sp1;
+        us.spec_out = sp1;
+        us.epi = EPI_ADD_U;
+        us.gate = GATE_USRC;
+        us.name = "usrc";
+        issue_job(us, -1);
+    }
+
+    // density update + (pointwise) equation of state
+    SpecJob den;
+    den.in_field = FS_U;
+    den.nin = D;
+    den.nout = D;
+    for (int a = 0; a < D; ++a) den.op[a] = OpSpec{AO_DNEG, (int8_t)a, RT_KAPPA, (int8_t)a};
+    den.spec_in = sp1;
+    den.spec_out = sp1;
+    den.epi = EPI_DEN;
+    den.coupled = 1;
+    den.name = "den";
+    issue_job(den, -1);
+
+    // pressure sources
+    if (any_p_direct_) timed("src_p", 0, [&] { launch_src_p(st(), d_sims_, d_t_, count(), max_psrc_, 0); });
+    if (any_p_add_) {
+        timed("src_p_scatter", 0, [&] { launch_src_p(st(), d_sims_, d_t_, count(), max_psrc_, 1); });
+        SpecJob ps;
+        ps.in_field = FS_SRCBUF;
+        ps.nin = 1;
+        ps.nout = 1;
+        ps.op[0] = OpSpec{AO_NONE, 0, RT_SKAPPA, 0};
+        ps.spec_in = 0;
+        ps.spec_out = 0;
+        ps.epi = EPI_ADD_RHO;
+        ps.gate = GATE_PSRC;
+        ps.name = "psrc";
+        issue_job(ps, -1);
+    }
+
+    // power-law absorption and dispersion, then the equation of state
+    if (any_abs_) {
+        SpecJob ab;
+        ab.in_field = FS_WORK;   // comp 0: rho0 * div u, comp 1: rho_sum
+        ab.nin = 2;
+        ab.nout = 2;
+        ab.op[0] = OpSpec{AO_NONE, 0, RT_NU1, 0};
+        ab.op[1] = OpSpec{AO_NONE, 0, RT_NU2, 1};
+        ab.spec_in = 0;
+        ab.spec_out = 0;
+        ab.epi = EPI_EOS_ABS;
+        ab.coupled = 1;
+        ab.gate = GATE_ABS;
+        ab.name = "abs";
+        issue_job(ab, -1);
+    }
+
+    // t = 0 override for an initial pressure (KSFO:514-521)
+    if (first && any_p0_) {
+        const Map& m = map_elems(-1);
+        launch_init_p0(st(), d_sims_, d_t_, m.d, m.n, d_p0s_);
+        SpecJob vi = vel;
+        vi.epi = EPI_VEL_INIT;
+        vi.gate = GATE_P0;
+        vi.name = "vel0";
+        issue_job(vi, -1);
+    }
+
+    // sensor sampling (KSFO:523-540)
+    if (any_recp_) timed("sample_p", 0, [&] { launch_sample(st(), d_sims_, d_t_, count(), max_pts_, 0, 0); });
+    if (any_recu_) {
+        SpecJob co;
+        co.in_field = FS_U;
+        co.nin = D;
+        co.nout = D;
+        for (int a = 0; a < D; ++a) co.op[a] = OpSpec{AO_COLLOC, (int8_t)a, RT_NONE, (int8_t)a};
+        co.spec_in = sp1;
+        co.spec_out = sp1;
+        co.epi = EPI_STORE;
+        co.out_field = FS_TMP;
+        co.gate = GATE_RECU;
+        co.name = "colloc";
+        issue_job(co, -1);
+        for (int a = 0; a < D; ++a) launch_sample(st(), d_sims_, d_t_, count(), max_pts_, 1, a);
+    }
+    timed("tick", 0, [&] { launch_tick(st(), d_t_); });
+}
+
+bool Engine::host_gate(const SimHost& h, int gate, int comp) const {
+    const SimDev& S = h.dev;
+    if (t_ >= h.nt) return false;
+    switch (gate) {
+        case GATE_PSRC: return S.has_p && t_ < S.psrc.len;
+        case GATE_USRC: return comp < h.dim && S.has_u[comp] && t_ < S.usrc[comp].len;
+        case GATE_P0: return S.has_p0 != 0;
+        case GATE_ABS: return comp == 0 ? S.absorb >= 2 : S.absorb == 3;
+        case GATE_RECU: return S.sensor.kind != 0 && (S.sensor.record_u_series || S.sensor.record_u_agg);
+        default: return true;
+    }
+}
+
+// Compulsory HBM bytes per grid point of a C2R epilogue (field reads and writes; scalars and
+// per-axis vectors cost nothing).
+double Engine::epi_bytes(const SimHost& h, int epi, int ncomp) const {
+    const SimDev& S = h.dev;
+    auto m = [](const FieldOrScalar& f) { return f.ptr ? 4.0 : 0.0; };
+    const int D = h.dim;
+    double eos = 4 + m(S.c2) + (S.absorb == 1 ? m(S.tau) : 0) + (S.nonlinear ? m(S.bona) : 0);
+    switch (epi) {
+        case EPI_STORE: return 4.0 * ncomp;
+        case EPI_VEL: { double b = 0; for (int a = 0; a < ncomp; ++a) b += 8 + m(S.dtor[a]); return b; }
+        case EPI_VEL_INIT: { double b = 0; for (int a = 0; a < ncomp; ++a) b += 4 + m(S.dtor[a]); return b; }
+        case EPI_ADD_U: return 8.0 * ncomp;
+        case EPI_DEN:
+            return 8.0 * D + 4 + m(S.dtrho0) + ((S.nonlinear || S.absorb >= 1) ? m(S.rho0) : 0) +
+                   (S.absorb >= 1 ? 4 : 0) + (S.eos_pointwise ? eos : 0);
+        case EPI_ADD_RHO: return 8.0 * D + 4 + (S.eos_pointwise ? eos + (S.absorb == 1 ? 4 : 0) : 0);
+        case EPI_EOS_ABS:
+            return 8 + m(S.c2) + m(S.tau) + (S.absorb == 3 ? m(S.eta) : 0) + (S.nonlinear ? m(S.bona) + m(S.rho0) : 0);
+        default: return 0;
+    }
+}
+
+std::vector<Engine::KernelTiming> Engine::profile_step(int reps) {
+    std::vector<KernelTiming> acc;
+    int tmax = 0;
+    for (auto& h : sims_) tmax = std::max(tmax, h.nt);
+    int done = 0;
+    for (int r = 0; r < reps && t_ < tmax; ++r) {
+        if (t_ == 0) { step(1); continue; }
+        std::vector<ProfRec> recs;
+        prof_ = &recs;
+        try {
+            issue_step(false);
+        } catch (...) {
+            prof_ = nullptr;
+            throw;
+        }
+        prof_ = nullptr;
+        ++t_;
+        check(cudaStreamSynchronize(st()), "profile sync");
+        if (acc.empty()) acc.resize(recs.size());
+        for (size_t i = 0; i < recs.size() && i < acc.size(); ++i) {
+            float ms = 0;
+            cudaEventElapsedTime(&ms, recs[i].a, recs[i].b);
+            acc[i].name = recs[i].name;
+            acc[i].bytes = recs[i].bytes;
+            acc[i].ms += ms;
+            cudaEventDestroy(recs[i].a);
+            cudaEventDestroy(recs[i].b);
+        }
+        ++done;
+    }
+    for (auto& k : acc) k.ms /= std::max(done, 1);
+    return acc;
+}
+
+void Engine::capture_graph() {
+    if (graph_exec_ && graph_stream_ == st()) return;
+    if (graph_exec_) { cudaGraphExecDestroy(graph_exec_); graph_exec_ = nullptr; }
+    if (graph_) { cudaGraphDestroy(graph_); graph_ = nullptr; }
+    check(cudaStreamBeginCapture(st(), cudaStreamCaptureModeThreadLocal), "begin capture");
+    try {
+        issue_step(false);
+    } catch (...) {
+        cudaGraph_t g;
+        cudaStreamEndCapture(st(), &g);
+        if (g) cudaGraphDestroy(g);
+        throw;
+    }
+    check(cudaStreamEndCapture(st(), &graph_), "end capture");
+    check(cudaGraphInstantiate(&graph_exec_, graph_, 0), "graph instantiate");
+    graph_stream_ = st();
+}
+
+// ------------------------------------------------------------------------------------------
+// setup of one simulation
+// ------------------------------------------------------------------------------------------
+static std::vector<int> flat_nonzero(const float* m, long long N) {
+    std::vector<int> r;
+    for (long long i = 0; i < N; ++i)
+        if (m[i] != 0.0f) r.push_back((int)i);
+    return r;
+}
+
+void Engine::smooth_field(int s, float* field) {
+    // smooth(..., restore_max): Re F^-1(W F(f)) * max|f| / max|out| (Filter/Filters.swift:273-347).
+    // The window is applied as its Hermitian part (W(k) + W(-k))/2, which gives exactly the real
+    // part the reference takes.
+    SimHost& h = sims_[s];
+    check(cudaMemcpyAsync(h.dev.tmp[0], field, h.N * sizeof(float), cudaMemcpyDeviceToDevice, st()), "copy");
+    check(cudaMemsetAsync(d_red_, 0, 2 * sizeof(unsigned int), st()), "memset");
+    launch_absmax(st(), h.dev.tmp[0], h.N, d_red_);
+    SpecJob sj;
+    sj.in_field = FS_TMP;
+    sj.nin = 1;
+    sj.nout = 1;
+    sj.op[0] = OpSpec{AO_NONE, 0, RT_WINDOW, 0};
+    sj.epi = EPI_STORE;
+    sj.out_field = FS_TMP;
+    sj.name = "smooth";
+    issue_job(sj, s);
+    launch_absmax(st(), h.dev.tmp[0], h.N, d_red_ + 1);
+    launch_scale(st(), h.dev.tmp[0], h.N, d_red_, d_red_ + 1);
+    check(cudaMemcpyAsync(field, h.dev.tmp[0], h.N * sizeof(float), cudaMemcpyDeviceToDevice, st()), "copy");
+}
+
+void Engine::setup_sim(int s, const kw_sim_desc& d) {
+    SimHost& h = sims_[s];
+    h.d = d;
+    if (d.abi_version != KW_ABI_VERSION) throw err(KW_ERR_INVALID, "descriptor abi_version mismatch");
+    if (d.dim < 1 || d.dim > 3) throw err(KW_ERR_INVALID, "kspaceFirstOrder: dim " + std::to_string(d.dim) + " not yet implemented");
+    h.dim = d.dim;
+    const int nref[3] = {d.nx, d.ny, d.nz};
+    const double dref[3] = {d.dx, d.dy, d.dz};
+    for (int a = 0; a < h.dim; ++a) {
+        if (nref[a] < 1) throw err(KW_ERR_INVALID, "grid size must be positive");
+        if (!(dref[a] > 0)) throw err(KW_ERR_INVALID, "grid spacing must be positive");
+        if (nref[a] > 8192) throw err(KW_ERR_UNSUPPORTED, "axis length above 8192");
+        h.n_ref[a] = nref[a];
+        h.d_ref[a] = dref[a];
+    }
+    if (d.nt <= 0) throw err(KW_ERR_INVALID, "call grid.makeTime(...) before running the solver");
+    if (!(d.dt > 0)) throw err(KW_ERR_INVALID, "dt must be positive");
+    if (!d.p0 && !d.p_mask && !d.u_mask)
+        throw err(KW_ERR_INVALID, std::to_string(h.dim) + "D solver requires source.p0 or a time-varying p/u source");
+    h.nt = d.nt;
+    if (h.dim == 1) { h.A = 1; h.B = 1; h.C = d.nx; }
+    else if (h.dim == 2) { h.A = 1; h.B = d.nx; h.C = d.ny; }
+    else { h.A = d.nx; h.B = d.ny; h.C = d.nz; }
+    h.N = (long long)h.A * h.B * h.C;
+    if (h.N > (1LL << 31) - 1) throw err(KW_ERR_UNSUPPORTED, "grids above 2^31 points are not supported");
+    h.Ch = h.C / 2 + 1;
+    h.Cp = h.Ch + (h.Ch & 1);
+    h.Ns = (long long)h.A * h.B * h.Cp;
+    const long long N = h.N;
+    auto grid_sized = [&](const kw_array& a) { return a.data && (a.len == 1 || (long long)a.len == N); };
+    if (!grid_sized(d.sound_speed)) throw err(KW_ERR_INVALID, "soundSpeed must be scalar or grid-shaped");
+    if (!grid_sized(d.density)) throw err(KW_ERR_INVALID, "density must be scalar or grid-shaped");
+    if (d.pml_size < 0) throw err(KW_ERR_INVALID, "pmlSize must be non-negative");
+    for (int a = 0; a < h.dim; ++a)
+        if (d.pml_size > h.n_ref[a]) throw err(KW_ERR_INVALID, "pmlSize larger than the grid");
+    if (d.alpha_coeff.data && !grid_sized(d.alpha_coeff)) throw err(KW_ERR_INVALID, "alphaCoeff must be scalar or grid-shaped");
+    if (d.b_on_a.data && !grid_sized(d.b_on_a)) throw err(KW_ERR_INVALID, "bOnA must be scalar or grid-shaped");
+    if (d.directivity_angle && h.dim == 2 && d.sensor_kind == KW_SENSOR_BINARY)
+        throw err(KW_ERR_UNSUPPORTED, "2D sensor directivity is not available in this build");
+
+    SimDev& v = h.dev;
+    std::memset(&v, 0, sizeof(v));
+    v.dim = h.dim; v.A = h.A; v.B = h.B; v.C = h.C; v.Ch = h.Ch; v.Cp = h.Cp;
+    v.N = h.N; v.Ns = h.Ns; v.nt = h.nt;
+    v.inv_n = (float)(1.0 / (double)N);
+    for (int L = 0; L < 3; ++L) v.axis_of_layout[L] = L + h.dim - 3;
+
+    // FFT plans
+    const bool odd = (h.C & 1) != 0;
+    build_plan(v.plan_row, odd ? h.C : h.C / 2);
+    build_plan(v.plan_b, h.B);
+    build_plan(v.plan_a, h.A);
+    {
+        std::vector<float2> rt(h.C / 2 + 1);
+        for (int k = 0; k <= h.C / 2; ++k) {
+            const double a = -2.0 * M_PI * (double)k / (double)h.C;
+            rt[k] = make_float2((float)std::cos(a), (float)std::sin(a));
+        }
+        v.row_tw = upload(rt);
+    }
+    max_A_ = std::max(max_A_, h.A);
+    max_B_ = std::max(max_B_, h.B);
+    max_M_ = std::max(max_M_, odd ? h.C : h.C / 2);
+
+    // device fields
+    const size_t fb = (size_t)N * sizeof(float);
+    const int nspec = h.dim + 1;
+    for (int i = 0; i < nspec; ++i) v.spec[i] = (float2*)dalloc((size_t)h.Ns * sizeof(float2));
+    v.p = (float*)dalloc(fb);
+    v.rho_sum = (float*)dalloc(fb);
+    for (int a = 0; a < h.dim; ++a) {
+        v.u[a] = (float*)dalloc(fb);
+        v.rho[a] = (float*)dalloc(fb);
+    }
+    v.tmp[0] = (float*)dalloc(fb);
+    v.nonfinite = d_flag_;
+
+    // ---- medium; smoothing on the device (KSFO:367-373) ----
+    const bool c0map = d.sound_speed.len > 1, rho0map = d.density.len > 1;
+    std::vector<double> c0(c0map ? N : 1), rho0(rho0map ? N : 1);
+    auto smooth_to_host = [&](const float* src, std::vector<double>& dst) {
+        float* f = (float*)dalloc(fb);
+        check(cudaMemcpyAsync(f, src, fb, cudaMemcpyHostToDevice, st()), "upload");
+        // the smoothing job needs the device descriptor (plans, buffers, window)
+        check(cudaMemcpyAsync(d_sims_ + s, &v, sizeof(SimDev), cudaMemcpyHostToDevice, st()), "upload sim");
+        smooth_field(s, f);
+        std::vector<float> host(N);
+        check(cudaMemcpyAsync(host.data(), f, fb, cudaMemcpyDeviceToHost, st()), "download");
+        check(cudaStreamSynchronize(st()), "sync");
+        for (long long i = 0; i < N; ++i) dst[i] = host[i];
+        return f;
+    };
+    const bool need_window = (d.smooth_c0 && c0map) || (d.smooth_rho0 && rho0map) || (d.p0 && d.smooth_p0);
+    if (need_window) {
+        // FFT-order smoothing window of the reference (Filters.swift:218-321), Hermitian part,
+        // over the half spectrum. 2D fills out[i][j] = win[(i+sx)%nx][(j+sy)%ny]; 1D/3D fill
+        // out[(i+sx)%n] = win[i]; both are reproduced.
+        std::vector<int> enl(h.dim);
+        int Lw = 1;
+        for (int a = 0; a < h.dim; ++a) { enl[a] = h.n_ref[a] % 2 ? h.n_ref[a] : h.n_ref[a] + 1; Lw = std::max(Lw, enl[a]); }
+        std::vector<double> winLin(Lw, 1.0);
+        if (Lw > 1)
+            for (int i = 0; i < Lw; ++i) {
+                const double x = 2.0 * M_PI * (double)i / (double)(Lw - 1);
+                winLin[i] = 0.42 - 0.5 * std::cos(x) + 0.08 * std::cos(2.0 * x);
+            }
+        const double radius = (double)(Lw - 1) / 2.0;
+        std::vector<std::vector<double>> pos(h.dim);   // window-axis coordinate of FFT-order index m
+        for (int a = 0; a < h.dim; ++a) {
+            const int n = h.n_ref[a], cnt = enl[a];
+            const int sx = (n + 1) / 2;
+            pos[a].resize(n);
+            for (int m = 0; m < n; ++m) {
+                const int wi = h.dim == 2 ? (m + sx) % n : ((m - sx) % n + n) % n;
+                pos[a][m] = cnt <= 1 ? 0.0 : -radius + 2.0 * radius * (double)wi / (double)(cnt - 1);
+            }
+        }
+        auto interp = [&](double r) {
+            const double p = std::min(r, radius) + radius;
+            const int i0 = std::min((int)std::floor(p), (int)winLin.size() - 2);
+            if (winLin.size() < 2) return 1.0;
+            const double fr = p - (double)i0;
+            return std::fabs(winLin[i0] * (1.0 - fr) + winLin[i0 + 1] * fr);
+        };
+        auto W = [&](const int* m) {
+            double r2 = 0;
+            for (int a = 0; a < h.dim; ++a) r2 += pos[a][m[a]] * pos[a][m[a]];
+            return interp(std::sqrt(r2));
+        };
+        std::vector<float> tab((size_t)h.Ns, 0.f);
+        for (int ia = 0; ia < h.A; ++ia)
+            for (int ib = 0; ib < h.B; ++ib)
+                for (int kc = 0; kc < h.Ch; ++kc) {
+                    int lay[3] = {ia, ib, kc}, ln[3] = {h.A, h.B, h.C};
+                    int m[3], mm[3];
+                    for (int a = 0; a < h.dim; ++a) {
+                        const int L = a + 3 - h.dim;
+                        m[a] = lay[L];
+                        mm[a] = (ln[L] - lay[L]) % ln[L];
+                    }
+                    tab[((size_t)ia * h.B + ib) * h.Cp + kc] = (float)(0.5 * (W(m) + W(mm)));
+                }
+        v.radial[RT_WINDOW] = upload(tab);
+    }
+    float* d_c0 = nullptr;
+    float* d_rho0 = nullptr;
+    if (d.smooth_c0 && c0map) d_c0 = smooth_to_host(d.sound_speed.data, c0);
+    else for (size_t i = 0; i < c0.size(); ++i) c0[i] = d.sound_speed.data[i];
+    if (d.smooth_rho0 && rho0map) d_rho0 = smooth_to_host(d.density.data, rho0);
+    else for (size_t i = 0; i < rho0.size(); ++i) rho0[i] = d.density.data[i];
+    (void)d_c0;
+    (void)d_rho0;
+    if (d.p0) {
+        float* f = (float*)dalloc(fb);
+        check(cudaMemcpyAsync(f, d.p0, fb, cudaMemcpyHostToDevice, st()), "upload p0");
+        if (d.smooth_p0) {
+            check(cudaMemcpyAsync(d_sims_ + s, &v, sizeof(SimDev), cudaMemcpyHostToDevice, st()), "upload sim");
+            smooth_field(s, f);
+        }
+        h.p0s = f;
+        v.has_p0 = 1;
+    }
+    auto c0_at = [&](long long i) { return c0map ? c0[i] : c0[0]; };
+    auto rho0_at = [&](long long i) { return rho0map ? rho0[i] : rho0[0]; };
+
+    // referenceSoundSpeed (KSFO:786-788), or the caller's fixed value
+    double cref = c0[0];
+    if (c0map) for (double x : c0) cref = std::max(cref, x);
+    if (!std::isnan(d.c_ref)) cref = d.c_ref;
+    h.cref = cref;
+    const double dt = d.dt;
+
+    // ---- per-axis operators, PML (KSFO:376-397, 764-769) ----
+    std::vector<std::vector<double>> kv(h.dim);
+    for (int a = 0; a < h.dim; ++a) {
+        const int n = h.n_ref[a];
+        const double dd = h.d_ref[a];
+        kv[a] = wavenumbers(n, dd);
+        std::vector<float2> dp(n), dn(n), co(n);
+        for (int i = 0; i < n; ++i) {
+            const double k = kv[a][i], th = k * (dd / 2.0);
+            const bool nyq = (n % 2 == 0) && i == n / 2;   // self-conjugate bin: Hermitian part
+            dp[i] = make_float2((float)(-k * std::sin(th)), nyq ? 0.f : (float)(k * std::cos(th)));
+            dn[i] = make_float2((float)(k * std::sin(th)), nyq ? 0.f : (float)(k * std::cos(th)));
+            co[i] = make_float2((float)std::cos(th), nyq ? 0.f : (float)(-std::sin(th)));
+        }
+        AxisDev& ax = v.ax[a];
+        ax.n = n;
+        ax.dpos = upload(dp);
+        ax.dneg = upload(dn);
+        ax.colloc = upload(co);
+        ax.pml = upload(to_f32(pml_profile(n, dd, dt, cref, d.pml_size, d.pml_alpha, false)));
+        ax.pml_sg = upload(to_f32(pml_profile(n, dd, dt, cref, d.pml_size, d.pml_alpha, true)));
+        ax.inv_d = (float)(1.0 / dd);
+    }
+
+    // ---- medium-derived quantities ----
+    auto field_or_scalar = [&](bool map, auto f) {
+        FieldOrScalar r{nullptr, 0.f};
+        if (!map) { r.s = (float)f(0); return r; }
+        std::vector<float> tmp(N);
+        for (long long i = 0; i < N; ++i) tmp[i] = (float)f(i);
+        r.ptr = upload(tmp);
+        return r;
+    };
+    v.c2 = field_or_scalar(c0map, [&](long long i) { return c0_at(i) * c0_at(i); });
+    v.dtrho0 = field_or_scalar(rho0map, [&](long long i) { return dt * rho0_at(i); });
+    v.rho0 = field_or_scalar(rho0map, [&](long long i) { return rho0_at(i); });
+    for (int a = 0; a < h.dim; ++a) {
+        // staggerDensity (KSFO:799-806): mean of neighbours, last index replicated
+        const int L = a + 3 - h.dim;
+        const long long stride = L == 2 ? 1 : (L == 1 ? h.C : (long long)h.B * h.C);
+        const int n = h.n_ref[a];
+        v.dtor[a] = field_or_scalar(rho0map, [&](long long i) {
+            if (!rho0map) return dt / rho0[0];
+            const long long ia = (i / stride) % n;
+            const double sg = ia < n - 1 ? 0.5 * (rho0[i] + rho0[i + stride]) : rho0[i];
+            return dt / sg;
+        });
+    }
+
+    // absorption (KSFO:851-882)
+    v.absorb = 0;
+    double y = 1.5;
+    if (d.alpha_coeff.data && d.alpha_mode != KW_ABSORPTION_NONE) {
+        y = std::isnan(d.alpha_power) ? 1.5 : d.alpha_power;
+        if (d.alpha_mode == KW_ABSORPTION_STOKES) y = 2.0;
+        const bool amap = d.alpha_coeff.len > 1;
+        const double np1 = db2neper(1.0, y);
+        auto anp = [&](long long i) { return (double)d.alpha_coeff.data[amap ? i : 0] * np1; };
+        const bool stokes = d.alpha_mode == KW_ABSORPTION_STOKES || std::fabs(y - 2.0) < 1e-10;
+        if (stokes) {
+            v.absorb = 1;
+            v.tau = field_or_scalar(amap || c0map, [&](long long i) { return -2.0 * anp(i) * c0_at(i); });
+        } else {
+            v.absorb = d.alpha_mode == KW_ABSORPTION_NO_DISPERSION ? 2 : 3;
+            v.tau = field_or_scalar(amap || c0map, [&](long long i) { return -2.0 * anp(i) * std::pow(c0_at(i), y - 1.0); });
+            if (v.absorb == 3) {
+                const double tn = std::tan(M_PI * y / 2.0);
+                v.eta = field_or_scalar(amap || c0map, [&](long long i) { return 2.0 * anp(i) * std::pow(c0_at(i), y) * tn; });
+            }
+        }
+        v.div_term = (float*)dalloc(fb);
+    }
+    v.eos_pointwise = v.absorb < 2 ? 1 : 0;
+    // nonlinearity (KSFO:902-907)
+    v.nonlinear = 0;
+    if (d.b_on_a.data) {
+        const bool bmap = d.b_on_a.len > 1;
+        double mx = 0;
+        for (size_t i = 0; i < d.b_on_a.len; ++i) mx = std::max(mx, (double)std::fabs(d.b_on_a.data[i]));
+        if (mx != 0.0) {
+            v.nonlinear = 1;
+            v.bona = field_or_scalar(bmap, [&](long long i) { return (double)d.b_on_a.data[bmap ? i : 0]; });
+        }
+    }
+
+    // ---- sources (KSFO:404-423, 129-201) ----
+    const double nd = (double)h.dim;
+    bool need_skappa = false;
+    if (d.p_mask && d.p.data) {
+        std::vector<int> idx = flat_nonzero(d.p_mask, N);
+        if (!idx.empty()) {
+            if (d.p.rows != 1 && d.p.rows != (int)idx.size())
+                throw err(KW_ERR_INVALID, "source.p rows must be 1 or the number of source points");
+            if (d.p.len < 0) throw err(KW_ERR_INVALID, "source.p length must be non-negative");
+            SourceDev& sd = v.psrc;
+            sd.nsrc = (int)idx.size();
+            sd.rows = d.p.rows;
+            sd.len = d.p.len;
+            sd.mode = d.p_mode;
+            sd.idx = upload(idx);
+            sd.signal = upload(std::vector<float>(d.p.data, d.p.data + (size_t)d.p.rows * std::max(d.p.len, 0)));
+            if (d.p_mode == KW_SOURCE_DIRICHLET) {
+                std::vector<float> sc(idx.size());
+                for (size_t q = 0; q < idx.size(); ++q) { const double c = c0_at(idx[q]); sc[q] = (float)(1.0 / (nd * c * c)); }
+                sd.scale[0] = upload(sc);
+            } else if (d.p_mode == KW_SOURCE_ADDITIVE_NO_CORRECTION) {
+                for (int a = 0; a < h.dim; ++a) {
+                    std::vector<float> sc(idx.size());
+                    for (size_t q = 0; q < idx.size(); ++q) sc[q] = (float)(2.0 * dt / (nd * c0_at(idx[q]) * h.d_ref[a]));
+                    sd.scale[a] = upload(sc);
+                }
+            } else {
+                std::vector<float> sc(idx.size());
+                for (size_t q = 0; q < idx.size(); ++q) sc[q] = (float)(2.0 * dt / (nd * c0_at(idx[q])));
+                sd.scale[0] = upload(sc);
+                v.src_buf[0] = (float*)dalloc(fb);
+                need_skappa = true;
+                any_p_add_ = true;
+            }
+            if (d.p_mode != KW_SOURCE_ADDITIVE) any_p_direct_ = true;
+            v.has_p = sd.len > 0;
+            max_psrc_ = std::max(max_psrc_, sd.nsrc);
+        }
+    }
+    if (d.u_mask) {
+        std::vector<int> idx = flat_nonzero(d.u_mask, N);
+        const kw_signal* sig[3] = {&d.ux, &d.uy, &d.uz};
+        if (!idx.empty()) {
+            int* didx = upload(idx);
+            for (int a = 0; a < h.dim; ++a) {
+                if (!sig[a]->data) continue;
+                if (sig[a]->rows != 1 && sig[a]->rows != (int)idx.size())
+                    throw err(KW_ERR_INVALID, "source velocity rows must be 1 or the number of source points");
+                SourceDev& sd = v.usrc[a];
+                sd.nsrc = (int)idx.size();
+                sd.rows = sig[a]->rows;
+                sd.len = std::max(sig[a]->len, 0);
+                sd.mode = d.u_mode;
+                sd.idx = didx;
+                sd.signal = upload(std::vector<float>(sig[a]->data, sig[a]->data + (size_t)sd.rows * sd.len));
+                std::vector<float> sc(idx.size());
+                for (size_t q = 0; q < idx.size(); ++q)
+                    sc[q] = d.u_mode == KW_SOURCE_DIRICHLET ? 1.f : (float)(2.0 * c0_at(idx[q]) * dt / h.d_ref[a]);
+                sd.scale[0] = upload(sc);
+                if (d.u_mode == KW_SOURCE_ADDITIVE) {
+                    v.src_buf[a] = (float*)dalloc(fb);
+                    need_skappa = true;
+                    any_u_add_ = true;
+                } else {
+                    any_u_direct_ = true;
+                }
+                v.has_u[a] = sd.len > 0;
+                max_usrc_ = std::max(max_usrc_, sd.nsrc);
+            }
+        }
+    }
+
+    // ---- radial tables over the half spectrum (FP64 -> FP32) ----
+    {
+        std::vector<double> kA(h.A, 0.0), kB(h.B, 0.0), kC(h.C, 0.0);
+        for (int a = 0; a < h.dim; ++a) {
+            const int L = a + 3 - h.dim;
+            std::vector<double>& dst = L == 0 ? kA : (L == 1 ? kB : kC);
+            dst = kv[a];
+        }
+        const size_t Ns = (size_t)h.Ns;
+        std::vector<float> kap(Ns, 0.f), skap, nu1, nu2;
+        if (need_skappa) skap.assign(Ns, 0.f);
+        if (v.absorb >= 2) { nu1.assign(Ns, 0.f); if (v.absorb == 3) nu2.assign(Ns, 0.f); }
+        const double half = cref * dt / 2.0;
+        for (int ia = 0; ia < h.A; ++ia)
+            for (int ib = 0; ib < h.B; ++ib)
+                for (int kc = 0; kc < h.Ch; ++kc) {
+                    const size_t i = ((size_t)ia * h.B + ib) * h.Cp + kc;
+                    const double k = std::sqrt(kA[ia] * kA[ia] + kB[ib] * kB[ib] + kC[kc] * kC[kc]);
+                    const double arg = k * half;
+                    kap[i] = (float)(arg == 0.0 ? 1.0 : std::sin(arg) / arg);
+                    if (need_skappa) skap[i] = (float)std::cos(arg);
+                    if (v.absorb >= 2) {
+                        nu1[i] = (float)(k == 0.0 ? 0.0 : std::pow(k, y - 2.0));
+                        if (v.absorb == 3) nu2[i] = (float)(k == 0.0 ? 0.0 : std::pow(k, y - 1.0));
+                    }
+                }
+        v.radial[RT_KAPPA] = upload(kap);
+        if (need_skappa) v.radial[RT_SKAPPA] = upload(skap);
+        if (v.absorb >= 2) {
+            v.radial[RT_NU1] = upload(nu1);
+            if (v.absorb == 3) v.radial[RT_NU2] = upload(nu2);
+        }
+    }
+
+    // ---- sensor (REC:8-97) ----
+    const unsigned rec = d.record;
+    h.record_p = (rec & (KW_RECORD_P | KW_RECORD_P_MAX | KW_RECORD_P_MIN | KW_RECORD_P_RMS | KW_RECORD_I_AVG)) != 0;
+    h.record_u = (rec & (KW_RECORD_UX | KW_RECORD_UY | KW_RECORD_UZ | KW_RECORD_U_MAX | KW_RECORD_U_RMS | KW_RECORD_I_AVG)) != 0;
+    h.record_ufinal = (rec & KW_RECORD_U_FINAL) != 0;
+    SensorDev& sn = v.sensor;
+    if (d.sensor_mask && (d.sensor_kind == KW_SENSOR_BINARY || d.sensor_kind == KW_SENSOR_CARTESIAN)) {
+        if (d.sensor_kind == KW_SENSOR_BINARY) {
+            std::vector<int> idx = flat_nonzero(d.sensor_mask, N);
+            sn.kind = 1;
+            sn.npts = (int)idx.size();
+            sn.ncorners = 1;
+            sn.idx = upload(idx);
+        } else {
+            if (d.sensor_points < 0) throw err(KW_ERR_INVALID, "sensor_points must be non-negative");
+            const int np = d.sensor_points, nc = 1 << h.dim;
+            std::vector<int> idx((size_t)np * nc);
+            std::vector<float> w((size_t)np * nc);
+            for (int p = 0; p < np; ++p) {
+                int i0[3];
+                double fr[3];
+                for (int a = 0; a < h.dim; ++a) {
+                    const double g = (double)d.sensor_mask[(size_t)a * np + p] / h.d_ref[a] + (double)(h.n_ref[a] / 2);
+                    if (!(g >= 0 && g <= (double)(h.n_ref[a] - 1)))
+                        throw err(KW_ERR_INVALID, "Cartesian sensor point outside grid bounds (axis " + std::to_string(a) + ")");
+                    const double f = std::floor(g);
+                    i0[a] = (int)f;
+                    fr[a] = g - f;
+                }
+                for (int c = 0; c < nc; ++c) {
+                    long long flat = 0;
+                    double ww = 1.0;
+                    for (int a = 0; a < h.dim; ++a) {
+                        const int bit = (c >> a) & 1;
+                        const int ai = std::min(i0[a] + bit, h.n_ref[a] - 1);
+                        ww *= bit == 1 ? fr[a] : (1.0 - fr[a]);
+                        flat = flat * h.n_ref[a] + ai;
+                    }
+                    idx[(size_t)p * nc + c] = (int)flat;
+                    w[(size_t)p * nc + c] = (float)ww;
+                }
+            }
+            sn.kind = 2;
+            sn.npts = np;
+            sn.ncorners = nc;
+            sn.idx = upload(idx);
+            sn.w = upload(w);
+        }
+        h.npts = sn.npts;
+        h.p_series = h.record_p && (rec & (KW_RECORD_P | KW_RECORD_I_AVG));
+        h.p_agg = h.record_p && (rec & (KW_RECORD_P_MAX | KW_RECORD_P_MIN | KW_RECORD_P_RMS));
+        h.u_series = h.record_u && (rec & (KW_RECORD_UX | KW_RECORD_UY | KW_RECORD_UZ | KW_RECORD_I_AVG));
+        h.u_agg = h.record_u && (rec & (KW_RECORD_U_MAX | KW_RECORD_U_RMS));
+        sn.record_p_series = h.p_series;
+        sn.record_p_agg = h.p_agg;
+        sn.record_u_series = h.u_series;
+        sn.record_u_agg = h.u_agg;
+        const size_t np = (size_t)std::max(sn.npts, 1);
+        if (h.p_series) sn.p_series = (float*)dalloc((size_t)h.nt * np * sizeof(float));
+        if (h.p_agg) {
+            sn.p_max = (float*)dalloc(np * 4); sn.p_min = (float*)dalloc(np * 4);
+            sn.p_ss = (float*)dalloc(np * 4); sn.p_ssc = (float*)dalloc(np * 4);
+        }
+        if (h.record_u) {
+            for (int a = 1; a < h.dim; ++a) v.tmp[a] = (float*)dalloc(fb);
+            for (int a = 0; a < h.dim; ++a) {
+                if (h.u_series) sn.u_series[a] = (float*)dalloc((size_t)h.nt * np * sizeof(float));
+                if (h.u_agg) {
+                    sn.u_max[a] = (float*)dalloc(np * 4);
+                    sn.u_ss[a] = (float*)dalloc(np * 4);
+                    sn.u_ssc[a] = (float*)dalloc(np * 4);
+                }
+            }
+            any_recu_ = true;
+        }
+        if (h.record_p) any_recp_ = true;
+        max_pts_ = std::max(max_pts_, sn.npts);
+    }
+    if (v.absorb >= 2) any_abs_ = true;
+    if (v.has_p0) any_p0_ = true;
+    check(cudaMemcpyAsync(d_sims_ + s, &v, sizeof(SimDev), cudaMemcpyHostToDevice, st()), "upload sim");
+}
+
+void Engine::create(const kw_sim_desc* descs, int n) {
+    if (n <= 0) throw err(KW_ERR_INVALID, "no simulations");
+    check(cudaSetDevice(ctx_->device), "cudaSetDevice");
+    sims_.resize(n);
+    outs_.resize(n);
+    dim_ = descs[0].dim;
+    for (int i = 1; i < n; ++i)
+        if (descs[i].dim != dim_) throw err(KW_ERR_INVALID, "all simulations of a batch must have the same dimensionality");
+    d_sims_ = (SimDev*)dalloc(sizeof(SimDev) * n);
+    d_t_ = (int*)dalloc(sizeof(int));
+    d_flag_ = (int*)dalloc(sizeof(int));
+    d_red_ = (unsigned int*)dalloc(4 * sizeof(unsigned int));
+    for (int i = 0; i < n; ++i) setup_sim(i, descs[i]);
+    std::vector<const float*> p0s(n);
+    for (int i = 0; i < n; ++i) p0s[i] = sims_[i].p0s;
+    d_p0s_ = (const float**)dalloc(sizeof(float*) * n);
+    check(cudaMemcpyAsync(d_p0s_, p0s.data(), sizeof(float*) * n, cudaMemcpyHostToDevice, st()), "upload");
+    check(cudaStreamSynchronize(st()), "setup sync");
+    reset();
+}
+
+void Engine::reset() {
+    for (auto& h : sims_) {
+        const size_t fb = (size_t)h.N * sizeof(float);
+        SimDev& v = h.dev;
+        check(cudaMemsetAsync(v.p, 0, fb, st()), "reset");
+        check(cudaMemsetAsync(v.rho_sum, 0, fb, st()), "reset");
+        if (v.div_term) check(cudaMemsetAsync(v.div_term, 0, fb, st()), "reset");
+        for (int a = 0; a < h.dim; ++a) {
+            check(cudaMemsetAsync(v.u[a], 0, fb, st()), "reset");
+            check(cudaMemsetAsync(v.rho[a], 0, fb, st()), "reset");
+        }
+        for (int a = 0; a < kMaxComp; ++a)
+            if (v.src_buf[a]) check(cudaMemsetAsync(v.src_buf[a], 0, fb, st()), "reset");
+    }
+    check(cudaMemsetAsync(d_t_, 0, sizeof(int), st()), "reset");
+    check(cudaMemsetAsync(d_flag_, 0, sizeof(int), st()), "reset");
+    t_ = 0;
+    finalized_t_ = -1;
+}
+
+void Engine::step(int nsteps) {
+    check(cudaGetLastError(), "pending error before step");
+    int tmax = 0;
+    for (auto& h : sims_) tmax = std::max(tmax, h.nt);
+    nsteps = std::min(nsteps, tmax - t_);
+    for (int k = 0; k < nsteps; ++k) {
+        if (t_ == 0) {
+            issue_step(true);
+        } else {
+            capture_graph();
+            check(cudaGraphLaunch(graph_exec_, st()), "graph launch");
+        }
+        ++t_;
+    }
+    check(cudaGetLastError(), "launch");
+}
+
+void Engine::run(const kw_callbacks* cb) {
+    reset();
+    int tmax = 0;
+    for (auto& h : sims_) tmax = std::max(tmax, h.nt);
+    const int interval = cb && cb->monitor_interval > 0 ? cb->monitor_interval : 1;
+    std::vector<float> host;
+    for (int t = 0; t < tmax; ++t) {
+        step(1);
+        if (cb && cb->monitor && t % interval == 0) {
+            const SimHost& h = sims_[0];
+            host.resize(h.N);
+            check(cudaMemcpyAsync(host.data(), h.dev.p, h.N * sizeof(float), cudaMemcpyDeviceToHost, st()), "monitor copy");
+            check(cudaStreamSynchronize(st()), "monitor sync");
+            cb->monitor(t, host.data(), host.size(), cb->user);
+        }
+        if (cb && cb->progress) cb->progress(t, tmax, cb->user);
+    }
+}
+
+int Engine::synchronize() {
+    const Map& m = map_elems(-1);
+    launch_check_finite(st(), d_sims_, d_t_, m.d, m.n);
+    check(cudaStreamSynchronize(st()), "synchronize");
+    int flag = 0;
+    check(cudaMemcpy(&flag, d_flag_, sizeof(int), cudaMemcpyDeviceToHost), "flag");
+    return flag ? KW_ERR_NONFINITE : KW_OK;
+}
+
+// ------------------------------------------------------------------------------------------
+// outputs (REC:129-168)
+// ------------------------------------------------------------------------------------------
+static bool present(const SimHost& h, int f, int T) {
+    const unsigned r = h.d.record;
+    const bool smp = h.dev.sensor.kind != 0 && T > 0;
+    const int a = (f - KW_FIELD_UX) % 3;
+    switch (f) {
+        case KW_FIELD_P: return smp && (r & KW_RECORD_P);
+        case KW_FIELD_P_MAX: return smp && (r & KW_RECORD_P_MAX);
+        case KW_FIELD_P_MIN: return smp && (r & KW_RECORD_P_MIN);
+        case KW_FIELD_P_RMS: return smp && (r & KW_RECORD_P_RMS);
+        case KW_FIELD_P_FINAL: return true;
+        case KW_FIELD_UX: case KW_FIELD_UY: case KW_FIELD_UZ:
+            return smp && a < h.dim && (r & (KW_RECORD_UX << a));
+        case KW_FIELD_UX_MAX: case KW_FIELD_UY_MAX: case KW_FIELD_UZ_MAX:
+            return smp && ((f - KW_FIELD_UX_MAX) < h.dim) && (r & KW_RECORD_U_MAX);
+        case KW_FIELD_UX_RMS: case KW_FIELD_UY_RMS: case KW_FIELD_UZ_RMS:
+            return smp && ((f - KW_FIELD_UX_RMS) < h.dim) && (r & KW_RECORD_U_RMS);
+        case KW_FIELD_UX_FINAL: case KW_FIELD_UY_FINAL: case KW_FIELD_UZ_FINAL:
+            return ((f - KW_FIELD_UX_FINAL) < h.dim) && (r & KW_RECORD_U_FINAL);
+        case KW_FIELD_IX_AVG: case KW_FIELD_IY_AVG: case KW_FIELD_IZ_AVG:
+            return smp && ((f - KW_FIELD_IX_AVG) < h.dim) && (r & KW_RECORD_I_AVG);
+        default: return false;
+    }
+}
+
+size_t Engine::output_size(int i, int f) const {
+    const SimHost& h = sims_[i];
+    const int T = std::min(t_, h.nt);
+    if (!present(h, f, T)) return 0;
+    switch (f) {
+        case KW_FIELD_P: case KW_FIELD_UX: case KW_FIELD_UY: case KW_FIELD_UZ:
+            return (size_t)h.npts * T;
+        case KW_FIELD_P_FINAL: case KW_FIELD_UX_FINAL: case KW_FIELD_UY_FINAL: case KW_FIELD_UZ_FINAL:
+            return (size_t)h.N;
+        default:
+            return (size_t)h.npts;
+    }
+}
+
+const float* Engine::device_field(int i, int f, size_t* count) const {
+    const SimHost& h = sims_[i];
+    *count = (size_t)h.N;
+    if (f == KW_FIELD_P_FINAL) return h.dev.p;
+    if (f >= KW_FIELD_UX_FINAL && f <= KW_FIELD_UZ_FINAL && f - KW_FIELD_UX_FINAL < h.dim) return h.dev.u[f - KW_FIELD_UX_FINAL];
+    *count = 0;
+    return nullptr;
+}
+
+void Engine::get_output(int i, int f, float* dst, size_t count) {
+    const SimHost& h = sims_[i];
+    const int T = std::min(t_, h.nt);
+    const size_t n = output_size(i, f);
+    if (n == 0) throw err(KW_ERR_INVALID, "output field not recorded for this simulation");
+    if (count != n) throw err(KW_ERR_INVALID, "output buffer size mismatch");
+    const SensorDev& sn = h.dev.sensor;
+    const size_t np = (size_t)h.npts;
+    auto d2h = [&](const float* src, float* d, size_t cnt) {
+        check(cudaMemcpyAsync(d, src, cnt * sizeof(float), cudaMemcpyDeviceToHost, st()), "output copy");
+    };
+    auto series = [&](const float* dev) {   // [T][np] on the device -> [np][T] row-major
+        std::vector<float> tmp((size_t)T * np);
+        d2h(dev, tmp.data(), tmp.size());
+        check(cudaStreamSynchronize(st()), "sync");
+        for (size_t q = 0; q < np; ++q)
+            for (int t = 0; t < T; ++t) dst[q * T + t] = tmp[(size_t)t * np + q];
+    };
+    auto rms = [&](const float* ss) {
+        std::vector<float> tmp(np);
+        d2h(ss, tmp.data(), np);
+        check(cudaStreamSynchronize(st()), "sync");
+        for (size_t q = 0; q < np; ++q) dst[q] = std::sqrt(tmp[q] / (float)T);
+    };
+    switch (f) {
+        case KW_FIELD_P: series(sn.p_series); return;
+        case KW_FIELD_P_MAX: d2h(sn.p_max, dst, np); break;
+        case KW_FIELD_P_MIN: d2h(sn.p_min, dst, np); break;
+        case KW_FIELD_P_RMS: rms(sn.p_ss); return;
+        case KW_FIELD_P_FINAL: d2h(h.dev.p, dst, (size_t)h.N); break;
+        case KW_FIELD_UX: case KW_FIELD_UY: case KW_FIELD_UZ: series(sn.u_series[f - KW_FIELD_UX]); return;
+        case KW_FIELD_UX_MAX: case KW_FIELD_UY_MAX: case KW_FIELD_UZ_MAX: d2h(sn.u_max[f - KW_FIELD_UX_MAX], dst, np); break;
+        case KW_FIELD_UX_RMS: case KW_FIELD_UY_RMS: case KW_FIELD_UZ_RMS: rms(sn.u_ss[f - KW_FIELD_UX_RMS]); return;
+        case KW_FIELD_UX_FINAL: case KW_FIELD_UY_FINAL: case KW_FIELD_UZ_FINAL:
+            d2h(h.dev.u[f - KW_FIELD_UX_FINAL], dst, (size_t)h.N);
+            break;
+        case KW_FIELD_IX_AVG: case KW_FIELD_IY_AVG: case KW_FIELD_IZ_AVG: {
+            // intensityAvg (REC:113-124) with the half-sample shift kernel h[m] in FP64
+            const int a = f - KW_FIELD_IX_AVG;
+            if ((size_t)T * sizeof(float) > 200 * 1024) throw err(KW_ERR_UNSUPPORTED, "iAvg needs nt <= 51200");
+            std::vector<double> hk(T, 0.0);
+            const int half = T / 2;
+            for (int m = 0; m < T; ++m) {
+                double acc = 0;
+                for (int k = 0; k < T; ++k) {
+                    const int kk = k <= half ? k : k - T;
+                    const double th = 2.0 * M_PI * (double)kk / (double)T * 0.5;
+                    acc += std::cos(th + 2.0 * M_PI * (double)k * (double)m / (double)T);
+                }
+                hk[m] = acc / (double)T;
+            }
+            std::vector<float> hf = to_f32(hk);
+            float* dh = (float*)dalloc(hf.size() * sizeof(float));
+            check(cudaMemcpyAsync(dh, hf.data(), hf.size() * sizeof(float), cudaMemcpyHostToDevice, st()), "upload");
+            float* out = (float*)dalloc(np * sizeof(float));
+            launch_intensity(st(), sn.p_series, sn.u_series[a], T, (int)np, dh, out);
+            check(cudaGetLastError(), "intensity");
+            d2h(out, dst, np);
+            break;
+        }
+        default: throw err(KW_ERR_INVALID, "unknown output field");
+    }
+    check(cudaStreamSynchronize(st()), "output sync");
+}
+
+}  // namespace kw

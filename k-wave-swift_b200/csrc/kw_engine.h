@@ -1,0 +1,158 @@
+// kw_engine.h — host engine: setup (FP64 precompute), step sequencing, recording, outputs.
+#pragma once
+
+#include <map>
+#include <memory>
+#include <string>
+#include <tuple>
+#include <vector>
+
+#include "../../include/kwave_cuda.h"
+#include "kw_common.h"
+#include "kw_kernels.cuh"
+
+namespace kw {
+
+struct Context {
+    int device = 0;
+    cudaStream_t own = nullptr;
+    cudaStream_t stream = nullptr;
+    std::string err;
+    int fail(int code, const std::string& msg) { err = msg; return code; }
+};
+
+// A status-carrying error used inside the engine; converted to kw_status at the ABI.
+struct KwError {
+    int code;
+    std::string msg;
+};
+
+// Host-side record of one simulation.
+struct SimHost {
+    kw_sim_desc d{};               // scalar fields of the descriptor (pointers not retained)
+    int dim = 0, A = 1, B = 1, C = 1, Ch = 1, Cp = 2;
+    int n_ref[3] = {1, 1, 1};      // nx, ny, nz
+    double d_ref[3] = {1, 1, 1};
+    long long N = 0, Ns = 0;
+    int nt = 0;
+    double cref = 0;
+    bool record_p = false, record_u = false, record_ufinal = false;
+    bool p_series = false, u_series = false, p_agg = false, u_agg = false;
+    int npts = 0;
+    float* p0s = nullptr;          // smoothed initial pressure (device) or null
+    SimDev dev{};
+};
+
+class Engine {
+public:
+    explicit Engine(Context* ctx) : ctx_(ctx) {}
+    ~Engine();
+    void create(const kw_sim_desc* descs, int count);
+    void reset();
+    void step(int nsteps);
+    void run(const kw_callbacks* cb);
+    int synchronize();             // returns KW_OK or KW_ERR_NONFINITE
+    int t() const { return t_; }
+    int count() const { return (int)sims_.size(); }
+    const SimHost& sim(int i) const { return sims_[i]; }
+    size_t output_size(int i, int field) const;
+    void get_output(int i, int field, float* dst, size_t count);
+    const float* device_field(int i, int field, size_t* count) const;
+    struct KernelTiming {
+        std::string name;
+        double ms;
+        double bytes;
+    };
+    // Run `reps` time steps launch by launch with CUDA events around each launch; returns the mean
+    // device time and the algorithmic HBM bytes of every launch of one step, in launch order.
+    std::vector<KernelTiming> profile_step(int reps);
+
+private:
+    struct Map {
+        BlockWork* d = nullptr;
+        int n = 0;
+    };
+    struct SpecJob {
+        int in_field = FS_P;
+        int nin = 1;
+        int fanout = 0;
+        int nout = 1;
+        OpSpec op[kMaxComp]{};
+        int spec_in = 0, spec_out = 0;
+        int epi = EPI_STORE;
+        int out_field = FS_TMP;
+        int coupled = 0;
+        int gate = GATE_NONE;
+        int comp_mask = 7;        // which components take part (per-comp jobs)
+        const char* name = "job";
+    };
+    struct ProfRec {
+        std::string name;
+        double bytes;
+        cudaEvent_t a, b;
+    };
+    template <class F>
+    void timed(const std::string& name, double bytes, F&& f) {
+        if (!prof_) { f(); return; }
+        ProfRec r{name, bytes, nullptr, nullptr};
+        cudaEventCreate(&r.a);
+        cudaEventCreate(&r.b);
+        cudaEventRecord(r.a, st());
+        f();
+        cudaEventRecord(r.b, st());
+        prof_->push_back(r);
+    }
+    bool host_gate(const SimHost& h, int gate, int comp) const;
+    double epi_bytes(const SimHost& h, int epi, int ncomp) const;
+
+    void* dalloc(size_t bytes);
+    template <class T>
+    T* upload(const std::vector<T>& v) {
+        if (v.empty()) return nullptr;
+        T* p = (T*)dalloc(v.size() * sizeof(T));
+        check(cudaMemcpyAsync(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, st()), "upload");
+        return p;
+    }
+    void check(cudaError_t e, const char* what);
+    cudaStream_t st() const { return ctx_->stream; }
+
+    void setup_sim(int s, const kw_sim_desc& d);
+    void build_plan(FFTPlanDev& pl, int n);
+    void smooth_field(int s, float* field);
+    const Map& map_rows(int rpc, int ncomp, int sim_only);
+    const Map& map_cols(int axis, int tw, int ncomp, int sim_only);
+    const Map& map_elems(int sim_only);
+    void issue_job(const SpecJob& job, int sim_only);
+    void issue_step(bool first);
+    void capture_graph();
+    void finalize_outputs();
+
+    Context* ctx_;
+    std::vector<SimHost> sims_;
+    std::vector<void*> allocs_;
+    SimDev* d_sims_ = nullptr;
+    int* d_t_ = nullptr;
+    int* d_flag_ = nullptr;
+    const float** d_p0s_ = nullptr;
+    unsigned int* d_red_ = nullptr;
+    int t_ = 0;
+    int dim_ = 0;
+    int max_psrc_ = 0, max_usrc_ = 0, max_pts_ = 0;
+    bool any_p_direct_ = false, any_p_add_ = false, any_u_direct_ = false, any_u_add_ = false;
+    bool any_abs_ = false, any_p0_ = false, any_recu_ = false, any_recp_ = false;
+    int max_A_ = 1, max_B_ = 1, max_M_ = 1;
+    std::map<std::tuple<int, int, int, int, int>, Map> maps_;
+    cudaGraph_t graph_ = nullptr;
+    cudaGraphExec_t graph_exec_ = nullptr;
+    cudaStream_t graph_stream_ = nullptr;
+    std::vector<ProfRec>* prof_ = nullptr;
+    bool finalized_ = false;
+    int finalized_t_ = -1;
+    // finalised aggregate outputs per sim (device)
+    struct Outs {
+        float* iavg[kMaxComp] = {nullptr, nullptr, nullptr};
+    };
+    std::vector<Outs> outs_;
+};
+
+}  // namespace kw

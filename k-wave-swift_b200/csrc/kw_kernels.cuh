@@ -1,0 +1,76 @@
+// kw_kernels.cuh — launch-side descriptions of the sm_100a kernels (host and device).
+#pragma once
+
+#include "kw_common.h"
+
+namespace kw {
+
+// Which real field a pass reads or writes.
+enum FieldSel {
+    FS_P = 0, FS_U, FS_RHO, FS_RHO_SUM, FS_DIV, FS_SRCBUF, FS_TMP,
+    FS_WORK   // power-law absorption inputs: component 0 = rho0 div u, component 1 = rho_sum
+};
+
+// A launch may be gated on a source being active at the current step.
+enum Gate { GATE_NONE = 0, GATE_PSRC, GATE_USRC, GATE_P0, GATE_ABS, GATE_RECU };
+
+enum ColMode { COL_FWD = 0, COL_INV, COL_FWD_OP_INV };
+
+struct RowR2CJob {
+    int in_field;          // FieldSel (component = BlockWork.comp)
+    int spec_out;          // component c -> spec[spec_out + c]
+    int apply_op;          // 1D: the row transform is the last forward pass
+    OpSpec op[kMaxComp];
+    int rows_per_cta;
+    int gate;
+};
+
+struct ColJob {
+    int layout_axis;       // 0 = A, 1 = B
+    int mode;              // ColMode
+    int spec_in;           // component c (or fan-out input) spec index
+    int spec_out;
+    int nout;              // outputs written by one CTA (fan-out) or 1
+    int fanout;
+    OpSpec op[kMaxComp];
+    int tw_cols;
+    int gate;
+};
+
+struct RowC2RJob {
+    int spec_in;           // output o reads spec[spec_in + o]
+    int ncomp;             // outputs handled by one CTA
+    int epi;               // Epilogue
+    int out_field;         // FieldSel for EPI_STORE
+    int rows_per_cta;
+    int gate;
+};
+
+struct Launch;  // host-side
+
+// Host entry points (kw_kernels.cu)
+void init_kernel_attributes();
+void launch_row_r2c(cudaStream_t st, const SimDev* d_sims, const int* d_t, const BlockWork* map, int nblocks,
+                    const RowR2CJob& job, size_t smem);
+void launch_col(cudaStream_t st, const SimDev* d_sims, const int* d_t, const BlockWork* map, int nblocks,
+                const ColJob& job, size_t smem);
+void launch_row_c2r(cudaStream_t st, const SimDev* d_sims, const int* d_t, const BlockWork* map, int nblocks,
+                    const RowC2RJob& job, size_t smem);
+
+// small kernels: one block row per simulation (map entries with tile = block index in sim)
+void launch_init_p0(cudaStream_t st, const SimDev* d_sims, const int* d_t, const BlockWork* map, int nblocks,
+                    const float* const* d_p0s);
+void launch_src_u(cudaStream_t st, const SimDev* d_sims, const int* d_t, int nsims, int max_src, int scatter_only);
+void launch_src_p(cudaStream_t st, const SimDev* d_sims, const int* d_t, int nsims, int max_src, int scatter_only);
+void launch_sample(cudaStream_t st, const SimDev* d_sims, const int* d_t, int nsims, int max_pts, int which,
+                   int comp);
+void launch_tick(cudaStream_t st, int* d_t);
+void launch_check_finite(cudaStream_t st, const SimDev* d_sims, const int* d_t, const BlockWork* map, int nblocks);
+
+// setup helpers on one field (single simulation)
+void launch_absmax(cudaStream_t st, const float* x, long long n, unsigned int* d_out_bits);
+void launch_scale(cudaStream_t st, float* x, long long n, const unsigned int* d_num_bits, const unsigned int* d_den_bits);
+void launch_intensity(cudaStream_t st, const float* p_series, const float* u_series, int nt_used, int npts,
+                      const float* h, float* out);
+
+}  // namespace kw

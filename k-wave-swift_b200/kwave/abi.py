@@ -99,6 +99,10 @@ class kw_callbacks(C.Structure):
     ]
 
 
+class kw_kernel_timing(C.Structure):
+    _fields_ = [("name", C.c_char * 48), ("ms", C.c_double), ("bytes", C.c_double)]
+
+
 # Every symbol include/kwave_cuda.h declares, with its ctypes signature.
 P = C.c_void_p
 SIGNATURES = {
@@ -120,6 +124,7 @@ SIGNATURES = {
     "kw_sim_get_output": (C.c_int, [P, C.c_int, C.POINTER(C.c_float), C.c_size_t]),
     "kw_sim_device_field": (C.c_int, [P, C.c_int, C.POINTER(C.POINTER(C.c_float)), C.POINTER(C.c_size_t)]),
     "kw_sim_destroy": (None, [P]),
+    "kw_sim_profile_step": (C.c_int, [P, C.c_int, C.POINTER(kw_kernel_timing), C.c_int, C.POINTER(C.c_int)]),
     "kw_batch_create": (C.c_int, [P, C.POINTER(kw_sim_desc), C.c_int, C.POINTER(P)]),
     "kw_batch_run": (C.c_int, [P, C.POINTER(kw_callbacks)]),
     "kw_batch_reset": (C.c_int, [P]),

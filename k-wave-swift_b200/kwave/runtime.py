@@ -150,6 +150,13 @@ class Simulation:
             setattr(o, name, self.output(name))
         return o
 
+    def profile_step(self, reps: int = 3) -> list[dict]:
+        """Per-launch mean device time (ms) and algorithmic bytes of one time step."""
+        buf = (abi.kw_kernel_timing * 256)()
+        n = C.c_int()
+        _check(self.lib, self.ctx.h, self.lib.kw_sim_profile_step(self.h, int(reps), buf, 256, C.byref(n)))
+        return [{"name": buf[i].name.decode(), "ms": buf[i].ms, "bytes": buf[i].bytes} for i in range(n.value)]
+
     def close(self) -> None:
         if self.h:
             self.lib.kw_sim_destroy(self.h)

@@ -325,8 +325,8 @@ def cases():
     m = np.zeros(n, np.float32)
     m[16] = 1
     s = np.zeros(n, np.float32)
-    s[40] = 1
-    s[50] = 1
+    s[24] = 1
+    s[30] = 1
     c = (1500 + 100 * rng.random(n)).astype(np.float32)
     cs["1d_source_hetero"] = dict(
         dim=1, shape=[n], spacing=[dx], dt=dt, nt=60, pml_size=8, c0=c, rho0=np.float32(1000),

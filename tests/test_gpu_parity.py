@@ -1,0 +1,176 @@
+"""GPU parity: the CUDA library (through its C ABI) against the FP64 oracle / golden fixtures.
+
+Tolerances (FP32 device arithmetic vs FP64 oracle): relative L2 <= 1e-4 on pressure time series
+and final fields; relative L2 <= 1e-3 on aggregates derived from sampled series and intensity.
+Sensor counts and row ordering must match exactly.
+"""
+import numpy as np
+import pytest
+
+import oracle
+from cases import GOLDEN_CASES, builder_from_case, load_golden, rel_l2, rel_max
+from kwave import (DescBuilder, KWaveGrid, KWaveMedium, KWaveSensor, KWaveSource, RecordField,
+                   SimulationOptions, SourceMode, makeBall, makeCartCircle, makeCircle, makeDisc,
+                   toneBurst)
+from kwave.runtime import Context
+
+pytestmark = pytest.mark.gpu
+
+TIGHT = {"p", "pFinal", "ux", "uy", "uz", "uxFinal", "uyFinal", "uzFinal"}
+
+
+def run_gpu(builder):
+    ctx = Context.default()
+    sim = ctx.create_sim(builder)
+    try:
+        sim.run()
+        return {k: v for k, v in vars(sim.outputs()).items()}
+    finally:
+        sim.close()
+
+
+def compare(out, ref, tight=1e-4, loose=1e-3):
+    for k, v in ref.items():
+        if v is None:
+            continue
+        assert out.get(k) is not None, f"missing output {k}"
+        assert out[k].shape == v.shape, (k, out[k].shape, v.shape)
+        e = rel_l2(out[k], v)
+        tol = tight if k in TIGHT else loose
+        assert e < tol, f"{k}: rel L2 {e:.3e} >= {tol}"
+    for k, v in out.items():
+        if v is not None:
+            assert ref.get(k) is not None, f"unexpected output {k}"
+
+
+@pytest.mark.parametrize("name", GOLDEN_CASES)
+def test_golden_case(name):
+    case, ref = load_golden(name)
+    compare(run_gpu(builder_from_case(case)), ref)
+
+
+def c1_builder(nt=None):
+    n = 128
+    g = KWaveGrid(n, 1e-4, n, 1e-4)
+    g.makeTime(1500.0, cfl=0.3, tEnd=4e-6)
+    if nt is not None:
+        g.setTime(nt, g.dt)
+    src = KWaveSource(p0=makeDisc(n, n, radius=5) * 1.0)
+    sen = KWaveSensor(mask=makeCircle(n, n, radius=40), record=RecordField.p | RecordField.pFinal | RecordField.pMax)
+    return DescBuilder(g, KWaveMedium(1500.0, 1000.0), src, sen, SimulationOptions(pmlSize=20, smoothP0=True))
+
+
+def test_c1_2d_ivp_vs_oracle():
+    b = c1_builder()
+    assert b.grid.nt == 201
+    ref, _ = oracle.run(b)
+    out = run_gpu(b)
+    assert out["p"].shape == (224, 201)
+    compare(out, ref)
+
+
+def test_3d_hetero_nonlinear_absorbing_source_vs_oracle():
+    rng = np.random.default_rng(7)
+    n = 40
+    dx = 1e-4
+    c = np.full((n, n, n), 1500, np.float32)
+    rho = np.full((n, n, n), 1000, np.float32)
+    for _ in range(3):
+        r = rng.integers(3, 7)
+        cx, cy, cz = rng.integers(10, 30, size=3)
+        m = makeBall(n, n, n, cx, cy, cz, r) > 0
+        c[m] = rng.uniform(1400, 1650)
+        rho[m] = rng.uniform(900, 1100)
+    g = KWaveGrid(n, dx, n, dx, n, dx)
+    g.makeTime(float(c.max()), cfl=0.3)
+    g.setTime(60, g.dt)
+    pm = np.zeros((n, n, n), np.float32)
+    pm[14:26, 14:26, 8] = 1
+    sig = (toneBurst(1 / g.dt, 1e6, 3) * 1e6).astype(np.float32)
+    sm = np.zeros((n, n, n), np.float32)
+    sm[:, :, 20] = 1
+    med = KWaveMedium(c, rho, alphaCoeff=0.75, alphaPower=1.5, alphaMode=1, bOnA=6.0)
+    b = DescBuilder(g, med, KWaveSource(pMask=pm, p=sig, pMode=SourceMode.additive),
+                    KWaveSensor(mask=sm, record=RecordField.p | RecordField.pMax), SimulationOptions(pmlSize=8))
+    ref, _ = oracle.run(b)
+    compare(run_gpu(b), ref)
+
+
+def crefl(a, axis):
+    return np.roll(np.flip(a, axis=axis), 1, axis=axis)
+
+
+def test_gpu_2d_disc_symmetric():
+    # SolverTests.swift:78-103 on the device
+    n = 64
+    g = KWaveGrid(n, 1e-4, n, 1e-4)
+    g.makeTime(1500.0, cfl=0.3, tEnd=3e-7)
+    b = DescBuilder(g, KWaveMedium(1500.0, 1000.0), KWaveSource(p0=makeDisc(n, n, radius=5)), KWaveSensor())
+    pf = run_gpu(b)["pFinal"]
+    m = np.max(np.abs(pf))
+    assert m > 0 and np.max(np.abs(pf - crefl(pf, 0))) / m < 1e-3 and np.max(np.abs(pf - crefl(pf, 1))) / m < 1e-3
+
+
+def test_gpu_3d_ivp_matches_oracle():
+    # GPUSmokeTests.swift:77-89 shape: 24^3 ball r=3, tEnd 3e-7
+    n = 24
+    g = KWaveGrid(n, 1e-4, n, 1e-4, n, 1e-4)
+    g.makeTime(1500.0, cfl=0.3, tEnd=3e-7)
+    b = DescBuilder(g, KWaveMedium(1500.0, 1000.0), KWaveSource(p0=makeBall(n, n, n, radius=3)), KWaveSensor())
+    ref, _ = oracle.run(b)
+    compare(run_gpu(b), ref)
+
+
+def test_odd_sizes_and_generic_radix():
+    # odd contiguous axis (R2C without the packed path) and a prime-factor length (generic radix)
+    g = KWaveGrid(34, 1e-4, 27, 1e-4)
+    g.setTime(30, 2e-8)
+    b = DescBuilder(g, KWaveMedium(1500.0, 1000.0), KWaveSource(p0=makeDisc(34, 27, radius=3)),
+                    KWaveSensor(mask=makeCircle(34, 27, radius=8), record=RecordField.p), SimulationOptions(pmlSize=5))
+    ref, _ = oracle.run(b)
+    compare(run_gpu(b), ref)
+    g = KWaveGrid(22, 1e-4, 26, 1e-4, 21, 1e-4)
+    g.setTime(20, 2e-8)
+    b = DescBuilder(g, KWaveMedium(1500.0, 1000.0), KWaveSource(p0=makeBall(22, 26, 21, radius=3)), KWaveSensor(),
+                    SimulationOptions(pmlSize=4))
+    ref, _ = oracle.run(b)
+    compare(run_gpu(b), ref)
+
+
+def test_batch_equals_individual_runs():
+    rng = np.random.default_rng(3)
+    builders = []
+    for n in (48, 64, 40):
+        g = KWaveGrid(n, 1e-4, n, 1e-4)
+        g.makeTime(1500.0, cfl=0.3)
+        g.setTime(int(rng.integers(30, 60)), g.dt)
+        sm = makeCartCircle(0.3 * n * 1e-4, 16)
+        pm = np.zeros((n, n), np.float32)
+        pm[10, 5:9] = 1
+        src = KWaveSource(pMask=pm, p=toneBurst(1 / g.dt, 2e6, 2).astype(np.float32))
+        builders.append(DescBuilder(g, KWaveMedium(1500.0, 1000.0), src, KWaveSensor(mask=sm, record=RecordField.p)))
+    ctx = Context.default()
+    singles = [run_gpu(b) for b in builders]
+    batch = ctx.create_batch(builders)
+    try:
+        batch.run()
+        for i, b in enumerate(builders):
+            p = batch.output(i, "p", b.grid.nt, 16)
+            assert np.array_equal(p, singles[i]["p"]), i
+            assert np.array_equal(batch.output(i, "pFinal", b.grid.nt, 16), singles[i]["pFinal"]), i
+    finally:
+        batch.close()
+
+
+def test_kspace_first_order_api_progress_and_monitor():
+    from kwave import kspaceFirstOrder
+    n = 32
+    g = KWaveGrid(n, 1e-4, n, 1e-4)
+    g.setTime(12, 2e-8)
+    steps, mons = [], []
+    opts = SimulationOptions(pmlSize=6, progress=lambda t, nt: steps.append((t, nt)),
+                             fieldMonitor=lambda t, p: mons.append((t, p.shape)), fieldMonitorInterval=5)
+    out = kspaceFirstOrder(g, KWaveMedium(1500.0, 1000.0), KWaveSource(p0=makeDisc(n, n, radius=3)), KWaveSensor(), opts)
+    assert out.pFinal.shape == (n, n)
+    assert steps == [(t, 12) for t in range(12)]
+    assert [m[0] for m in mons] == [0, 5, 10] and all(m[1] == (n, n) for m in mons)
