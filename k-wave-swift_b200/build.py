@@ -44,18 +44,20 @@ def _newest_header() -> float:
     return max((os.path.getmtime(h) for h in hs), default=0.0)
 
 
-def build(verbose_ptxas: bool = False, force: bool = False) -> str:
-    os.makedirs(OUT, exist_ok=True)
+def build(verbose_ptxas: bool = False, force: bool = False, out_dir: str = OUT, defines: tuple = ()) -> str:
+    """Compile every source and link the library into out_dir (defines: extra -D flags)."""
+    os.makedirs(out_dir, exist_ok=True)
+    lib = os.path.join(out_dir, "libkwave_cuda.so")
     nvcc = _nvcc()
     srcs = sorted(glob.glob(os.path.join(CSRC, "*.cu")) + glob.glob(os.path.join(CSRC, "*.cpp")))
     hdr = _newest_header()
     jobs = []
     objs = []
     for s in srcs:
-        obj = os.path.join(OUT, os.path.basename(s) + ".o")
+        obj = os.path.join(out_dir, os.path.basename(s) + ".o")
         objs.append(obj)
         if force or not os.path.exists(obj) or os.path.getmtime(obj) < max(os.path.getmtime(s), hdr):
-            cmd = [nvcc, *_host_compiler(), *ARCH, *COMMON, "-c", s, "-o", obj]
+            cmd = [nvcc, *_host_compiler(), *ARCH, *COMMON, *[f"-D{d}" for d in defines], "-c", s, "-o", obj]
             if s.endswith(".cpp"):
                 cmd[cmd.index("-c"):cmd.index("-c")] = ["-x", "cu"]
             if verbose_ptxas and s.endswith(".cu"):
@@ -73,18 +75,20 @@ def build(verbose_ptxas: bool = False, force: bool = False) -> str:
                 raise RuntimeError("nvcc failed: " + " ".join(cmd[-3:]))
             if verbose_ptxas:
                 sys.stderr.write(r.stderr)
-    if jobs or not os.path.exists(LIB):
-        link = [nvcc, *_host_compiler(), *ARCH, "-shared", "-cudart", "static", "-o", LIB, *objs]
+    if jobs or not os.path.exists(lib):
+        link = [nvcc, *_host_compiler(), *ARCH, "-shared", "-cudart", "static", "-o", lib, *objs]
         r = subprocess.run(link, capture_output=True, text=True)
         if r.returncode != 0:
             sys.stderr.write(r.stdout + r.stderr)
             raise RuntimeError("link failed")
-    return LIB
+    return lib
 
 
 if __name__ == "__main__":
     ap = argparse.ArgumentParser()
     ap.add_argument("--verbose-ptxas", action="store_true")
     ap.add_argument("--force", action="store_true")
+    ap.add_argument("--out", default=OUT)
+    ap.add_argument("-D", dest="defines", action="append", default=[])
     a = ap.parse_args()
-    print(build(a.verbose_ptxas, a.force))
+    print(build(a.verbose_ptxas, a.force, a.out, tuple(a.defines)))

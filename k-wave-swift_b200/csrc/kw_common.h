@@ -26,7 +26,32 @@ struct FFTPlanDev {
     const float2* tw;         // exp(-2 pi i r k / (Ns R)), k in [0, Ns), r in [1, R)
     const float2* gen;        // for generic-prime stages: exp(-2 pi i m / R) at tw_off-independent offsets
     int gen_off[kMaxStages];
+    const float2* twn;        // W_n^m = exp(-2 pi i m / n), m < n (compile-time specialised kernels)
 };
+
+// Lines per CTA of the pass kernels, shared by the host (tile maps, shared-memory sizes) and the
+// kernels. Row passes stage L rows of M = C/2 complex values; column passes stage L columns of
+// length N.
+// About 4096 complex values per tile: short lines are batched 32 to a CTA, long ones 2.
+__host__ __device__ constexpr int tile_lines(int n) {
+    return n <= 128 ? 32 : (n <= 256 ? 16 : (n <= 512 ? 8 : (n <= 1024 ? 4 : 2)));
+}
+__host__ __device__ constexpr int row_lines(int M) { return tile_lines(M); }
+__host__ __device__ constexpr int col_lines(int N) { return tile_lines(N); }
+// operator (fwd -> H -> inv) column passes keep an extra work tile and the staged radial table
+__host__ __device__ constexpr int col_lines_op(int N) { return tile_lines(N) > 2 ? tile_lines(N) / 2 : 2; }
+// C2R passes also stage their epilogue inputs, so they take half as many lines
+__host__ __device__ constexpr int c2r_lines(int M) { return tile_lines(M) > 2 ? tile_lines(M) / 2 : 2; }
+
+// Line lengths with compile-time specialised pass kernels (in-place, one shared buffer per tile);
+// every other length runs the runtime-plan kernels (ping-pong, two buffers per tile).
+#define KW_FFT_SIZES(X) X(8) X(12) X(16) X(24) X(32) X(48) X(64) X(96) X(128) X(192) X(256) X(384) \
+    X(512) X(768) X(1024)
+__host__ __device__ constexpr bool has_fixed_kernel(int n) {
+#define KW_IS(m) n == m ||
+    return KW_FFT_SIZES(KW_IS) false;
+#undef KW_IS
+}
 
 // Per-axis operator vectors in FFT order (length n of that axis). Each is already made
 // Hermitian (real part at the Nyquist bin), so Re(ifft(H * fft(x))) == C2R(H * R2C(x)).
@@ -124,7 +149,8 @@ struct SimDev {
     float2* spec[4];
 
     // medium
-    FieldOrScalar c2, dtrho0, rho0, tau, eta, bona;
+    float dt;              // time step (FP32, multiplies rho0 like the reference's dt * rho0)
+    FieldOrScalar c2, rho0, tau, eta, bona;
     FieldOrScalar dtor[kMaxComp];
     int nonlinear;
     int absorb;            // 0 none, 1 Stokes, 2 power law without dispersion, 3 with dispersion

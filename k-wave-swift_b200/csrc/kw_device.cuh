@@ -1,0 +1,71 @@
+// kw_device.cuh — device helpers shared by the pass kernels and the small kernels.
+#pragma once
+
+#include "kw_fft.cuh"
+#include "kw_kernels.cuh"
+
+namespace kw {
+
+// ------------------------------------------------------------------------------------------
+// helpers
+// ------------------------------------------------------------------------------------------
+__device__ __forceinline__ void load_sim(SimDev& dst, const SimDev* __restrict__ src) {
+    static_assert(sizeof(SimDev) % 4 == 0, "SimDev must be word sized");
+    const int* s = reinterpret_cast<const int*>(src);
+    int* d = reinterpret_cast<int*>(&dst);
+    for (int i = threadIdx.x; i < (int)(sizeof(SimDev) / 4); i += blockDim.x) d[i] = __ldg(s + i);
+    __syncthreads();
+}
+
+__device__ __forceinline__ float* field_ptr(const SimDev& S, int sel, int comp) {
+    switch (sel) {
+        case FS_P: return S.p;
+        case FS_U: return S.u[comp];
+        case FS_RHO: return S.rho[comp];
+        case FS_RHO_SUM: return S.rho_sum;
+        case FS_DIV: return S.div_term;
+        case FS_SRCBUF: return S.src_buf[comp];
+        case FS_WORK: return comp == 0 ? S.div_term : S.rho_sum;   // power-law inputs
+        default: return S.tmp[comp];
+    }
+}
+
+__device__ __forceinline__ bool gate_open(const SimDev& S, int gate, int comp, int t) {
+    if (t >= S.nt) return false;
+    if (gate == GATE_PSRC) return S.has_p && t < S.psrc.len;
+    if (gate == GATE_USRC) return S.has_u[comp] && t < S.usrc[comp].len;
+    if (gate == GATE_P0) return S.has_p0 != 0;
+    if (gate == GATE_ABS) return comp == 0 ? S.absorb >= 2 : S.absorb == 3;
+    if (gate == GATE_RECU) return S.sensor.kind != 0 && (S.sensor.record_u_series || S.sensor.record_u_agg);
+    return true;
+}
+
+// wavenumber index along reference axis `ax` for spectrum coordinates (ka, kb, kc)
+__device__ __forceinline__ int axis_index(const SimDev& S, int ax, int ka, int kb, int kc) {
+    const int L = ax + 3 - S.dim;
+    return L == 0 ? ka : (L == 1 ? kb : kc);
+}
+
+__device__ __forceinline__ float2 op_factor(const SimDev& S, const OpSpec& op, int ka, int kb, int kc, long long flat) {
+    float2 f = make_float2(S.inv_n, 0.f);
+    if (op.axis_op != AO_NONE) {
+        const AxisDev& ax = S.ax[op.axis];
+        const int idx = axis_index(S, op.axis, ka, kb, kc);
+        const float2* v = op.axis_op == AO_DPOS ? ax.dpos : (op.axis_op == AO_DNEG ? ax.dneg : ax.colloc);
+        f = cscale(__ldg(v + idx), S.inv_n);
+    }
+    if (op.radial != RT_NONE) f = cscale(f, __ldg(S.radial[op.radial] + flat));
+    return f;
+}
+
+// equation of state at one point when it is pointwise (lossless / Stokes / B/A):
+// p = c0^2 (rho + tau rho0 divU + B/A rho^2 / (2 rho0))   (KSpaceFirstOrder.swift:467-474, 836-845, 897)
+__device__ __forceinline__ float eos_point(const SimDev& S, long long i, float rs, float divterm) {
+    float e = rs;
+    if (S.absorb == 1) e = e + S.tau.at(i) * divterm;
+    if (S.nonlinear) e = e + S.bona.at(i) * (rs * rs) / (2.f * S.rho0.at(i));
+    return S.c2.at(i) * e;
+}
+
+
+}  // namespace kw

@@ -125,201 +125,12 @@ void Engine::build_plan(FFTPlanDev& pl, int n) {
     if (gen.empty()) gen.push_back(make_float2(1.f, 0.f));
     pl.tw = upload(tw);
     pl.gen = upload(gen);
-}
-
-// ------------------------------------------------------------------------------------------
-// block maps
-// ------------------------------------------------------------------------------------------
-const Engine::Map& Engine::map_rows(int rpc, int ncomp, int sim_only) {
-    auto key = std::make_tuple(0, rpc, ncomp, sim_only, 0);
-    auto it = maps_.find(key);
-    if (it != maps_.end()) return it->second;
-    std::vector<BlockWork> v;
-    for (int s = 0; s < count(); ++s) {
-        if (sim_only >= 0 && s != sim_only) continue;
-        const int rows = sims_[s].A * sims_[s].B;
-        const int tiles = (rows + rpc - 1) / rpc;
-        for (int c = 0; c < ncomp; ++c)
-            for (int tI = 0; tI < tiles; ++tI) v.push_back(BlockWork{s, c, tI});
+    std::vector<float2> twn(std::max(n, 1));
+    for (int m2 = 0; m2 < n; ++m2) {
+        const double a = -2.0 * M_PI * (double)m2 / (double)n;
+        twn[m2] = make_float2((float)std::cos(a), (float)std::sin(a));
     }
-    Map m;
-    m.d = upload(v);
-    m.n = (int)v.size();
-    return maps_[key] = m;
-}
-
-const Engine::Map& Engine::map_cols(int axis, int tw, int ncomp, int sim_only) {
-    auto key = std::make_tuple(1 + axis, tw, ncomp, sim_only, 0);
-    auto it = maps_.find(key);
-    if (it != maps_.end()) return it->second;
-    std::vector<BlockWork> v;
-    for (int s = 0; s < count(); ++s) {
-        if (sim_only >= 0 && s != sim_only) continue;
-        const SimHost& h = sims_[s];
-        const int inner = axis == 0 ? h.B * h.Cp : h.Cp;
-        const int outer = axis == 0 ? 1 : h.A;
-        const int tiles = outer * ((inner + tw - 1) / tw);
-        for (int c = 0; c < ncomp; ++c)
-            for (int tI = 0; tI < tiles; ++tI) v.push_back(BlockWork{s, c, tI});
-    }
-    Map m;
-    m.d = upload(v);
-    m.n = (int)v.size();
-    return maps_[key] = m;
-}
-
-const Engine::Map& Engine::map_elems(int sim_only) {
-    auto key = std::make_tuple(9, 0, 0, sim_only, 0);
-    auto it = maps_.find(key);
-    if (it != maps_.end()) return it->second;
-    std::vector<BlockWork> v;
-    for (int s = 0; s < count(); ++s) {
-        if (sim_only >= 0 && s != sim_only) continue;
-        const long long tiles = (sims_[s].N + 255) / 256;
-        for (long long tI = 0; tI < tiles; ++tI) v.push_back(BlockWork{s, 0, (int)tI});
-    }
-    Map m;
-    m.d = upload(v);
-    m.n = (int)v.size();
-    return maps_[key] = m;
-}
-
-// ------------------------------------------------------------------------------------------
-// spectral job: R2C rows -> column passes (operator fused in the last) -> C2R rows + epilogue
-// ------------------------------------------------------------------------------------------
-void Engine::issue_job(const SpecJob& job, int sim_only) {
-    const int comps_in = job.fanout ? 1 : job.nin;
-    const int M = max_M_;
-    // rows per CTA for the forward row pass
-    int rpc = 16;
-    while (rpc > 1 && (size_t)2 * M * (rpc + 1) * sizeof(float2) > kSmemBudget) rpc /= 2;
-    long long total_rows = 0;
-    for (int s = 0; s < count(); ++s)
-        if (sim_only < 0 || s == sim_only) total_rows += (long long)sims_[s].A * sims_[s].B;
-    while (rpc > 1 && total_rows * comps_in / rpc < 2 * 148) rpc /= 2;
-
-    RowR2CJob rj{};
-    rj.in_field = job.in_field;
-    rj.spec_out = job.spec_in;
-    rj.apply_op = dim_ == 1 ? 1 : 0;
-    for (int c = 0; c < kMaxComp; ++c) rj.op[c] = job.op[c];
-    rj.rows_per_cta = rpc;
-    rj.gate = job.gate;
-    // algorithmic bytes per launch (compulsory HBM reads + writes of the open simulations)
-    auto sum_sims = [&](auto per_sim) {
-        double b = 0;
-        for (int s = 0; s < count(); ++s)
-            if ((sim_only < 0 || s == sim_only) && t_ < sims_[s].nt) b += per_sim(sims_[s]);
-        return b;
-    };
-    auto spec_bytes = [](const SimHost& h) { return (double)h.A * h.B * h.Ch * sizeof(float2); };
-    auto open_comps = [&](const SimHost& h, int ncomp) {
-        int n = 0;
-        for (int c = 0; c < ncomp; ++c) n += host_gate(h, job.gate, c) ? 1 : 0;
-        return n;
-    };
-    {
-        const Map& m = map_rows(rpc, comps_in, sim_only);
-        const double bytes = sum_sims([&](const SimHost& h) { return open_comps(h, comps_in) * ((double)h.N * 4 + spec_bytes(h)); });
-        timed(std::string("r2c:") + job.name, bytes, [&] {
-            launch_row_r2c(st(), d_sims_, d_t_, m.d, m.n, rj, (size_t)2 * M * (rpc + 1) * sizeof(float2));
-        });
-    }
-
-    auto col_tw = [&](int n, int bufs, long long lines_total) {
-        int tw = 16;
-        while (tw > 1 && (size_t)bufs * n * tw * sizeof(float2) > kSmemBudget) tw /= 2;
-        while (tw > 2 && lines_total / tw < 2 * 148) tw /= 2;
-        return tw;
-    };
-    auto lines_of = [&](int axis) {
-        long long L = 0;
-        for (int s = 0; s < count(); ++s)
-            if (sim_only < 0 || s == sim_only) {
-                const SimHost& h = sims_[s];
-                L += axis == 0 ? (long long)h.B * h.Cp : (long long)h.A * h.Cp;
-            }
-        return L;
-    };
-
-    int spec_final = job.spec_in;
-    if (dim_ >= 2) {
-        if (dim_ == 3) {
-            ColJob cj{};
-            cj.layout_axis = 1;
-            cj.mode = COL_FWD;
-            cj.spec_in = job.spec_in;
-            cj.tw_cols = col_tw(max_B_, 2, lines_of(1) * comps_in);
-            cj.gate = job.gate;
-            const Map& m = map_cols(1, cj.tw_cols, comps_in, sim_only);
-            const double bytes = sum_sims([&](const SimHost& h) { return open_comps(h, comps_in) * 2 * spec_bytes(h); });
-            timed(std::string("colB_fwd:") + job.name, bytes, [&] {
-                launch_col(st(), d_sims_, d_t_, m.d, m.n, cj, (size_t)2 * max_B_ * cj.tw_cols * sizeof(float2));
-            });
-        }
-        const int last = dim_ == 3 ? 0 : 1;
-        const int nlast = last == 0 ? max_A_ : max_B_;
-        ColJob cj{};
-        cj.layout_axis = last;
-        cj.mode = COL_FWD_OP_INV;
-        cj.spec_in = job.spec_in;
-        cj.spec_out = job.spec_out;
-        cj.nout = job.nout;
-        cj.fanout = job.fanout;
-        for (int c = 0; c < kMaxComp; ++c) cj.op[c] = job.op[c];
-        cj.tw_cols = col_tw(nlast, 3, lines_of(last) * (job.fanout ? 1 : job.nout));
-        cj.gate = job.gate;
-        {
-            const Map& m = map_cols(last, cj.tw_cols, job.fanout ? 1 : job.nout, sim_only);
-            const double bytes = sum_sims([&](const SimHost& h) {
-                const int no = open_comps(h, job.fanout ? 1 : job.nout);
-                if (no == 0) return 0.0;
-                const double tables = job.op[0].radial != RT_NONE ? (double)h.A * h.B * h.Ch * 4 : 0.0;
-                return job.fanout ? spec_bytes(h) * (1 + job.nout) + tables : no * (2 * spec_bytes(h) + tables);
-            });
-            timed(std::string(last == 0 ? "colA_op:" : "colB_op:") + job.name, bytes, [&] {
-                launch_col(st(), d_sims_, d_t_, m.d, m.n, cj, (size_t)3 * nlast * cj.tw_cols * sizeof(float2));
-            });
-        }
-        spec_final = job.spec_out;
-        if (dim_ == 3) {
-            ColJob ci{};
-            ci.layout_axis = 1;
-            ci.mode = COL_INV;
-            ci.spec_in = job.spec_out;
-            ci.tw_cols = col_tw(max_B_, 2, lines_of(1) * job.nout);
-            ci.gate = job.gate;
-            const Map& m = map_cols(1, ci.tw_cols, job.nout, sim_only);
-            const double bytes = sum_sims([&](const SimHost& h) {
-                return (job.fanout ? (open_comps(h, 1) ? job.nout : 0) : open_comps(h, job.nout)) * 2 * spec_bytes(h);
-            });
-            timed(std::string("colB_inv:") + job.name, bytes, [&] {
-                launch_col(st(), d_sims_, d_t_, m.d, m.n, ci, (size_t)2 * max_B_ * ci.tw_cols * sizeof(float2));
-            });
-        }
-    }
-
-    const int ncta = job.coupled ? job.nout : 1;
-    int rpc2 = 16;
-    while (rpc2 > 1 && (size_t)2 * M * (ncta * rpc2 + 1) * sizeof(float2) > kSmemBudget) rpc2 /= 2;
-    while (rpc2 > 1 && total_rows * (job.coupled ? 1 : job.nout) / rpc2 < 2 * 148) rpc2 /= 2;
-    RowC2RJob cj{};
-    cj.spec_in = spec_final;
-    cj.ncomp = ncta;
-    cj.epi = job.epi;
-    cj.out_field = job.out_field;
-    cj.rows_per_cta = rpc2;
-    cj.gate = job.gate;
-    const Map& m = map_rows(rpc2, job.coupled ? 1 : job.nout, sim_only);
-    const double bytes = sum_sims([&](const SimHost& h) {
-        int no = job.coupled ? (open_comps(h, 1) ? job.nout : 0) : open_comps(h, job.nout);
-        if (job.epi == EPI_EOS_ABS && no) no = h.dev.absorb == 3 ? 2 : 1;
-        if (no == 0) return 0.0;
-        return no * spec_bytes(h) + (double)h.N * epi_bytes(h, job.epi, job.coupled ? 1 : no);
-    });
-    timed(std::string("c2r:") + job.name, bytes, [&] {
-        launch_row_c2r(st(), d_sims_, d_t_, m.d, m.n, cj, (size_t)2 * M * (ncta * rpc2 + 1) * sizeof(float2));
-    });
+    pl.twn = upload(twn);
 }
 
 // ------------------------------------------------------------------------------------------
@@ -463,11 +274,29 @@ double Engine::epi_bytes(const SimHost& h, int epi, int ncomp) const {
         case EPI_VEL_INIT: { double b = 0; for (int a = 0; a < ncomp; ++a) b += 4 + m(S.dtor[a]); return b; }
         case EPI_ADD_U: return 8.0 * ncomp;
         case EPI_DEN:
-            return 8.0 * D + 4 + m(S.dtrho0) + ((S.nonlinear || S.absorb >= 1) ? m(S.rho0) : 0) +
+            return 8.0 * D + 4 + m(S.rho0) +
                    (S.absorb >= 1 ? 4 : 0) + (S.eos_pointwise ? eos : 0);
         case EPI_ADD_RHO: return 8.0 * D + 4 + (S.eos_pointwise ? eos + (S.absorb == 1 ? 4 : 0) : 0);
         case EPI_EOS_ABS:
             return 8 + m(S.c2) + m(S.tau) + (S.absorb == 3 ? m(S.eta) : 0) + (S.nonlinear ? m(S.bona) + m(S.rho0) : 0);
+        default: return 0;
+    }
+}
+
+// Number of fields the C2R epilogue `epi` stages per row (an upper bound of the device-side plan:
+// velocity u / dt/rho_sg; density rho_a, rho0, and the pointwise EoS inputs; power-law EoS inputs).
+int Engine::aux_slots(const SimHost& h, int epi) const {
+    const SimDev& S = h.dev;
+    auto m = [](const FieldOrScalar& f) { return f.ptr ? 1 : 0; };
+    switch (epi) {
+        case EPI_VEL: return 2;
+        case EPI_VEL_INIT: return 1;
+        case EPI_ADD_U: return 1;
+        case EPI_DEN:
+        case EPI_ADD_RHO:
+            return h.dim + 1 + (S.eos_pointwise ? m(S.c2) + (S.absorb == 1 ? m(S.tau) + 1 : 0) + (S.nonlinear ? m(S.bona) : 0) : 0);
+        case EPI_EOS_ABS:
+            return 1 + m(S.c2) + m(S.tau) + (S.absorb == 3 ? m(S.eta) : 0) + (S.nonlinear ? m(S.bona) + m(S.rho0) : 0);
         default: return 0;
     }
 }
@@ -567,7 +396,7 @@ void Engine::setup_sim(int s, const kw_sim_desc& d) {
     for (int a = 0; a < h.dim; ++a) {
         if (nref[a] < 1) throw err(KW_ERR_INVALID, "grid size must be positive");
         if (!(dref[a] > 0)) throw err(KW_ERR_INVALID, "grid spacing must be positive");
-        if (nref[a] > 8192) throw err(KW_ERR_UNSUPPORTED, "axis length above 8192");
+        if (nref[a] > 4096) throw err(KW_ERR_UNSUPPORTED, "axis length above 4096");
         h.n_ref[a] = nref[a];
         h.d_ref[a] = dref[a];
     }
@@ -618,7 +447,8 @@ void Engine::setup_sim(int s, const kw_sim_desc& d) {
     }
     max_A_ = std::max(max_A_, h.A);
     max_B_ = std::max(max_B_, h.B);
-    max_M_ = std::max(max_M_, odd ? h.C : h.C / 2);
+    h.M = odd ? h.C : h.C / 2;
+    max_M_ = std::max(max_M_, h.M);
 
     // device fields
     const size_t fb = (size_t)N * sizeof(float);
@@ -762,7 +592,7 @@ void Engine::setup_sim(int s, const kw_sim_desc& d) {
         return r;
     };
     v.c2 = field_or_scalar(c0map, [&](long long i) { return c0_at(i) * c0_at(i); });
-    v.dtrho0 = field_or_scalar(rho0map, [&](long long i) { return dt * rho0_at(i); });
+    v.dt = (float)dt;
     v.rho0 = field_or_scalar(rho0map, [&](long long i) { return rho0_at(i); });
     for (int a = 0; a < h.dim; ++a) {
         // staggerDensity (KSFO:799-806): mean of neighbours, last index replicated

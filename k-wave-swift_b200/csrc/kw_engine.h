@@ -31,6 +31,7 @@ struct KwError {
 struct SimHost {
     kw_sim_desc d{};               // scalar fields of the descriptor (pointers not retained)
     int dim = 0, A = 1, B = 1, C = 1, Ch = 1, Cp = 2;
+    int M = 1;                     // complex length of the row transform (C/2, or C when C is odd)
     int n_ref[3] = {1, 1, 1};      // nx, ny, nz
     double d_ref[3] = {1, 1, 1};
     long long N = 0, Ns = 0;
@@ -104,6 +105,7 @@ private:
     }
     bool host_gate(const SimHost& h, int gate, int comp) const;
     double epi_bytes(const SimHost& h, int epi, int ncomp) const;
+    int aux_slots(const SimHost& h, int epi) const;
 
     void* dalloc(size_t bytes);
     template <class T>
@@ -119,8 +121,8 @@ private:
     void setup_sim(int s, const kw_sim_desc& d);
     void build_plan(FFTPlanDev& pl, int n);
     void smooth_field(int s, float* field);
-    const Map& map_rows(int rpc, int ncomp, int sim_only);
-    const Map& map_cols(int axis, int tw, int ncomp, int sim_only);
+    const Map& map_rows(int lines_per_row, int ncomp, int sim_only, int sclass);
+    const Map& map_cols(int axis, int ncomp, int sim_only, bool op, int sclass);
     const Map& map_elems(int sim_only);
     void issue_job(const SpecJob& job, int sim_only);
     void issue_step(bool first);

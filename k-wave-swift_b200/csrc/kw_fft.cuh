@@ -214,3 +214,97 @@ __device__ float2* fft_lines(float2* a, float2* b, const FFTPlanDev& pl, int nli
 }
 
 }  // namespace kw
+
+// ============================================================================================
+// Compile-time specialised Stockham transform for the common line lengths N = 2^a 3^b 5^c.
+// The radix sequence, the number of lines per CTA (L) and every index are template constants,
+// so a butterfly costs only its loads, twiddles, DFT and stores. One twiddle table per length
+// (W_N^m = exp(-2 pi i m / N), m < N, FP64 rounded to FP32) serves every stage:
+// exp(-2 pi i r k / (Ns R)) = W_N^{r k N / (Ns R)}.
+// ============================================================================================
+namespace kw {
+
+// radix sequence: greedy 16, 8, 4, 2, then 3, 5 (the host plan uses the same rule)
+__host__ __device__ constexpr int radix_at(int n, int k) {
+    const int order[6] = {16, 8, 4, 2, 3, 5};
+    int m = n, idx = 0;
+    for (int oi = 0; oi < 6; ++oi) {
+        const int r = order[oi];
+        while (m % r == 0 && m > 1) {
+            if (idx == k) return r;
+            ++idx;
+            m /= r;
+        }
+    }
+    return 1;
+}
+
+__host__ __device__ constexpr bool fixed_fft_length(int n) {
+    if (n < 2) return false;
+    int m = n;
+    while (m % 2 == 0) m /= 2;
+    while (m % 3 == 0) m /= 3;
+    while (m % 5 == 0) m /= 5;
+    return m == 1;
+}
+
+// One in-place Stockham stage: every thread first gathers, twiddles and transforms all of its
+// butterflies in registers, the block synchronises, then every thread scatters its results into
+// the same buffer. One shared buffer per tile instead of two.
+template <int N, int R, int Ns, int L, int LDI, bool INV>
+__device__ __forceinline__ void tstage_inplace(float2* __restrict__ buf, const float2* __restrict__ twn, int nl) {
+    constexpr int NB = N / R;
+    constexpr int TPL = 256 / L;                 // threads per line
+    constexpr int BPT = (NB + TPL - 1) / TPL;    // butterflies per thread
+    const int l = threadIdx.x % L;
+    const int j0 = threadIdx.x / L;
+    const bool active = l < nl;
+    float2 v[BPT][R];
+#pragma unroll
+    for (int b = 0; b < BPT; ++b) {
+        const int j = j0 + b * TPL;
+        if (active && j < NB) {
+#pragma unroll
+            for (int r = 0; r < R; ++r) v[b][r] = buf[(j + r * NB) * LDI + l];
+            const int k = j % Ns;
+            if (Ns > 1) {
+#pragma unroll
+                for (int r = 1; r < R; ++r) v[b][r] = twiddle<INV>(v[b][r], __ldg(twn + r * k * (N / (Ns * R))));
+            }
+            DFT<R, INV>::run(v[b]);
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int b = 0; b < BPT; ++b) {
+        const int j = j0 + b * TPL;
+        if (active && j < NB) {
+            const int k = j % Ns;
+            const int base = (j - k) * R + k;
+#pragma unroll
+            for (int r = 0; r < R; ++r) buf[(base + r * Ns) * LDI + l] = v[b][r];
+        }
+    }
+    __syncthreads();
+}
+
+template <int N, int S, int Ns, int L, int LDI, bool INV>
+struct TStages {
+    __device__ __forceinline__ static void run(float2* buf, const float2* __restrict__ twn, int nl) {
+        constexpr int R = radix_at(N, S);
+        if constexpr (R > 1) {
+            tstage_inplace<N, R, Ns, L, LDI, INV>(buf, twn, nl);
+            TStages<N, S + 1, Ns * R, L, LDI, INV>::run(buf, twn, nl);
+        }
+    }
+};
+
+// Transform (in place) nl <= L interleaved lines of length N: element i of line l at
+// buf[i * LDI + l]. The caller synchronises before (data staged); the call ends synchronised.
+template <int N, int L, int LDI, bool INV>
+__device__ __forceinline__ float2* fft_tile(float2* buf, float2* /*unused*/, const float2* __restrict__ twn, int nl) {
+    TStages<N, 0, 1, L, LDI, INV>::run(buf, twn, nl);
+    return buf;
+}
+
+}  // namespace kw

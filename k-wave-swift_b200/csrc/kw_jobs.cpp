@@ -1,0 +1,214 @@
+// kw_jobs.cpp — tile maps and the launch sequence of one spectral job:
+//   R2C rows -> column passes (the k-space operator fused into the last) -> C2R rows + epilogue.
+// Each pass is launched once per size class (line length) of the engine's simulations, so every
+// launch runs the kernel instantiation specialised for its line length.
+#include "kw_engine.h"
+
+#include <algorithm>
+#include <set>
+
+namespace kw {
+
+// size class of a row pass / column pass of one simulation (0 = runtime-plan kernels)
+static int row_class(const SimHost& h) { return (h.C % 2 == 0 && has_fixed_kernel(h.M)) ? h.M : 0; }
+static int col_class(const SimHost& h, int axis) {
+    const int n = axis == 0 ? h.A : h.B;
+    return has_fixed_kernel(n) ? n : 0;
+}
+
+// Row-pass tiles of the simulations of size class `sclass`. lines_per_row == 0: R2C tiles of
+// row_lines(M) rows; otherwise C2R tiles of c2r_lines(M) lines, i.e. c2r_lines(M) / lines_per_row
+// rows (a coupled C2R epilogue stages every component of a row in the same CTA).
+const Engine::Map& Engine::map_rows(int lines_per_row, int ncomp, int sim_only, int sclass) {
+    auto key = std::make_tuple(0, lines_per_row, ncomp, sim_only, sclass);
+    auto it = maps_.find(key);
+    if (it != maps_.end()) return it->second;
+    std::vector<BlockWork> v;
+    for (int s = 0; s < count(); ++s) {
+        if ((sim_only >= 0 && s != sim_only) || row_class(sims_[s]) != sclass) continue;
+        const int rows = sims_[s].A * sims_[s].B;
+        const int rpc = lines_per_row == 0 ? row_lines(sims_[s].M)
+                                           : std::max(1, c2r_lines(sims_[s].M) / lines_per_row);
+        const int tiles = (rows + rpc - 1) / rpc;
+        for (int c = 0; c < ncomp; ++c)
+            for (int tI = 0; tI < tiles; ++tI) v.push_back(BlockWork{s, c, tI});
+    }
+    Map m;
+    m.d = upload(v);
+    m.n = (int)v.size();
+    return maps_[key] = m;
+}
+
+// Column-pass tiles: col_lines(n) (col_lines_op(n) for an operator pass) contiguous columns.
+const Engine::Map& Engine::map_cols(int axis, int ncomp, int sim_only, bool op, int sclass) {
+    auto key = std::make_tuple(1 + axis + (op ? 2 : 0), 0, ncomp, sim_only, sclass);
+    auto it = maps_.find(key);
+    if (it != maps_.end()) return it->second;
+    std::vector<BlockWork> v;
+    for (int s = 0; s < count(); ++s) {
+        if ((sim_only >= 0 && s != sim_only) || col_class(sims_[s], axis) != sclass) continue;
+        const SimHost& h = sims_[s];
+        const int n = axis == 0 ? h.A : h.B;
+        const int tw = op ? col_lines_op(n) : col_lines(n);
+        const int inner = axis == 0 ? h.B * h.Cp : h.Cp;
+        const int outer = axis == 0 ? 1 : h.A;
+        const int tiles = outer * ((inner + tw - 1) / tw);
+        for (int c = 0; c < ncomp; ++c)
+            for (int tI = 0; tI < tiles; ++tI) v.push_back(BlockWork{s, c, tI});
+    }
+    Map m;
+    m.d = upload(v);
+    m.n = (int)v.size();
+    return maps_[key] = m;
+}
+
+const Engine::Map& Engine::map_elems(int sim_only) {
+    auto key = std::make_tuple(9, 0, 0, sim_only, 0);
+    auto it = maps_.find(key);
+    if (it != maps_.end()) return it->second;
+    std::vector<BlockWork> v;
+    for (int s = 0; s < count(); ++s) {
+        if (sim_only >= 0 && s != sim_only) continue;
+        const long long tiles = (sims_[s].N + 255) / 256;
+        for (long long tI = 0; tI < tiles; ++tI) v.push_back(BlockWork{s, 0, (int)tI});
+    }
+    Map m;
+    m.d = upload(v);
+    m.n = (int)v.size();
+    return maps_[key] = m;
+}
+
+// Staged tiles are laid out back to back in shared memory and filled with 16-byte cp.async copies,
+// so every tile size is rounded up to a multiple of four float2 (32 bytes).
+static long long round4(long long te) { return (te + 3) & ~3LL; }
+
+void Engine::issue_job(const SpecJob& job, int sim_only) {
+    const int comps_in = job.fanout ? 1 : job.nin;
+    auto in_launch = [&](int s) { return sim_only < 0 || s == sim_only; };
+    auto spec_bytes = [](const SimHost& h) { return (double)h.A * h.B * h.Ch * sizeof(float2); };
+    auto open_comps = [&](const SimHost& h, int ncomp) {
+        int n = 0;
+        for (int c = 0; c < ncomp; ++c) n += host_gate(h, job.gate, c) ? 1 : 0;
+        return n;
+    };
+    // algorithmic bytes of a launch (compulsory HBM reads + writes of its open simulations)
+    auto sum_sims = [&](auto in_class, auto per_sim) {
+        double b = 0;
+        for (int s = 0; s < count(); ++s)
+            if (in_launch(s) && in_class(sims_[s]) && t_ < sims_[s].nt) b += per_sim(sims_[s]);
+        return b;
+    };
+    auto classes = [&](auto cls) {
+        std::set<int> r;
+        for (int s = 0; s < count(); ++s)
+            if (in_launch(s)) r.insert(cls(sims_[s]));
+        return r;
+    };
+
+    // ---- forward row pass (R2C) ----
+    for (int sc : classes(row_class)) {
+        auto in_class = [&](const SimHost& h) { return row_class(h) == sc; };
+        long long te = 0;
+        for (int s = 0; s < count(); ++s)
+            if (in_launch(s) && in_class(sims_[s])) te = std::max(te, (long long)sims_[s].M * (row_lines(sims_[s].M) + 1));
+        RowR2CJob rj{};
+        rj.in_field = job.in_field;
+        rj.spec_out = job.spec_in;
+        rj.apply_op = dim_ == 1 ? 1 : 0;
+        for (int c = 0; c < kMaxComp; ++c) rj.op[c] = job.op[c];
+        rj.gate = job.gate;
+        te = round4(te);
+        rj.tile_elems = te;
+        const Map& m = map_rows(0, comps_in, sim_only, sc);
+        const double bytes = sum_sims(in_class, [&](const SimHost& h) { return open_comps(h, comps_in) * ((double)h.N * 4 + spec_bytes(h)); });
+        const size_t smem = (size_t)(sc ? 2 : 3) * te * sizeof(float2);
+        timed(std::string("r2c:") + job.name, bytes, [&] { launch_row_r2c(st(), d_sims_, d_t_, m.d, m.n, rj, smem, sc); });
+    }
+
+    // ---- column passes ----
+    // shared memory: two staged tiles (+ staged radial tables and an operator work tile) (+ one
+    // ping-pong tile for the runtime plan)
+    auto col_launch = [&](int axis, int mode, const char* label, int ncomp_map, auto bytes_of) {
+        const bool op = mode == COL_FWD_OP_INV;
+        for (int sc : classes([&](const SimHost& h) { return col_class(h, axis); })) {
+            auto in_class = [&](const SimHost& h) { return col_class(h, axis) == sc; };
+            long long te = 0;
+            for (int s = 0; s < count(); ++s)
+                if (in_launch(s) && in_class(sims_[s])) {
+                    const int n = axis == 0 ? sims_[s].A : sims_[s].B;
+                    te = std::max(te, (long long)n * (op ? col_lines_op(n) : col_lines(n)));
+                }
+            te = round4(te);
+            ColJob cj{};
+            cj.layout_axis = axis;
+            cj.mode = mode;
+            cj.spec_in = job.spec_in;
+            cj.spec_out = job.spec_out;
+            cj.nout = job.nout;
+            cj.fanout = job.fanout;
+            for (int c = 0; c < kMaxComp; ++c) cj.op[c] = job.op[c];
+            cj.gate = job.gate;
+            cj.tile_elems = te;
+            if (mode == COL_INV) cj.spec_in = job.spec_out, cj.fanout = 0;
+            const Map& m = map_cols(axis, ncomp_map, sim_only, op, sc);
+            const double bytes = sum_sims(in_class, bytes_of);
+            const long long tiles = sc ? (op ? 4 : 2) : (op ? 5 : 3);
+            const size_t smem = (size_t)(tiles * te * sizeof(float2));
+            timed(std::string(label) + job.name, bytes, [&] { launch_col(st(), d_sims_, d_t_, m.d, m.n, cj, smem, sc); });
+        }
+    };
+    int spec_final = job.spec_in;
+    if (dim_ >= 2) {
+        if (dim_ == 3)
+            col_launch(1, COL_FWD, "colB_fwd:", comps_in,
+                       [&](const SimHost& h) { return open_comps(h, comps_in) * 2 * spec_bytes(h); });
+        const int last = dim_ == 3 ? 0 : 1;
+        col_launch(last, COL_FWD_OP_INV, last == 0 ? "colA_op:" : "colB_op:", job.fanout ? 1 : job.nout,
+                   [&](const SimHost& h) {
+                       const int no = open_comps(h, job.fanout ? 1 : job.nout);
+                       if (no == 0) return 0.0;
+                       const double tables = job.op[0].radial != RT_NONE ? (double)h.A * h.B * h.Ch * 4 : 0.0;
+                       return job.fanout ? spec_bytes(h) * (1 + job.nout) + tables : no * (2 * spec_bytes(h) + tables);
+                   });
+        spec_final = job.spec_out;
+        if (dim_ == 3)
+            col_launch(1, COL_INV, "colB_inv:", job.nout, [&](const SimHost& h) {
+                return (job.fanout ? (open_comps(h, 1) ? job.nout : 0) : open_comps(h, job.nout)) * 2 * spec_bytes(h);
+            });
+    }
+
+    // ---- inverse row pass (C2R) + epilogue ----
+    const int ncta = job.coupled ? job.nout : 1;
+    for (int sc : classes(row_class)) {
+        auto in_class = [&](const SimHost& h) { return row_class(h) == sc; };
+        long long te = 0, aux_floats = 0;
+        for (int s = 0; s < count(); ++s)
+            if (in_launch(s) && in_class(sims_[s])) {
+                const SimHost& h = sims_[s];
+                te = std::max(te, (long long)(h.C % 2 ? h.M : h.M + 1) * (c2r_lines(h.M) + 1));
+                const int rpc = std::max(1, c2r_lines(h.M) / ncta);
+                aux_floats = std::max(aux_floats, (long long)aux_slots(h, job.epi) * rpc * h.C);
+            }
+        te = round4(te);
+        aux_floats = (aux_floats + 3) & ~3LL;
+        RowC2RJob cj{};
+        cj.spec_in = spec_final;
+        cj.ncomp = ncta;
+        cj.epi = job.epi;
+        cj.out_field = job.out_field;
+        cj.gate = job.gate;
+        cj.generic = sc ? 0 : 1;
+        cj.tile_elems = te;
+        const Map& m = map_rows(ncta, job.coupled ? 1 : job.nout, sim_only, sc);
+        const double bytes = sum_sims(in_class, [&](const SimHost& h) {
+            int no = job.coupled ? (open_comps(h, 1) ? job.nout : 0) : open_comps(h, job.nout);
+            if (job.epi == EPI_EOS_ABS && no) no = h.dev.absorb == 3 ? 2 : 1;
+            if (no == 0) return 0.0;
+            return no * spec_bytes(h) + (double)h.N * epi_bytes(h, job.epi, job.coupled ? 1 : no);
+        });
+        const size_t smem = (size_t)(sc ? 2 : 3) * te * sizeof(float2) + (size_t)aux_floats * sizeof(float);
+        timed(std::string("c2r:") + job.name, bytes, [&] { launch_row_c2r(st(), d_sims_, d_t_, m.d, m.n, cj, smem, sc); });
+    }
+}
+
+}  // namespace kw

@@ -21,8 +21,8 @@ struct RowR2CJob {
     int spec_out;          // component c -> spec[spec_out + c]
     int apply_op;          // 1D: the row transform is the last forward pass
     OpSpec op[kMaxComp];
-    int rows_per_cta;
     int gate;
+    long long tile_elems;  // float2 elements of one staged tile (max over the launch's simulations)
 };
 
 struct ColJob {
@@ -33,8 +33,8 @@ struct ColJob {
     int nout;              // outputs written by one CTA (fan-out) or 1
     int fanout;
     OpSpec op[kMaxComp];
-    int tw_cols;
     int gate;
+    long long tile_elems;
 };
 
 struct RowC2RJob {
@@ -42,20 +42,25 @@ struct RowC2RJob {
     int ncomp;             // outputs handled by one CTA
     int epi;               // Epilogue
     int out_field;         // FieldSel for EPI_STORE
-    int rows_per_cta;
     int gate;
+    int generic;           // some simulation needs the runtime-plan (ping-pong) path
+    long long tile_elems;
 };
 
-struct Launch;  // host-side
-
-// Host entry points (kw_kernels.cu)
+// Host entry points (kw_passes.cu, kw_small.cu). The pass launchers take the tile map and its
+// length; the grid is persistent.
+// `size_class` is the line length of the launch's simulations when it has a specialised kernel
+// (has_fixed_kernel), else 0 (runtime plan).
 void init_kernel_attributes();
-void launch_row_r2c(cudaStream_t st, const SimDev* d_sims, const int* d_t, const BlockWork* map, int nblocks,
-                    const RowR2CJob& job, size_t smem);
-void launch_col(cudaStream_t st, const SimDev* d_sims, const int* d_t, const BlockWork* map, int nblocks,
-                const ColJob& job, size_t smem);
-void launch_row_c2r(cudaStream_t st, const SimDev* d_sims, const int* d_t, const BlockWork* map, int nblocks,
-                    const RowC2RJob& job, size_t smem);
+void init_r2c_attributes(int optin);
+void init_col_attributes(int optin);
+void init_c2r_attributes(int optin);
+void launch_row_r2c(cudaStream_t st, const SimDev* d_sims, const int* d_t, const BlockWork* map, int nmap,
+                    const RowR2CJob& job, size_t smem, int size_class);
+void launch_col(cudaStream_t st, const SimDev* d_sims, const int* d_t, const BlockWork* map, int nmap,
+                const ColJob& job, size_t smem, int size_class);
+void launch_row_c2r(cudaStream_t st, const SimDev* d_sims, const int* d_t, const BlockWork* map, int nmap,
+                    const RowC2RJob& job, size_t smem, int size_class);
 
 // small kernels: one block row per simulation (map entries with tile = block index in sim)
 void launch_init_p0(cudaStream_t st, const SimDev* d_sims, const int* d_t, const BlockWork* map, int nblocks,

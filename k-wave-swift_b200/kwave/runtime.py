@@ -16,7 +16,7 @@ from . import abi
 from .api import DescBuilder, KWaveError, SimulationOutput, output_shape
 
 _PKG_DIR = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-LIB_PATH = os.path.join(_PKG_DIR, "_build", "libkwave_cuda.so")
+LIB_PATH = os.environ.get("KWAVE_CUDA_LIB") or os.path.join(_PKG_DIR, "_build", "libkwave_cuda.so")
 
 _lib: Optional[C.CDLL] = None
 _lock = threading.Lock()
