@@ -269,6 +269,16 @@ typedef struct kw_kernel_timing {
 } kw_kernel_timing;
 KW_API int kw_sim_profile_step(kw_sim* sim, int reps, kw_kernel_timing* out, int max_entries, int* n_entries);
 
+/* ---- standalone spectral operator ------------------------------------------------------------
+ * Staggered spectral derivative of one device field along `axis` (0 = x):
+ *   out = Re F^-1( i k exp(shift * i k d/2) F(in) ),  shift = +1 or -1,
+ * the reference's derivativeOperator (Solver/KSpaceFirstOrder.swift:764-769) applied on its own
+ * (the time step also multiplies by kappa). d_in and d_out are device pointers to nx*ny*nz
+ * row-major floats (unused sizes 1) and may not overlap. Runs on the context's stream and returns
+ * after the result is written. The half-spectrum scratch is allocated and freed inside the call. */
+KW_API int kw_spectral_derivative(kw_context* ctx, int dim, int nx, int ny, int nz, double dx, double dy, double dz,
+                                  int axis, int shift, const float* d_in, float* d_out);
+
 /* ---- many independent simulations in one launch sequence -----------------------------------
  * Simulations of the same dimensionality (any sizes, any nt) step together: every kernel of a
  * step covers the tiles of all simulations that are still running, so small grids fill the GPU.

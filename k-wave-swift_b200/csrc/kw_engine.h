@@ -67,6 +67,9 @@ public:
     // Run `reps` time steps launch by launch with CUDA events around each launch; returns the mean
     // device time and the algorithmic HBM bytes of every launch of one step, in launch order.
     std::vector<KernelTiming> profile_step(int reps);
+    // Standalone staggered spectral derivative of a device field (kw_derivative.cpp).
+    void create_derivative(int dim, const int* n, const double* d, int axis, int shift, const float* in, float* out);
+    void run_derivative();
 
 private:
     struct Map {
@@ -148,6 +151,7 @@ private:
     cudaGraphExec_t graph_exec_ = nullptr;
     cudaStream_t graph_stream_ = nullptr;
     std::vector<ProfRec>* prof_ = nullptr;
+    int deriv_axis_ = 0, deriv_shift_ = 1;
     bool finalized_ = false;
     int finalized_t_ = -1;
     // finalised aggregate outputs per sim (device)
