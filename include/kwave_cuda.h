@@ -279,6 +279,21 @@ KW_API int kw_sim_profile_step(kw_sim* sim, int reps, kw_kernel_timing* out, int
 KW_API int kw_spectral_derivative(kw_context* ctx, int dim, int nx, int ny, int nz, double dx, double dy, double dz,
                                   int axis, int shift, const float* d_in, float* d_out);
 
+/* Allocation-free variant of kw_spectral_derivative (no counterpart in the reference). Same
+ * arguments and result; it never calls cudaMalloc or cudaFree. It is for callers that cannot
+ * allocate device memory: a host whose own memory manager already holds the device memory, or a
+ * loop that cannot take cudaMalloc/cudaFree's device-wide synchronisation. Its scratch (the
+ * half-spectrum, twiddle tables, operator vector, tile maps) lives in one file-scope device array
+ * of KW_NOALLOC_SCRATCH_BYTES that every GPU loading this library keeps until the process exits;
+ * problems that need more are rejected with KW_ERR_INVALID and a message naming the limit (about
+ * 2 M half-spectrum values: e.g. 2D 1024^2 or 3D 128^3 fit). The first call on a device looks up
+ * the array's device address (cudaGetSymbolAddress); make that first call before any stream
+ * capture. All calls share the array and it keeps the last call's contents (each call clears what
+ * it uses); calls whose work overlaps on the GPU race on it. */
+#define KW_NOALLOC_SCRATCH_BYTES (16u * 1024u * 1024u)
+KW_API int kw_spectral_derivative_noalloc(kw_context* ctx, int dim, int nx, int ny, int nz, double dx, double dy,
+                                          double dz, int axis, int shift, const float* d_in, float* d_out);
+
 /* ---- many independent simulations in one launch sequence -----------------------------------
  * Simulations of the same dimensionality (any sizes, any nt) step together: every kernel of a
  * step covers the tiles of all simulations that are still running, so small grids fill the GPU.

@@ -209,6 +209,20 @@ int kw_spectral_derivative(kw_context* ctx, int dim, int nx, int ny, int nz, dou
     });
 }
 
+int kw_spectral_derivative_noalloc(kw_context* ctx, int dim, int nx, int ny, int nz, double dx, double dy, double dz,
+                                   int axis, int shift, const float* d_in, float* d_out) {
+    if (!ctx) return KW_ERR_INVALID;
+    return guarded(ctx, [&]() {
+        const int n[3] = {nx, ny, nz};
+        const double d[3] = {dx, dy, dz};
+        kw::Engine eng(&ctx->c);
+        eng.set_arena(kw::noalloc_scratch(ctx->c.device), KW_NOALLOC_SCRATCH_BYTES);
+        eng.create_derivative(dim, n, d, axis, shift, d_in, d_out);
+        eng.run_derivative();
+        return KW_OK;
+    });
+}
+
 int kw_batch_create(kw_context* ctx, const kw_sim_desc* descs, int count, kw_batch** out) {
     if (!ctx || !descs || count <= 0 || !out) return KW_ERR_INVALID;
     *out = nullptr;

@@ -24,6 +24,17 @@ void Engine::check(cudaError_t e, const char* what) {
 
 void* Engine::dalloc(size_t bytes) {
     if (bytes == 0) bytes = 16;
+    if (arena_) {
+        // allocation-free mode: carve 256-byte aligned pieces out of the caller-provided region
+        const size_t off = (arena_used_ + 255) & ~(size_t)255;
+        if (off + bytes > arena_size_)
+            throw err(KW_ERR_INVALID, "problem needs more than the " + std::to_string(arena_size_) +
+                                          "-byte allocation-free scratch (at least " + std::to_string(off + bytes) +
+                                          " bytes); use the allocating entry point");
+        arena_used_ = off + bytes;
+        check(cudaMemsetAsync(arena_ + off, 0, bytes, st()), "memset");
+        return arena_ + off;
+    }
     void* p = nullptr;
     cudaError_t e = cudaMalloc(&p, bytes);
     if (e != cudaSuccess) {

@@ -27,6 +27,9 @@ struct KwError {
     std::string msg;
 };
 
+// Device address of the allocation-free scratch array on `device` (kw_noalloc.cu).
+void* noalloc_scratch(int device);
+
 // Host-side record of one simulation.
 struct SimHost {
     kw_sim_desc d{};               // scalar fields of the descriptor (pointers not retained)
@@ -70,6 +73,12 @@ public:
     // Standalone staggered spectral derivative of a device field (kw_derivative.cpp).
     void create_derivative(int dim, const int* n, const double* d, int axis, int shift, const float* in, float* out);
     void run_derivative();
+    // Take every device buffer from [base, base + bytes) instead of cudaMalloc (call before create).
+    void set_arena(void* base, size_t bytes) {
+        arena_ = static_cast<char*>(base);
+        arena_size_ = bytes;
+        arena_used_ = 0;
+    }
 
 private:
     struct Map {
@@ -152,6 +161,8 @@ private:
     cudaStream_t graph_stream_ = nullptr;
     std::vector<ProfRec>* prof_ = nullptr;
     int deriv_axis_ = 0, deriv_shift_ = 1;
+    char* arena_ = nullptr;
+    size_t arena_size_ = 0, arena_used_ = 0;
     bool finalized_ = false;
     int finalized_t_ = -1;
     // finalised aggregate outputs per sim (device)

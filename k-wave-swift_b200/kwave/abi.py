@@ -127,6 +127,8 @@ SIGNATURES = {
     "kw_sim_profile_step": (C.c_int, [P, C.c_int, C.POINTER(kw_kernel_timing), C.c_int, C.POINTER(C.c_int)]),
     "kw_spectral_derivative": (C.c_int, [P, C.c_int, C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double,
                                          C.c_int, C.c_int, P, P]),
+    "kw_spectral_derivative_noalloc": (C.c_int, [P, C.c_int, C.c_int, C.c_int, C.c_int, C.c_double, C.c_double,
+                                                 C.c_double, C.c_int, C.c_int, P, P]),
     "kw_batch_create": (C.c_int, [P, C.POINTER(kw_sim_desc), C.c_int, C.POINTER(P)]),
     "kw_batch_run": (C.c_int, [P, C.POINTER(kw_callbacks)]),
     "kw_batch_reset": (C.c_int, [P]),
