@@ -43,6 +43,14 @@ __host__ __device__ constexpr int col_lines_op(int N) { return tile_lines(N) > 2
 // C2R passes also stage their epilogue inputs, so they take half as many lines
 __host__ __device__ constexpr int c2r_lines(int M) { return tile_lines(M) > 2 ? tile_lines(M) / 2 : 2; }
 
+// Register-resident two-stage column transforms (kw_pass_colr.cu): N = R1 * R2 with R1 >= R2,
+// R2 threads per line, each holding R1 values; 256 threads, so 256 / R2 lines per CTA.
+__host__ __device__ constexpr bool has_two_stage_col(int n) {
+    return n == 16 || n == 32 || n == 64 || n == 128 || n == 256;
+}
+__host__ __device__ constexpr int colr_r1(int n) { return n >= 128 ? 16 : (n >= 32 ? 8 : 4); }
+__host__ __device__ constexpr int colr_lines(int n) { return 256 / (n / colr_r1(n)); }
+
 // Line lengths with compile-time specialised pass kernels (in-place, one shared buffer per tile);
 // every other length runs the runtime-plan kernels (ping-pong, two buffers per tile).
 #define KW_FFT_SIZES(X) X(8) X(12) X(16) X(24) X(32) X(48) X(64) X(96) X(128) X(192) X(256) X(384) \

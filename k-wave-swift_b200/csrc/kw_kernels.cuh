@@ -54,13 +54,25 @@ struct RowC2RJob {
 void init_kernel_attributes();
 void init_r2c_attributes(int optin);
 void init_col_attributes(int optin);
+void init_colr_attributes(int optin);
 void init_c2r_attributes(int optin);
 void launch_row_r2c(cudaStream_t st, const SimDev* d_sims, const int* d_t, const BlockWork* map, int nmap,
                     const RowR2CJob& job, size_t smem, int size_class);
 void launch_col(cudaStream_t st, const SimDev* d_sims, const int* d_t, const BlockWork* map, int nmap,
                 const ColJob& job, size_t smem, int size_class);
+// register-resident column pass for has_two_stage_col(n) lengths; one CTA per map entry, whose
+// tile indexes colr_lines(n) consecutive (outer, column) lines
+void launch_colr(cudaStream_t st, const SimDev* d_sims, const int* d_t, const BlockWork* map, int nmap,
+                 const ColJob& job, int n);
 void launch_row_c2r(cudaStream_t st, const SimDev* d_sims, const int* d_t, const BlockWork* map, int nmap,
                     const RowC2RJob& job, size_t smem, int size_class);
+// register-resident row passes for even rows with has_two_stage_col(M) half lengths; one CTA per
+// map entry, whose tile indexes colr_lines(M) consecutive rows
+void init_rowr_attributes(int optin);
+void launch_rowr_r2c(cudaStream_t st, const SimDev* d_sims, const int* d_t, const BlockWork* map, int nmap,
+                     const RowR2CJob& job, int M);
+void launch_rowr_c2r(cudaStream_t st, const SimDev* d_sims, const int* d_t, const BlockWork* map, int nmap,
+                     const RowC2RJob& job, int M);
 
 // small kernels: one block row per simulation (map entries with tile = block index in sim)
 void launch_init_p0(cudaStream_t st, const SimDev* d_sims, const int* d_t, const BlockWork* map, int nblocks,

@@ -1,0 +1,347 @@
+// kw_pass_rowr.cu — register-resident row passes for even rows whose half length M = C / 2 has
+// a two-stage transform (has_two_stage_col: M = 16 ... 256, i.e. C = 32 ... 512).
+//
+// A 256-thread CTA owns 256 / T consecutive rows; the T threads of a row are consecutive lanes, so
+// every load and store walks the row contiguously. Thread t of a row holds the packed values
+// z[t + T m] = x[2n] + i x[2n+1] (n = t + T m) of the M-point transform in registers
+// (kw_fft_reg.cuh), i.e. the real samples 2n and 2n+1, which is also the pair its epilogue updates.
+//
+//   R2C   load the real row as float2 -> forward transform -> Hermitian split into X[0 .. M]
+//   C2R   load X[k] and X[M-k] -> Hermitian merge -> inverse transform -> fused physics update
+//
+// Coupled epilogues (density: one spectrum per axis; power law: two) transform their components
+// one after the other in the same CTA and park the finished ones in shared memory (each thread its
+// own slots). The epilogue reads its field inputs for a few pairs at a time before any store, so
+// their latencies overlap.
+#include "kw_fft_reg.cuh"
+#include "kw_pass_common.cuh"
+
+namespace kw {
+
+// ---------------------------------------------------------------------------------------------
+// R2C: X[k] = (Z[k] + conj Z[M-k]) / 2 - i W_C^k (Z[k] - conj Z[M-k]) / 2, k = 0 .. M
+// ---------------------------------------------------------------------------------------------
+template <int M>
+__global__ void __launch_bounds__(256) k_rowr_r2c(const SimDev* __restrict__ sims, const int* __restrict__ d_t,
+                                                  const BlockWork* __restrict__ map, int nmap, RowR2CJob job) {
+    using P = TwoStage<M>;
+    using Lay = RowLayout<M>;
+    constexpr int R1 = P::R1, T = P::T, TW = P::LINES;
+    __shared__ float2 sh[Lay::SLOTS];
+    if (blockIdx.x >= nmap) return;
+    const BlockWork bw = map[blockIdx.x];
+    const SimDev& S = sims[bw.sim];
+    if (!gate_open(S, job.gate, bw.comp, *d_t)) return;
+    const int t = threadIdx.x % T, l = threadIdx.x / T;
+    const int row = bw.tile * TW + l;
+    const bool ok = row < S.A * S.B;
+    const float2* in = reinterpret_cast<const float2*>(field_ptr(S, job.in_field, bw.comp) + (long long)row * (2 * M));
+    float2 v[R1];
+#pragma unroll
+    for (int r = 0; r < R1; ++r) v[r] = ok ? in[t + T * r] : make_float2(0.f, 0.f);
+    FftReg<M, false, Lay>::run(v, sh, t, l, S.plan_row.twn);
+    // the split needs Z[M - k], held by another thread of the row
+#pragma unroll
+    for (int m = 0; m < R1; ++m) sh[Lay::at(t + T * m, l)] = v[m];
+    __syncthreads();
+    if (!ok) return;
+    float2* out = S.spec[job.spec_out + bw.comp] + (long long)row * S.Cp;
+    const float2* __restrict__ tw = S.row_tw;
+    auto bin = [&](int k, float2 zk, float2 zm) {
+        const float2 E = make_float2(0.5f * (zk.x + zm.x), 0.5f * (zk.y - zm.y));
+        const float2 D = make_float2(0.5f * (zk.x - zm.x), 0.5f * (zk.y + zm.y));
+        const float2 O = make_float2(D.y, -D.x);   // -i D
+        return cadd(E, cmul(O, __ldg(tw + k)));
+    };
+#pragma unroll
+    for (int m = 0; m < R1; ++m) {
+        const int k = t + T * m;
+        out[k] = bin(k, v[m], sh[Lay::at(k == 0 ? 0 : M - k, l)]);
+    }
+    if (t == 0) out[M] = bin(M, v[0], v[0]);
+}
+
+// ---------------------------------------------------------------------------------------------
+// C2R + epilogue
+// ---------------------------------------------------------------------------------------------
+__device__ __forceinline__ float2 ld_state(const float* p, long long e) { return *reinterpret_cast<const float2*>(p + e); }
+__device__ __forceinline__ void st_state(float* p, long long e, float2 v) { *reinterpret_cast<float2*>(p + e) = v; }
+__device__ __forceinline__ float2 ld_medium(const FieldOrScalar& f, long long e) {
+    return f.ptr ? __ldg(reinterpret_cast<const float2*>(f.ptr + e)) : make_float2(f.s, f.s);
+}
+__device__ __forceinline__ float& half(float2& v, int h) { return h ? v.y : v.x; }
+
+template <int M, int EPI>
+__global__ void __launch_bounds__(256) k_rowr_c2r(const SimDev* __restrict__ sims, const int* __restrict__ d_t,
+                                                  const BlockWork* __restrict__ map, int nmap, RowC2RJob job) {
+    using P = TwoStage<M>;
+    using Lay = RowLayout<M>;
+    constexpr int R1 = P::R1, T = P::T, TW = P::LINES;
+    // pairs whose inputs are loaded together (the density update reads the most fields)
+    constexpr int MB = (EPI == EPI_DEN || R1 < 4) ? 2 : 4;
+    __shared__ float2 sh[Lay::SLOTS];
+    extern __shared__ __align__(16) float2 parked[];   // coupled epilogues: [ncomp - 1][R1][256]
+    if (blockIdx.x >= nmap) return;
+    const BlockWork bw = map[blockIdx.x];
+    const SimDev& S = sims[bw.sim];
+    if (!gate_open(S, job.gate, bw.comp, *d_t)) return;
+    const int t = threadIdx.x % T, l = threadIdx.x / T;
+    const int row = bw.tile * TW + l;
+    const bool ok = row < S.A * S.B;
+    const int comp0 = job.ncomp == 1 ? bw.comp : 0;
+    const int ncomp = (EPI == EPI_EOS_ABS && S.absorb != 3) ? 1 : job.ncomp;
+    const float2* __restrict__ tw = S.row_tw;
+
+    // Z'[k] = (X[k] + conj X[M-k]) + i exp(+2 pi i k / C) (X[k] - conj X[M-k]), X[0] and X[M] real
+    float2 v[R1];
+    for (int cc = 0; cc < ncomp; ++cc) {
+        const float2* X = S.spec[job.spec_in + comp0 + cc] + (long long)row * S.Cp;
+#pragma unroll
+        for (int m = 0; m < R1; ++m) {
+            const int k = t + T * m;
+            float2 a0 = make_float2(0.f, 0.f), b0 = a0;
+            if (ok) { a0 = X[k]; b0 = X[M - k]; }
+            if (k == 0) { a0.y = 0.f; b0.y = 0.f; }
+            const float2 s = make_float2(a0.x + b0.x, a0.y - b0.y);
+            const float2 dd = make_float2(a0.x - b0.x, a0.y + b0.y);
+            const float2 e = cmulc(dd, __ldg(tw + k));
+            v[m] = make_float2(s.x - e.y, s.y + e.x);
+        }
+        FftReg<M, true, Lay>::run(v, sh, t, l, S.plan_row.twn);
+        if (cc + 1 < ncomp) {
+#pragma unroll
+            for (int m = 0; m < R1; ++m) parked[(cc * R1 + m) * 256 + threadIdx.x] = v[m];
+        }
+    }
+    if (!ok) return;
+
+    const long long rbase = (long long)row * (2 * M);
+    const int ca = row / S.B, cb = row - ca * S.B;
+    const int D = S.dim;
+    // samples 2n, 2n+1 of component cc (pair index m)
+    auto dpair = [&](int cc, int m) { return cc + 1 < ncomp ? parked[(cc * R1 + m) * 256 + threadIdx.x] : v[m]; };
+    // per-axis profiles: constant along the row except for the row's own axis (a = D - 1), which
+    // is read at samples 2n, 2n+1
+    auto row_const = [&](const float* vec, int a) { return __ldg(vec + (a + 3 - D == 0 ? ca : cb)); };
+    auto row_pair = [&](const float* vec, int n) { return __ldg(reinterpret_cast<const float2*>(vec) + n); };
+
+#pragma unroll
+    for (int m0 = 0; m0 < R1; m0 += MB) {
+        if constexpr (EPI == EPI_STORE) {
+            for (int cc = 0; cc < ncomp; ++cc) {
+                float* out = field_ptr(S, job.out_field, comp0 + cc);
+#pragma unroll
+                for (int b = 0; b < MB; ++b) st_state(out, rbase + 2 * (t + T * (m0 + b)), dpair(cc, m0 + b));
+            }
+        } else if constexpr (EPI == EPI_VEL || EPI == EPI_VEL_INIT || EPI == EPI_ADD_U) {
+            // u = pml_sg (pml_sg u - dt/rho_sg d)   (KSpaceFirstOrder.swift:453-454)
+            // u = (dt/rho_sg / 2) d                 (KSpaceFirstOrder.swift:519-520)
+            // u = u + d                             (additive velocity source)
+            const int a = comp0;
+            float* u = S.u[a];
+            const bool along_row = a == D - 1;
+            const float sgc = (EPI == EPI_VEL && !along_row) ? row_const(S.ax[a].pml_sg, a) : 0.f;
+            float2 uu[MB], dr[MB], sg[MB];
+#pragma unroll
+            for (int b = 0; b < MB; ++b) {
+                const int n = t + T * (m0 + b);
+                const long long e = rbase + 2 * n;
+                if (EPI != EPI_VEL_INIT) uu[b] = ld_state(u, e);
+                if (EPI != EPI_ADD_U) dr[b] = ld_medium(S.dtor[a], e);
+                if (EPI == EPI_VEL) sg[b] = along_row ? row_pair(S.ax[a].pml_sg, n) : make_float2(sgc, sgc);
+            }
+#pragma unroll
+            for (int b = 0; b < MB; ++b) {
+                const float2 d = v[m0 + b];
+                float2 o;
+#pragma unroll
+                for (int h = 0; h < 2; ++h) {
+                    const float dh = h ? d.y : d.x;
+                    if (EPI == EPI_VEL) half(o, h) = half(sg[b], h) * (half(sg[b], h) * half(uu[b], h) - half(dr[b], h) * dh);
+                    else if (EPI == EPI_VEL_INIT) half(o, h) = (half(dr[b], h) / 2.f) * dh;
+                    else half(o, h) = half(uu[b], h) + dh;
+                }
+                st_state(u, rbase + 2 * (t + T * (m0 + b)), o);
+            }
+        } else if constexpr (EPI == EPI_DEN || EPI == EPI_ADD_RHO) {
+            // density (KSpaceFirstOrder.swift:457-465) or additive pressure source
+            // (KSpaceFirstOrder.swift:167-172), then the pointwise equation of state when there is one
+            float2 ro[kMaxComp][MB], pmr[MB], r0[MB], c2[MB], tau[MB], bona[MB], eta[MB];
+            float pmc[kMaxComp - 1];
+#pragma unroll
+            for (int a = 0; a < kMaxComp - 1; ++a)
+                if (EPI == EPI_DEN && a < D - 1) pmc[a] = row_const(S.ax[a].pml, a);
+            const bool need_r0 = EPI == EPI_DEN || S.nonlinear;
+#pragma unroll
+            for (int b = 0; b < MB; ++b) {
+                const int n = t + T * (m0 + b);
+                const long long e = rbase + 2 * n;
+#pragma unroll
+                for (int a = 0; a < kMaxComp; ++a)
+                    if (a < D) ro[a][b] = ld_state(S.rho[a], e);
+                if (EPI == EPI_DEN) pmr[b] = row_pair(S.ax[D - 1].pml, n);
+                if (need_r0) r0[b] = ld_medium(S.rho0, e);
+                if (S.eos_pointwise) {
+                    c2[b] = ld_medium(S.c2, e);
+                    if (S.absorb == 1) tau[b] = ld_medium(S.tau, e);
+                    if (S.nonlinear) bona[b] = ld_medium(S.bona, e);
+                    if (EPI == EPI_ADD_RHO && S.absorb == 1) eta[b] = ld_state(S.div_term, e);
+                }
+            }
+#pragma unroll
+            for (int b = 0; b < MB; ++b) {
+                const int m = m0 + b;
+                const long long e = rbase + 2 * (t + T * m);
+                float2 rn[kMaxComp], rs2, dv2, p2;
+#pragma unroll
+                for (int h = 0; h < 2; ++h) {
+                    const float r0v = need_r0 ? half(r0[b], h) : 0.f;
+                    float rs = 0.f, divterm = 0.f;
+                    if (EPI == EPI_DEN) {
+                        float nl = 1.f;
+                        if (S.nonlinear) {
+                            float rp = 0.f;
+#pragma unroll
+                            for (int a = 0; a < kMaxComp; ++a)
+                                if (a < D) rp = a == 0 ? half(ro[a][b], h) : rp + half(ro[a][b], h);
+                            nl = (2.f * rp + r0v) / r0v;
+                        }
+                        const float dtr = S.dt * r0v;   // dt * rho0 in FP32 (KSpaceFirstOrder.swift:400)
+                        float dv = 0.f;
+#pragma unroll
+                        for (int a = 0; a < kMaxComp; ++a)
+                            if (a < D) {
+                                float2 dp = dpair(a, m);
+                                const float d = half(dp, h);
+                                const float pmv = a == D - 1 ? half(pmr[b], h) : pmc[a < kMaxComp - 1 ? a : 0];
+                                const float mass = S.nonlinear ? dtr * d * nl : dtr * d;
+                                const float r = pmv * (pmv * half(ro[a][b], h) - mass);
+                                half(rn[a], h) = r;
+                                rs = a == 0 ? r : rs + r;
+                                dv = a == 0 ? d : dv + d;
+                            }
+                        if (S.absorb >= 1) divterm = r0v * dv;
+                    } else {
+                        const float d = h ? v[m].y : v[m].x;
+#pragma unroll
+                        for (int a = 0; a < kMaxComp; ++a)
+                            if (a < D) {
+                                const float r = half(ro[a][b], h) + d * S.ax[a].inv_d;
+                                half(rn[a], h) = r;
+                                rs = a == 0 ? r : rs + r;
+                            }
+                        if (S.absorb == 1) divterm = half(eta[b], h);
+                    }
+                    half(rs2, h) = rs;
+                    half(dv2, h) = divterm;
+                    if (S.eos_pointwise) {   // p = c0^2 (rho + tau divterm + B/A rho^2 / (2 rho0))
+                        float ee = rs;
+                        if (S.absorb == 1) ee = ee + half(tau[b], h) * divterm;
+                        if (S.nonlinear) ee = ee + half(bona[b], h) * (rs * rs) / (2.f * r0v);
+                        half(p2, h) = half(c2[b], h) * ee;
+                    }
+                }
+#pragma unroll
+                for (int a = 0; a < kMaxComp; ++a)
+                    if (a < D) st_state(S.rho[a], e, rn[a]);
+                st_state(S.rho_sum, e, rs2);
+                if (EPI == EPI_DEN && S.absorb >= 1) st_state(S.div_term, e, dv2);
+                if (S.eos_pointwise) st_state(S.p, e, p2);
+            }
+        } else if constexpr (EPI == EPI_EOS_ABS) {
+            // power-law absorption / dispersion (KSpaceFirstOrder.swift:836-845)
+            float2 rs[MB], c2[MB], tau[MB], eta[MB], bona[MB], r0[MB];
+#pragma unroll
+            for (int b = 0; b < MB; ++b) {
+                const long long e = rbase + 2 * (t + T * (m0 + b));
+                rs[b] = ld_state(S.rho_sum, e);
+                c2[b] = ld_medium(S.c2, e);
+                tau[b] = ld_medium(S.tau, e);
+                if (S.absorb == 3) eta[b] = ld_medium(S.eta, e);
+                if (S.nonlinear) { bona[b] = ld_medium(S.bona, e); r0[b] = ld_medium(S.rho0, e); }
+            }
+#pragma unroll
+            for (int b = 0; b < MB; ++b) {
+                const int m = m0 + b;
+                const float2 d0 = dpair(0, m);
+                float2 d1 = make_float2(0.f, 0.f);
+                if (S.absorb == 3) d1 = dpair(1, m);
+                float2 p2;
+#pragma unroll
+                for (int h = 0; h < 2; ++h) {
+                    const float r = half(rs[b], h);
+                    float term = half(tau[b], h) * (h ? d0.y : d0.x);
+                    if (S.absorb == 3) term = term - half(eta[b], h) * (h ? d1.y : d1.x);
+                    float ee = r + term;
+                    if (S.nonlinear) ee = ee + half(bona[b], h) * (r * r) / (2.f * half(r0[b], h));
+                    half(p2, h) = half(c2[b], h) * ee;
+                }
+                st_state(S.p, rbase + 2 * (t + T * m), p2);
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
+// host side
+// ---------------------------------------------------------------------------------------------
+template <int M>
+static size_t rowr_park_bytes(int ncomp) { return (size_t)(ncomp > 1 ? ncomp - 1 : 0) * colr_r1(M) * 256 * sizeof(float2); }
+
+template <int EPI>
+static void set_rowr_attrs(int optin) {
+    set_max_smem((const void*)k_rowr_c2r<16, EPI>, optin);
+    set_max_smem((const void*)k_rowr_c2r<32, EPI>, optin);
+    set_max_smem((const void*)k_rowr_c2r<64, EPI>, optin);
+    set_max_smem((const void*)k_rowr_c2r<128, EPI>, optin);
+    set_max_smem((const void*)k_rowr_c2r<256, EPI>, optin);
+}
+
+void init_rowr_attributes(int optin) {
+    set_rowr_attrs<EPI_DEN>(optin);
+    set_rowr_attrs<EPI_EOS_ABS>(optin);
+}
+
+void launch_rowr_r2c(cudaStream_t st, const SimDev* d_sims, const int* d_t, const BlockWork* map, int nmap,
+                     const RowR2CJob& job, int M) {
+    if (nmap <= 0) return;
+    switch (M) {
+        case 16: k_rowr_r2c<16><<<nmap, 256, 0, st>>>(d_sims, d_t, map, nmap, job); break;
+        case 32: k_rowr_r2c<32><<<nmap, 256, 0, st>>>(d_sims, d_t, map, nmap, job); break;
+        case 64: k_rowr_r2c<64><<<nmap, 256, 0, st>>>(d_sims, d_t, map, nmap, job); break;
+        case 128: k_rowr_r2c<128><<<nmap, 256, 0, st>>>(d_sims, d_t, map, nmap, job); break;
+        case 256: k_rowr_r2c<256><<<nmap, 256, 0, st>>>(d_sims, d_t, map, nmap, job); break;
+        default: break;
+    }
+}
+
+template <int M>
+static void launch_c2r_m(cudaStream_t st, const SimDev* d_sims, const int* d_t, const BlockWork* map, int nmap,
+                         const RowC2RJob& job) {
+    const size_t smem = rowr_park_bytes<M>(job.ncomp);
+    switch (job.epi) {
+        case EPI_STORE: k_rowr_c2r<M, EPI_STORE><<<nmap, 256, smem, st>>>(d_sims, d_t, map, nmap, job); break;
+        case EPI_VEL: k_rowr_c2r<M, EPI_VEL><<<nmap, 256, smem, st>>>(d_sims, d_t, map, nmap, job); break;
+        case EPI_VEL_INIT: k_rowr_c2r<M, EPI_VEL_INIT><<<nmap, 256, smem, st>>>(d_sims, d_t, map, nmap, job); break;
+        case EPI_ADD_U: k_rowr_c2r<M, EPI_ADD_U><<<nmap, 256, smem, st>>>(d_sims, d_t, map, nmap, job); break;
+        case EPI_DEN: k_rowr_c2r<M, EPI_DEN><<<nmap, 256, smem, st>>>(d_sims, d_t, map, nmap, job); break;
+        case EPI_ADD_RHO: k_rowr_c2r<M, EPI_ADD_RHO><<<nmap, 256, smem, st>>>(d_sims, d_t, map, nmap, job); break;
+        case EPI_EOS_ABS: k_rowr_c2r<M, EPI_EOS_ABS><<<nmap, 256, smem, st>>>(d_sims, d_t, map, nmap, job); break;
+        default: break;
+    }
+}
+
+void launch_rowr_c2r(cudaStream_t st, const SimDev* d_sims, const int* d_t, const BlockWork* map, int nmap,
+                     const RowC2RJob& job, int M) {
+    if (nmap <= 0) return;
+    switch (M) {
+        case 16: launch_c2r_m<16>(st, d_sims, d_t, map, nmap, job); break;
+        case 32: launch_c2r_m<32>(st, d_sims, d_t, map, nmap, job); break;
+        case 64: launch_c2r_m<64>(st, d_sims, d_t, map, nmap, job); break;
+        case 128: launch_c2r_m<128>(st, d_sims, d_t, map, nmap, job); break;
+        case 256: launch_c2r_m<256>(st, d_sims, d_t, map, nmap, job); break;
+        default: break;
+    }
+}
+
+}  // namespace kw

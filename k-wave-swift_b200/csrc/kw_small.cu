@@ -202,6 +202,7 @@ void init_kernel_attributes() {
     init_r2c_attributes(optin);
     init_col_attributes(optin);
     init_c2r_attributes(optin);
+    init_rowr_attributes(optin);
     cudaFuncSetAttribute((const void*)k_intensity, cudaFuncAttributeMaxDynamicSharedMemorySize, optin - 1024);
     cudaGetLastError();  // the attribute calls must not leave a sticky error behind
 }
