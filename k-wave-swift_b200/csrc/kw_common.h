@@ -6,10 +6,12 @@
 //   3D (nx,ny,nz):  A = nx, B = ny, C = nz
 // i.e. exactly the row-major order of the reference's MLXArray fields. Spectra are the
 // half-spectrum of a real transform along C: [A][B][Cp] float2 with Ch = C/2 + 1 bins per row,
-// padded to Cp = Ch rounded up to even so that every spectrum row starts 16-byte aligned.
+// padded to Cp = Ch rounded up to a multiple of 4, so that every spectrum row and every row of a
+// float table over the half spectrum starts 16-byte aligned (TMA strides). Padding bins hold zeros.
 #pragma once
 
 #include <cstdint>
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 namespace kw {
@@ -43,13 +45,26 @@ __host__ __device__ constexpr int col_lines_op(int N) { return tile_lines(N) > 2
 // C2R passes also stage their epilogue inputs, so they take half as many lines
 __host__ __device__ constexpr int c2r_lines(int M) { return tile_lines(M) > 2 ? tile_lines(M) / 2 : 2; }
 
-// Register-resident two-stage column transforms (kw_pass_colr.cu): N = R1 * R2 with R1 >= R2,
-// R2 threads per line, each holding R1 values; 256 threads, so 256 / R2 lines per CTA.
+// Register-resident column transforms (kw_fft_reg.cuh) for line lengths 16 ... 256: N / R1
+// threads per line, each holding R1 values, so 256 / (N / R1) lines per 256 threads. The in-place
+// passes (kw_pass_colp.cu) hold colr_r1(N) values per thread, the operator pass (kw_pass_colop.cu)
+// colop_r1(N).
 __host__ __device__ constexpr bool has_two_stage_col(int n) {
     return n == 16 || n == 32 || n == 64 || n == 128 || n == 256;
 }
 __host__ __device__ constexpr int colr_r1(int n) { return n >= 128 ? 16 : (n >= 32 ? 8 : 4); }
-__host__ __device__ constexpr int colr_lines(int n) { return 256 / (n / colr_r1(n)); }
+__host__ __device__ constexpr int colop_r1(int n) { return colr_r1(n); }
+__host__ __device__ constexpr int reg_lines(int n, int r1) { return 256 / (n / r1); }
+__host__ __device__ constexpr int colr_lines(int n) { return reg_lines(n, colr_r1(n)); }
+__host__ __device__ constexpr int colop_lines(int n) { return reg_lines(n, colop_r1(n)); }
+
+// Register-resident row passes (kw_pass_rowr.cu) for even rows whose half length M is a power of
+// two in [16, 2048]. R2C threads hold colr_r1(M) values; C2R threads, whose epilogues keep more
+// state, hold c2r_r1(M) (more threads per row, fewer registers each).
+__host__ __device__ constexpr bool has_reg_row(int M) { return M >= 16 && M <= 2048 && (M & (M - 1)) == 0; }
+__host__ __device__ constexpr int c2r_r1(int M) { return M <= 16 ? 4 : 8; }
+__host__ __device__ constexpr int r2c_rows(int M) { return reg_lines(M, colr_r1(M)); }
+__host__ __device__ constexpr int c2r_rows(int M) { return reg_lines(M, c2r_r1(M)); }
 
 // Line lengths with compile-time specialised pass kernels (in-place, one shared buffer per tile);
 // every other length runs the runtime-plan kernels (ping-pong, two buffers per tile).
@@ -131,6 +146,12 @@ struct SensorDev {
     float* u_max[kMaxComp]; float* u_ss[kMaxComp]; float* u_ssc[kMaxComp];
 };
 
+// Tensor maps of one simulation (TMA descriptors, kw_tmaps.cpp): spectrum s viewed as tiles of
+// pass-axis lines for layout axis A (2D view [A][B*Cp]) or B (3D view [A][B][Cp]); only the views
+// an in-place column pass of a register-plan length needs are encoded.
+__host__ __device__ constexpr int tmap_spec(int s, int layout_axis) { return 2 * s + layout_axis; }
+constexpr int kNumTmaps = 8;
+
 struct SimDev {
     int dim;
     int A, B, C, Ch, Cp;
@@ -145,6 +166,7 @@ struct SimDev {
     FFTPlanDev plan_a;     // column plan along A (length A)
     float inv_n;           // 1 / N
     const float* radial[RT_COUNT];   // [A][B][Cp] tables (nullptr when unused)
+    const CUtensorMap* tmaps;        // [kNumTmaps] (device memory, 64-byte aligned)
 
     // state
     float* p;

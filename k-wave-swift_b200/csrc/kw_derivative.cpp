@@ -44,7 +44,7 @@ void Engine::create_derivative(int dim, const int* n, const double* d, int axis,
     else { h.A = n[0]; h.B = n[1]; h.C = n[2]; }
     h.N = (long long)h.A * h.B * h.C;
     h.Ch = h.C / 2 + 1;
-    h.Cp = h.Ch + (h.Ch & 1);
+    h.Cp = (h.Ch + 3) & ~3;   // a multiple of 4 (16-byte rows of the float radial tables)
     h.Ns = (long long)h.A * h.B * h.Cp;
     h.M = (h.C & 1) ? h.C : h.C / 2;
     h.nt = 1;
@@ -52,7 +52,7 @@ void Engine::create_derivative(int dim, const int* n, const double* d, int axis,
 
     d_sims_ = (SimDev*)dalloc(sizeof(SimDev));
     d_t_ = (int*)dalloc(sizeof(int));
-    d_flag_ = (int*)dalloc(sizeof(int));
+    d_flag_ = (int*)dalloc(2 * sizeof(int));
     d_red_ = (unsigned int*)dalloc(4 * sizeof(unsigned int));
     d_p0s_ = (const float**)dalloc(sizeof(float*));
 
@@ -93,6 +93,7 @@ void Engine::create_derivative(int dim, const int* n, const double* d, int axis,
     v.p = const_cast<float*>(in);
     v.tmp[0] = out;
     v.nonfinite = d_flag_;
+    build_tensor_maps(h, v);
     check(cudaMemcpyAsync(d_sims_, &v, sizeof(SimDev), cudaMemcpyHostToDevice, st()), "upload sim");
     deriv_axis_ = axis;
     deriv_shift_ = shift;
@@ -113,6 +114,7 @@ void Engine::run_derivative() {
     issue_job(j, -1);
     check(cudaGetLastError(), "launch");
     check(cudaStreamSynchronize(st()), "derivative sync");
+    check_kernel_error();
 }
 
 }  // namespace kw

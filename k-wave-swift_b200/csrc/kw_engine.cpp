@@ -422,7 +422,7 @@ void Engine::setup_sim(int s, const kw_sim_desc& d) {
     h.N = (long long)h.A * h.B * h.C;
     if (h.N > (1LL << 31) - 1) throw err(KW_ERR_UNSUPPORTED, "grids above 2^31 points are not supported");
     h.Ch = h.C / 2 + 1;
-    h.Cp = h.Ch + (h.Ch & 1);
+    h.Cp = (h.Ch + 3) & ~3;   // a multiple of 4 (16-byte rows of the float radial tables)
     h.Ns = (long long)h.A * h.B * h.Cp;
     const long long N = h.N;
     auto grid_sized = [&](const kw_array& a) { return a.data && (a.len == 1 || (long long)a.len == N); };
@@ -540,6 +540,7 @@ void Engine::setup_sim(int s, const kw_sim_desc& d) {
                     tab[((size_t)ia * h.B + ib) * h.Cp + kc] = (float)(0.5 * (W(m) + W(mm)));
                 }
         v.radial[RT_WINDOW] = upload(tab);
+        build_tensor_maps(h, v);   // the smoothing jobs below run the TMA-fed column pass
     }
     float* d_c0 = nullptr;
     float* d_rho0 = nullptr;
@@ -840,6 +841,7 @@ void Engine::setup_sim(int s, const kw_sim_desc& d) {
     }
     if (v.absorb >= 2) any_abs_ = true;
     if (v.has_p0) any_p0_ = true;
+    build_tensor_maps(h, v);
     check(cudaMemcpyAsync(d_sims_ + s, &v, sizeof(SimDev), cudaMemcpyHostToDevice, st()), "upload sim");
 }
 
@@ -853,7 +855,7 @@ void Engine::create(const kw_sim_desc* descs, int n) {
         if (descs[i].dim != dim_) throw err(KW_ERR_INVALID, "all simulations of a batch must have the same dimensionality");
     d_sims_ = (SimDev*)dalloc(sizeof(SimDev) * n);
     d_t_ = (int*)dalloc(sizeof(int));
-    d_flag_ = (int*)dalloc(sizeof(int));
+    d_flag_ = (int*)dalloc(2 * sizeof(int));   // [0] non-finite pressure, [1] device-side wait timeout
     d_red_ = (unsigned int*)dalloc(4 * sizeof(unsigned int));
     for (int i = 0; i < n; ++i) setup_sim(i, descs[i]);
     std::vector<const float*> p0s(n);
@@ -879,7 +881,7 @@ void Engine::reset() {
             if (v.src_buf[a]) check(cudaMemsetAsync(v.src_buf[a], 0, fb, st()), "reset");
     }
     check(cudaMemsetAsync(d_t_, 0, sizeof(int), st()), "reset");
-    check(cudaMemsetAsync(d_flag_, 0, sizeof(int), st()), "reset");
+    check(cudaMemsetAsync(d_flag_, 0, 2 * sizeof(int), st()), "reset");
     t_ = 0;
     finalized_t_ = -1;
 }
@@ -924,9 +926,19 @@ int Engine::synchronize() {
     const Map& m = map_elems(-1);
     launch_check_finite(st(), d_sims_, d_t_, m.d, m.n);
     check(cudaStreamSynchronize(st()), "synchronize");
+    check_kernel_error();
     int flag = 0;
     check(cudaMemcpy(&flag, d_flag_, sizeof(int), cudaMemcpyDeviceToHost), "flag");
     return flag ? KW_ERR_NONFINITE : KW_OK;
+}
+
+// A pass kernel whose bounded wait ran out leaves a code in d_flag_[1] (kw_async.cuh).
+void Engine::check_kernel_error() {
+    int code = 0;
+    check(cudaMemcpy(&code, d_flag_ + 1, sizeof(int), cudaMemcpyDeviceToHost), "kernel error flag");
+    if (code != 0)
+        throw err(KW_ERR_TIMEOUT, "a device-side wait of a pass kernel timed out (code " + std::to_string(code) +
+                                      "); the results of this run are invalid");
 }
 
 // ------------------------------------------------------------------------------------------

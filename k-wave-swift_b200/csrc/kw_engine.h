@@ -30,6 +30,11 @@ struct KwError {
 // Device address of the allocation-free scratch array on `device` (kw_noalloc.cu).
 void* noalloc_scratch(int device);
 
+struct SimHost;
+// true when the column pass along `layout_axis` (0 = A, 1 = B) of this simulation runs the
+// TMA-fed warp-specialised kernel (kw_tmaps.cpp)
+bool colp_enabled(const SimHost& h, int layout_axis);
+
 // Host-side record of one simulation.
 struct SimHost {
     kw_sim_desc d{};               // scalar fields of the descriptor (pointers not retained)
@@ -131,6 +136,8 @@ private:
     cudaStream_t st() const { return ctx_->stream; }
 
     void setup_sim(int s, const kw_sim_desc& d);
+    void build_tensor_maps(SimHost& h, SimDev& v);   // kw_tmaps.cpp
+    void check_kernel_error();
     void build_plan(FFTPlanDev& pl, int n);
     void smooth_field(int s, float* field);
     const Map& map_rows(int lines_per_row, int ncomp, int sim_only, int sclass);

@@ -10,10 +10,12 @@
 namespace kw {
 
 // size class of a row pass / column pass of one simulation (0 = runtime-plan kernels)
-static int row_class(const SimHost& h) { return (h.C % 2 == 0 && has_fixed_kernel(h.M)) ? h.M : 0; }
+static int row_class(const SimHost& h) {
+    return (h.C % 2 == 0 && (has_fixed_kernel(h.M) || has_reg_row(h.M))) ? h.M : 0;
+}
 // register-resident row kernels (kw_pass_rowr.cu) serve the even rows of two-stage half length;
 // the 1D forward row pass, which also applies the operator, keeps the staged kernel
-static bool rowr_class(int sclass) { return sclass != 0 && has_two_stage_col(sclass); }
+static bool rowr_class(int sclass) { return sclass != 0 && has_reg_row(sclass); }
 static int col_class(const SimHost& h, int axis) {
     const int n = axis == 0 ? h.A : h.B;
     return has_fixed_kernel(n) ? n : 0;
@@ -22,7 +24,8 @@ static int col_class(const SimHost& h, int axis) {
 // Row-pass tiles of the simulations of size class `sclass`. lines_per_row == 0: R2C tiles of
 // row_lines(M) rows; lines_per_row > 0: C2R tiles of c2r_lines(M) lines, i.e. c2r_lines(M) /
 // lines_per_row rows (a coupled C2R epilogue stages every component of a row in the same CTA);
-// lines_per_row < 0: tiles of colr_lines(M) rows for the register-resident kernels.
+// lines_per_row = -1 / -2: tiles of r2c_rows(M) / c2r_rows(M) rows for the register-resident R2C /
+// C2R kernels.
 const Engine::Map& Engine::map_rows(int lines_per_row, int ncomp, int sim_only, int sclass) {
     auto key = std::make_tuple(0, lines_per_row, ncomp, sim_only, sclass);
     auto it = maps_.find(key);
@@ -31,9 +34,10 @@ const Engine::Map& Engine::map_rows(int lines_per_row, int ncomp, int sim_only, 
     for (int s = 0; s < count(); ++s) {
         if ((sim_only >= 0 && s != sim_only) || row_class(sims_[s]) != sclass) continue;
         const int rows = sims_[s].A * sims_[s].B;
-        const int rpc = lines_per_row < 0    ? colr_lines(sims_[s].M)
-                        : lines_per_row == 0 ? row_lines(sims_[s].M)
-                                             : std::max(1, c2r_lines(sims_[s].M) / lines_per_row);
+        const int rpc = lines_per_row == -1  ? r2c_rows(sims_[s].M)
+                        : lines_per_row == -2 ? c2r_rows(sims_[s].M)
+                        : lines_per_row == 0  ? row_lines(sims_[s].M)
+                                              : std::max(1, c2r_lines(sims_[s].M) / lines_per_row);
         const int tiles = (rows + rpc - 1) / rpc;
         for (int c = 0; c < ncomp; ++c)
             for (int tI = 0; tI < tiles; ++tI) v.push_back(BlockWork{s, c, tI});
@@ -45,8 +49,7 @@ const Engine::Map& Engine::map_rows(int lines_per_row, int ncomp, int sim_only, 
 }
 
 // Column-pass tiles: col_lines(n) (col_lines_op(n) for an operator pass) contiguous columns, or
-// for the register-resident two-stage lengths colr_lines(n) lines of the flattened (outer, column)
-// index.
+// for the register-plan lengths colr_lines(n) (colop_lines(n)) columns of one plane.
 const Engine::Map& Engine::map_cols(int axis, int ncomp, int sim_only, bool op, int sclass) {
     auto key = std::make_tuple(1 + axis + (op ? 2 : 0), 0, ncomp, sim_only, sclass);
     auto it = maps_.find(key);
@@ -59,9 +62,9 @@ const Engine::Map& Engine::map_cols(int axis, int ncomp, int sim_only, bool op, 
         const int inner = axis == 0 ? h.B * h.Cp : h.Cp;
         const int outer = axis == 0 ? 1 : h.A;
         int tiles;
-        if (sclass && has_two_stage_col(sclass)) {   // tiles of colr_lines(n) flattened (outer, column) lines
-            const int tw = colr_lines(n);
-            tiles = (outer * inner + tw - 1) / tw;
+        if (sclass && has_two_stage_col(sclass)) {   // register-plan kernels: columns of one plane
+            const int tw = op ? colop_lines(n) : colr_lines(n);
+            tiles = outer * ((inner + tw - 1) / tw);
         } else {
             const int tw = op ? col_lines_op(n) : col_lines(n);
             tiles = outer * ((inner + tw - 1) / tw);
@@ -135,7 +138,7 @@ void Engine::issue_job(const SpecJob& job, int sim_only) {
         const bool reg = rowr_class(sc) && !rj.apply_op;
         const Map& m = map_rows(reg ? -1 : 0, comps_in, sim_only, sc);
         const double bytes = sum_sims(in_class, [&](const SimHost& h) { return open_comps(h, comps_in) * ((double)h.N * 4 + spec_bytes(h)); });
-        const size_t smem = (size_t)(sc ? 2 : 3) * te * sizeof(float2);
+        const size_t smem = (size_t)(has_fixed_kernel(sc) ? 2 : 3) * te * sizeof(float2);
         if (reg)
             timed(std::string("r2c:") + job.name, bytes, [&] { launch_rowr_r2c(st(), d_sims_, d_t_, m.d, m.n, rj, sc); });
         else
@@ -171,8 +174,11 @@ void Engine::issue_job(const SpecJob& job, int sim_only) {
             const double bytes = sum_sims(in_class, bytes_of);
             const long long tiles = sc ? (op ? 4 : 2) : (op ? 5 : 3);
             const size_t smem = (size_t)(tiles * te * sizeof(float2));
-            if (sc && has_two_stage_col(sc))
-                timed(std::string(label) + job.name, bytes, [&] { launch_colr(st(), d_sims_, d_t_, m.d, m.n, cj, sc); });
+            if (sc && has_two_stage_col(sc) && op)
+                timed(std::string(label) + job.name, bytes, [&] { launch_colop(st(), d_sims_, d_t_, m.d, m.n, cj, sc); });
+            else if (sc && has_two_stage_col(sc))
+                timed(std::string(label) + job.name, bytes,
+                      [&] { launch_colp(st(), d_sims_, d_t_, m.d, m.n, cj, sc, d_flag_ + 1); });
             else
                 timed(std::string(label) + job.name, bytes, [&] { launch_col(st(), d_sims_, d_t_, m.d, m.n, cj, smem, sc); });
         }
@@ -217,17 +223,17 @@ void Engine::issue_job(const SpecJob& job, int sim_only) {
         cj.epi = job.epi;
         cj.out_field = job.out_field;
         cj.gate = job.gate;
-        cj.generic = sc ? 0 : 1;
+        cj.generic = has_fixed_kernel(sc) ? 0 : 1;
         cj.tile_elems = te;
         const bool reg = rowr_class(sc);
-        const Map& m = map_rows(reg ? -1 : ncta, job.coupled ? 1 : job.nout, sim_only, sc);
+        const Map& m = map_rows(reg ? -2 : ncta, job.coupled ? 1 : job.nout, sim_only, sc);
         const double bytes = sum_sims(in_class, [&](const SimHost& h) {
             int no = job.coupled ? (open_comps(h, 1) ? job.nout : 0) : open_comps(h, job.nout);
             if (job.epi == EPI_EOS_ABS && no) no = h.dev.absorb == 3 ? 2 : 1;
             if (no == 0) return 0.0;
             return no * spec_bytes(h) + (double)h.N * epi_bytes(h, job.epi, job.coupled ? 1 : no);
         });
-        const size_t smem = (size_t)(sc ? 2 : 3) * te * sizeof(float2) + (size_t)aux_floats * sizeof(float);
+        const size_t smem = (size_t)(has_fixed_kernel(sc) ? 2 : 3) * te * sizeof(float2) + (size_t)aux_floats * sizeof(float);
         if (reg)
             timed(std::string("c2r:") + job.name, bytes, [&] { launch_rowr_c2r(st(), d_sims_, d_t_, m.d, m.n, cj, sc); });
         else

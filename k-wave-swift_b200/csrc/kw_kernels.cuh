@@ -54,20 +54,25 @@ struct RowC2RJob {
 void init_kernel_attributes();
 void init_r2c_attributes(int optin);
 void init_col_attributes(int optin);
-void init_colr_attributes(int optin);
 void init_c2r_attributes(int optin);
 void launch_row_r2c(cudaStream_t st, const SimDev* d_sims, const int* d_t, const BlockWork* map, int nmap,
                     const RowR2CJob& job, size_t smem, int size_class);
 void launch_col(cudaStream_t st, const SimDev* d_sims, const int* d_t, const BlockWork* map, int nmap,
                 const ColJob& job, size_t smem, int size_class);
-// register-resident column pass for has_two_stage_col(n) lengths; one CTA per map entry, whose
-// tile indexes colr_lines(n) consecutive (outer, column) lines
-void launch_colr(cudaStream_t st, const SimDev* d_sims, const int* d_t, const BlockWork* map, int nmap,
-                 const ColJob& job, int n);
 void launch_row_c2r(cudaStream_t st, const SimDev* d_sims, const int* d_t, const BlockWork* map, int nmap,
                     const RowC2RJob& job, size_t smem, int size_class);
-// register-resident row passes for even rows with has_two_stage_col(M) half lengths; one CTA per
-// map entry, whose tile indexes colr_lines(M) consecutive rows
+// register-resident operator column pass for has_two_stage_col(n) lengths; one CTA per map entry,
+// whose tile indexes colop_lines(n) consecutive columns (the pass's outer extent is 1)
+void init_colop_attributes(int optin);
+void launch_colop(cudaStream_t st, const SimDev* d_sims, const int* d_t, const BlockWork* map, int nmap,
+                  const ColJob& job, int n);
+// TMA-fed warp-specialised in-place column pass for has_two_stage_col(n) lengths (persistent grid);
+// tiles are colr_lines(n) columns of one plane; `err` receives a KernelError code if a wait times out
+void init_colp_attributes();
+void launch_colp(cudaStream_t st, const SimDev* d_sims, const int* d_t, const BlockWork* map, int nmap,
+                 const ColJob& job, int n, int* err);
+// register-resident row passes for even rows with has_reg_row(M) half lengths; one CTA per map
+// entry, whose tile indexes r2c_rows(M) / c2r_rows(M) consecutive rows
 void init_rowr_attributes(int optin);
 void launch_rowr_r2c(cudaStream_t st, const SimDev* d_sims, const int* d_t, const BlockWork* map, int nmap,
                      const RowR2CJob& job, int M);

@@ -219,7 +219,7 @@ void init_col_attributes(int optin) {
     set_col_attrs<COL_FWD>(optin);
     set_col_attrs<COL_INV>(optin);
     set_col_attrs<COL_FWD_OP_INV>(optin);
-    init_colr_attributes(optin);
+    init_colop_attributes(optin);
 }
 
 template <int MODE>

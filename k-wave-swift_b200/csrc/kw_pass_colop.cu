@@ -1,0 +1,142 @@
+// kw_pass_colop.cu — the operator column pass: the last forward pass of a spectral job (along A in
+// 3D, along B in 2D) for the register-plan lengths (has_two_stage_col: N = 16 ... 256).
+//
+// A CTA owns TW = colop_lines(N) consecutive spectrum columns; thread t of line l loads rows
+// t + T r straight from HBM (consecutive lanes read consecutive columns), transforms forward
+// (kw_fft_reg.cuh), multiplies by the radial table and 1/N, and transforms back with the
+// intermediate product kept in registers. Outputs whose per-axis factor is along another axis share
+// one inverse and take the factor on the way out; an output whose factor varies along the line
+// gets its own inverse. With several outputs the product is parked in shared memory (each thread
+// its own slots) so that only one line's worth of registers is live. Many small CTAs per SM keep
+// enough loads in flight.
+#include "kw_fft_reg.cuh"
+#include "kw_pass_common.cuh"
+
+namespace kw {
+
+template <int N>
+__global__ void __launch_bounds__(256) k_colop(const SimDev* __restrict__ sims, const int* __restrict__ d_t,
+                                               const BlockWork* __restrict__ map, int nmap, ColJob job) {
+    using P = RegPlan<N, colop_r1(N)>;
+    using Lay = ColLayout<P, N>;
+    constexpr int R1 = P::R1, T = P::T, TW = P::LINES;
+    __shared__ float2 sh[Lay::SLOTS];
+    extern __shared__ __align__(16) float2 parked[];   // [R1][256] when the job has several outputs
+    if (blockIdx.x >= nmap) return;
+    const BlockWork bw = map[blockIdx.x];
+    const SimDev& S = sims[bw.sim];
+    if (!gate_open(S, job.gate, bw.comp, *d_t)) return;
+
+    // the pass's lines are the columns of one plane (the layout axis before it has length 1)
+    const bool axisA = job.layout_axis == 0;
+    const int inner = axisA ? S.B * S.Cp : S.Cp;
+    const int l = threadIdx.x % TW;
+    const int t = threadIdx.x / TW;
+    const int c = bw.tile * TW + l;
+    const bool col_ok = c < inner;
+    const long long base = col_ok ? c : 0;
+    const float2* __restrict__ twn = axisA ? S.plan_a.twn : S.plan_b.twn;
+    const int comp_in = job.fanout ? 0 : bw.comp;
+    const float2* in = S.spec[job.spec_in + comp_in] + base;
+
+    float2 v[R1];
+#pragma unroll
+    for (int r = 0; r < R1; ++r) v[r] = col_ok ? in[(long long)(t + T * r) * inner] : make_float2(0.f, 0.f);
+
+    FftReg<N, P, false, Lay>::run(v, sh, t, l, twn);          // v[m] = X(row t + T m)
+    int kb = 0, kc = c;
+    if (axisA) { kb = c / S.Cp; kc = c - kb * S.Cp; }
+    const bool bin_ok = col_ok && kc < S.Ch;
+    const int pass_ref_axis = (axisA ? 0 : 1) - (3 - S.dim);
+    const int nouts = job.fanout ? job.nout : 1;
+    auto op_of = [&](int oc) { return oc == 0 ? job.op[0] : (oc == 1 ? job.op[1] : job.op[2]); };
+    auto out_comp = [&](int oo) { return job.fanout ? oo : bw.comp; };
+    auto factor_vec = [&](const OpSpec& op) -> const float2* {
+        if (op.axis_op == AO_NONE) return nullptr;
+        const AxisDev& ax = S.ax[op.axis];
+        return op.axis_op == AO_DPOS ? ax.dpos : (op.axis_op == AO_DNEG ? ax.dneg : ax.colloc);
+    };
+    auto along = [&](const OpSpec& op) { return op.axis_op != AO_NONE && op.axis == pass_ref_axis; };
+    const int rad = op_of(job.fanout ? 0 : bw.comp).radial;
+    // X * radial / N: the factor common to every output (padding bins are never stored: they stay zero)
+    const float* tab = rad != RT_NONE ? S.radial[rad] + base : nullptr;
+    const float inv_n = S.inv_n;
+#pragma unroll
+    for (int m = 0; m < R1; ++m) {
+        float f = inv_n;
+        if (tab && bin_ok) f *= __ldg(tab + (long long)(t + T * m) * inner);
+        v[m] = bin_ok ? cscale(v[m], f) : make_float2(0.f, 0.f);
+    }
+    // H_o = F_o(k_a) kappa / N. A factor F_o along another axis is constant along the line, so
+    // it commutes with the inverse: those outputs share one inverse and take F_o on the way out.
+    // With several outputs the product is parked in shared memory (this thread's own slots) so
+    // that only one line's worth of registers is live.
+    bool shared = false;
+    for (int oo = 0; oo < nouts; ++oo) shared |= !along(op_of(out_comp(oo)));
+    const bool park = nouts > 1;
+    if (park) {
+#pragma unroll
+        for (int m = 0; m < R1; ++m) parked[m * 256 + threadIdx.x] = v[m];
+    }
+    if (shared) {
+        FftReg<N, P, true, Lay>::run(v, sh, t, l, twn);
+        for (int oo = 0; oo < nouts; ++oo) {
+            const int oc = out_comp(oo);
+            const OpSpec op = op_of(oc);
+            if (along(op)) continue;
+            const float2* fv = factor_vec(op);
+            float2 f = make_float2(1.f, 0.f);
+            if (fv && bin_ok) f = __ldg(fv + axis_index(S, op.axis, 0, kb, kc));
+            float2* out = S.spec[job.spec_out + oc] + base;
+            if (bin_ok) {
+#pragma unroll
+                for (int m = 0; m < R1; ++m) out[(long long)(t + T * m) * inner] = cmul(v[m], f);
+            }
+        }
+    }
+    for (int oo = 0; oo < nouts; ++oo) {   // outputs whose factor varies along the line
+        const int oc = out_comp(oo);
+        const OpSpec op = op_of(oc);
+        if (!along(op)) continue;
+        const float2* fv = factor_vec(op);
+        if (park) {
+#pragma unroll
+            for (int m = 0; m < R1; ++m) v[m] = parked[m * 256 + threadIdx.x];
+        }
+#pragma unroll
+        for (int m = 0; m < R1; ++m) v[m] = cmul(v[m], __ldg(fv + t + T * m));
+        FftReg<N, P, true, Lay>::run(v, sh, t, l, twn);
+        float2* out = S.spec[job.spec_out + oc] + base;
+        if (bin_ok) {
+#pragma unroll
+            for (int m = 0; m < R1; ++m) out[(long long)(t + T * m) * inner] = v[m];
+        }
+    }
+}
+
+template <int N>
+static size_t colop_park_bytes(const ColJob& job) {
+    return job.fanout && job.nout > 1 ? (size_t)colop_r1(N) * 256 * sizeof(float2) : 0;
+}
+
+void init_colop_attributes(int optin) {
+    set_max_smem((const void*)k_colop<16>, optin);
+    set_max_smem((const void*)k_colop<32>, optin);
+    set_max_smem((const void*)k_colop<64>, optin);
+    set_max_smem((const void*)k_colop<128>, optin);
+    set_max_smem((const void*)k_colop<256>, optin);
+}
+
+void launch_colop(cudaStream_t st, const SimDev* d_sims, const int* d_t, const BlockWork* map, int nmap,
+                  const ColJob& job, int n) {
+    if (nmap <= 0) return;
+    switch (n) {
+#define KW_CASE(n) \
+    case n: k_colop<n><<<nmap, 256, colop_park_bytes<n>(job), st>>>(d_sims, d_t, map, nmap, job); break;
+        KW_CASE(16) KW_CASE(32) KW_CASE(64) KW_CASE(128) KW_CASE(256)
+#undef KW_CASE
+        default: break;
+    }
+}
+
+}  // namespace kw

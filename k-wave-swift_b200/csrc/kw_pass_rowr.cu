@@ -1,5 +1,5 @@
-// kw_pass_rowr.cu — register-resident row passes for even rows whose half length M = C / 2 has
-// a two-stage transform (has_two_stage_col: M = 16 ... 256, i.e. C = 32 ... 512).
+// kw_pass_rowr.cu — register-resident row passes for even rows whose half length M = C / 2 is a
+// power of two in [16, 2048] (has_reg_row).
 //
 // A 256-thread CTA owns 256 / T consecutive rows; the T threads of a row are consecutive lanes, so
 // every load and store walks the row contiguously. Thread t of a row holds the packed values
@@ -24,8 +24,8 @@ namespace kw {
 template <int M>
 __global__ void __launch_bounds__(256) k_rowr_r2c(const SimDev* __restrict__ sims, const int* __restrict__ d_t,
                                                   const BlockWork* __restrict__ map, int nmap, RowR2CJob job) {
-    using P = TwoStage<M>;
-    using Lay = RowLayout<M>;
+    using P = RegPlan<M, colr_r1(M)>;
+    using Lay = RowLayout<P, M>;
     constexpr int R1 = P::R1, T = P::T, TW = P::LINES;
     __shared__ float2 sh[Lay::SLOTS];
     if (blockIdx.x >= nmap) return;
@@ -39,7 +39,7 @@ __global__ void __launch_bounds__(256) k_rowr_r2c(const SimDev* __restrict__ sim
     float2 v[R1];
 #pragma unroll
     for (int r = 0; r < R1; ++r) v[r] = ok ? in[t + T * r] : make_float2(0.f, 0.f);
-    FftReg<M, false, Lay>::run(v, sh, t, l, S.plan_row.twn);
+    FftReg<M, P, false, Lay>::run(v, sh, t, l, S.plan_row.twn);
     // the split needs Z[M - k], held by another thread of the row
 #pragma unroll
     for (int m = 0; m < R1; ++m) sh[Lay::at(t + T * m, l)] = v[m];
@@ -74,8 +74,8 @@ __device__ __forceinline__ float& half(float2& v, int h) { return h ? v.y : v.x;
 template <int M, int EPI>
 __global__ void __launch_bounds__(256) k_rowr_c2r(const SimDev* __restrict__ sims, const int* __restrict__ d_t,
                                                   const BlockWork* __restrict__ map, int nmap, RowC2RJob job) {
-    using P = TwoStage<M>;
-    using Lay = RowLayout<M>;
+    using P = RegPlan<M, c2r_r1(M)>;
+    using Lay = RowLayout<P, M>;
     constexpr int R1 = P::R1, T = P::T, TW = P::LINES;
     // pairs whose inputs are loaded together (the density update reads the most fields)
     constexpr int MB = (EPI == EPI_DEN || R1 < 4) ? 2 : 4;
@@ -107,7 +107,7 @@ __global__ void __launch_bounds__(256) k_rowr_c2r(const SimDev* __restrict__ sim
             const float2 e = cmulc(dd, __ldg(tw + k));
             v[m] = make_float2(s.x - e.y, s.y + e.x);
         }
-        FftReg<M, true, Lay>::run(v, sh, t, l, S.plan_row.twn);
+        FftReg<M, P, true, Lay>::run(v, sh, t, l, S.plan_row.twn);
         if (cc + 1 < ncomp) {
 #pragma unroll
             for (int m = 0; m < R1; ++m) parked[(cc * R1 + m) * 256 + threadIdx.x] = v[m];
@@ -286,7 +286,7 @@ __global__ void __launch_bounds__(256) k_rowr_c2r(const SimDev* __restrict__ sim
 // host side
 // ---------------------------------------------------------------------------------------------
 template <int M>
-static size_t rowr_park_bytes(int ncomp) { return (size_t)(ncomp > 1 ? ncomp - 1 : 0) * colr_r1(M) * 256 * sizeof(float2); }
+static size_t rowr_park_bytes(int ncomp) { return (size_t)(ncomp > 1 ? ncomp - 1 : 0) * c2r_r1(M) * 256 * sizeof(float2); }
 
 template <int EPI>
 static void set_rowr_attrs(int optin) {
@@ -295,6 +295,9 @@ static void set_rowr_attrs(int optin) {
     set_max_smem((const void*)k_rowr_c2r<64, EPI>, optin);
     set_max_smem((const void*)k_rowr_c2r<128, EPI>, optin);
     set_max_smem((const void*)k_rowr_c2r<256, EPI>, optin);
+    set_max_smem((const void*)k_rowr_c2r<512, EPI>, optin);
+    set_max_smem((const void*)k_rowr_c2r<1024, EPI>, optin);
+    set_max_smem((const void*)k_rowr_c2r<2048, EPI>, optin);
 }
 
 void init_rowr_attributes(int optin) {
@@ -311,6 +314,9 @@ void launch_rowr_r2c(cudaStream_t st, const SimDev* d_sims, const int* d_t, cons
         case 64: k_rowr_r2c<64><<<nmap, 256, 0, st>>>(d_sims, d_t, map, nmap, job); break;
         case 128: k_rowr_r2c<128><<<nmap, 256, 0, st>>>(d_sims, d_t, map, nmap, job); break;
         case 256: k_rowr_r2c<256><<<nmap, 256, 0, st>>>(d_sims, d_t, map, nmap, job); break;
+        case 512: k_rowr_r2c<512><<<nmap, 256, 0, st>>>(d_sims, d_t, map, nmap, job); break;
+        case 1024: k_rowr_r2c<1024><<<nmap, 256, 0, st>>>(d_sims, d_t, map, nmap, job); break;
+        case 2048: k_rowr_r2c<2048><<<nmap, 256, 0, st>>>(d_sims, d_t, map, nmap, job); break;
         default: break;
     }
 }
@@ -340,6 +346,9 @@ void launch_rowr_c2r(cudaStream_t st, const SimDev* d_sims, const int* d_t, cons
         case 64: launch_c2r_m<64>(st, d_sims, d_t, map, nmap, job); break;
         case 128: launch_c2r_m<128>(st, d_sims, d_t, map, nmap, job); break;
         case 256: launch_c2r_m<256>(st, d_sims, d_t, map, nmap, job); break;
+        case 512: launch_c2r_m<512>(st, d_sims, d_t, map, nmap, job); break;
+        case 1024: launch_c2r_m<1024>(st, d_sims, d_t, map, nmap, job); break;
+        case 2048: launch_c2r_m<2048>(st, d_sims, d_t, map, nmap, job); break;
         default: break;
     }
 }

@@ -203,6 +203,7 @@ void init_kernel_attributes() {
     init_col_attributes(optin);
     init_c2r_attributes(optin);
     init_rowr_attributes(optin);
+    init_colp_attributes();
     cudaFuncSetAttribute((const void*)k_intensity, cudaFuncAttributeMaxDynamicSharedMemorySize, optin - 1024);
     cudaGetLastError();  // the attribute calls must not leave a sticky error behind
 }
