@@ -45,26 +45,33 @@ __host__ __device__ constexpr int col_lines_op(int N) { return tile_lines(N) > 2
 // C2R passes also stage their epilogue inputs, so they take half as many lines
 __host__ __device__ constexpr int c2r_lines(int M) { return tile_lines(M) > 2 ? tile_lines(M) / 2 : 2; }
 
-// Register-resident column transforms (kw_fft_reg.cuh) for line lengths 16 ... 256: N / R1
-// threads per line, each holding R1 values, so 256 / (N / R1) lines per 256 threads. The in-place
-// passes (kw_pass_colp.cu) hold colr_r1(N) values per thread, the operator pass (kw_pass_colop.cu)
-// colop_r1(N).
-__host__ __device__ constexpr bool has_two_stage_col(int n) {
-    return n == 16 || n == 32 || n == 64 || n == 128 || n == 256;
+// Register-resident transforms (kw_fft_reg.cuh): lengths with a register plan are the powers of
+// two 16 ... 4096 and 12 * 2^k, 24 ... 3072. N / R1 threads hold R1 values each, so one 256-thread
+// group covers 256 / (N / R1) lines. The in-place column passes (TMA-fed, kw_pass_colp.cu) take
+// lengths up to 256 (one TMA box), the operator column pass (kw_pass_colop.cu) up to 1024, the row
+// passes (kw_pass_rowr.cu) half lengths up to 2048.
+__host__ __device__ constexpr bool is_pow2(int n) { return n > 0 && (n & (n - 1)) == 0; }
+__host__ __device__ constexpr bool has_reg_plan(int n) {
+    return (is_pow2(n) && n >= 16 && n <= 4096) || (n % 12 == 0 && is_pow2(n / 12) && n / 12 >= 2 && n / 12 <= 256);
 }
-__host__ __device__ constexpr int colr_r1(int n) { return n >= 128 ? 16 : (n >= 32 ? 8 : 4); }
-__host__ __device__ constexpr int colop_r1(int n) { return colr_r1(n); }
+__host__ __device__ constexpr int reg_r1(int n) { return n % 3 == 0 ? 12 : (n >= 128 ? 16 : (n >= 32 ? 8 : 4)); }
 __host__ __device__ constexpr int reg_lines(int n, int r1) { return 256 / (n / r1); }
-__host__ __device__ constexpr int colr_lines(int n) { return reg_lines(n, colr_r1(n)); }
-__host__ __device__ constexpr int colop_lines(int n) { return reg_lines(n, colop_r1(n)); }
-
-// Register-resident row passes (kw_pass_rowr.cu) for even rows whose half length M is a power of
-// two in [16, 2048]. R2C threads hold colr_r1(M) values; C2R threads, whose epilogues keep more
-// state, hold c2r_r1(M) (more threads per row, fewer registers each).
-__host__ __device__ constexpr bool has_reg_row(int M) { return M >= 16 && M <= 2048 && (M & (M - 1)) == 0; }
-__host__ __device__ constexpr int c2r_r1(int M) { return M <= 16 ? 4 : 8; }
-__host__ __device__ constexpr int r2c_rows(int M) { return reg_lines(M, colr_r1(M)); }
+__host__ __device__ constexpr bool has_colp(int n) { return has_reg_plan(n) && n <= 256; }
+__host__ __device__ constexpr bool has_colop(int n) { return has_reg_plan(n) && n <= 1024; }
+__host__ __device__ constexpr int colr_lines(int n) { return reg_lines(n, reg_r1(n)); }
+__host__ __device__ constexpr int colop_lines(int n) { return reg_lines(n, reg_r1(n)); }
+// Row passes for even rows: R2C threads hold reg_r1(M) values; C2R threads, whose epilogues keep
+// more state, hold c2r_r1(M) (more threads per row, fewer registers each).
+__host__ __device__ constexpr bool has_reg_row(int M) { return has_reg_plan(M) && M <= 2048; }
+__host__ __device__ constexpr int c2r_r1(int M) { return M % 3 == 0 ? 12 : (M <= 16 ? 4 : 8); }
+__host__ __device__ constexpr int r2c_rows(int M) { return reg_lines(M, reg_r1(M)); }
 __host__ __device__ constexpr int c2r_rows(int M) { return reg_lines(M, c2r_r1(M)); }
+
+// size lists of the instantiated register-plan kernels
+#define KW_REG_ROW_SIZES(X) X(16) X(32) X(64) X(128) X(256) X(512) X(1024) X(2048) X(24) X(48) X(96) X(192) X(384) \
+    X(768) X(1536)
+#define KW_COLP_SIZES(X) X(16) X(32) X(64) X(128) X(256) X(24) X(48) X(96) X(192)
+#define KW_COLOP_SIZES(X) X(16) X(32) X(64) X(128) X(256) X(512) X(1024) X(24) X(48) X(96) X(192) X(384) X(768)
 
 // Line lengths with compile-time specialised pass kernels (in-place, one shared buffer per tile);
 // every other length runs the runtime-plan kernels (ping-pong, two buffers per tile).

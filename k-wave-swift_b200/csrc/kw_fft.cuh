@@ -116,6 +116,38 @@ struct DFT<8, INV> {
     }
 };
 
+// 12 = 3 x 4: DFT4 over n2 for each n1 (x[n1 + 3 n2]), twiddle W12^{n1 k2}, DFT3 over n1 for each
+// k2; output k2 + 4 k1.
+template <bool INV>
+struct DFT<12, INV> {
+    __device__ __forceinline__ static void run(float2* v) {
+        const float h = 0.86602540378443864676f;  // sqrt(3) / 2
+        float2 y[3][4];
+#pragma unroll
+        for (int n1 = 0; n1 < 3; ++n1) {
+#pragma unroll
+            for (int n2 = 0; n2 < 4; ++n2) y[n1][n2] = v[n1 + 3 * n2];
+            dft4<INV>(y[n1][0], y[n1][1], y[n1][2], y[n1][3]);
+        }
+        // exp(-2 pi i m / 12) for m = n1 k2: m = 1, 2, 3 (n1 = 1) and 2, 4, 6 (n1 = 2)
+        const float2 w1 = make_float2(h, -0.5f), w2 = make_float2(0.5f, -h), w3 = make_float2(0.f, -1.f);
+        const float2 w4 = make_float2(-0.5f, -h), w6 = make_float2(-1.f, 0.f);
+        y[1][1] = twiddle<INV>(y[1][1], w1);
+        y[1][2] = twiddle<INV>(y[1][2], w2);
+        y[1][3] = twiddle<INV>(y[1][3], w3);
+        y[2][1] = twiddle<INV>(y[2][1], w2);
+        y[2][2] = twiddle<INV>(y[2][2], w4);
+        y[2][3] = twiddle<INV>(y[2][3], w6);
+#pragma unroll
+        for (int k2 = 0; k2 < 4; ++k2) {
+            float2 t[3] = {y[0][k2], y[1][k2], y[2][k2]};
+            DFT<3, INV>::run(t);
+#pragma unroll
+            for (int k1 = 0; k1 < 3; ++k1) v[k2 + 4 * k1] = t[k1];
+        }
+    }
+};
+
 template <bool INV>
 struct DFT<16, INV> {
     __device__ __forceinline__ static void run(float2* v) {

@@ -1,5 +1,5 @@
-// kw_fft_reg.cuh — register-resident Stockham transform of N = R1 * R1 * ... * Rlast points
-// (N a power of two; every later radix divides R1).
+// kw_fft_reg.cuh — register-resident Stockham transform of N = R1 * R_1 * ... * R_last points
+// (every later radix divides R1: powers of two with R1 = 4, 8 or 16, and 12 * 2^k with R1 = 12).
 //
 // A line is handled by T = N / R1 threads; thread t holds the R1 values x[t + T r] (r < R1).
 //   stage 0   radix-R1 DFT in registers (butterfly j = t); outputs y[t R1 + r] to shared memory
@@ -23,12 +23,14 @@ struct RegPlan {
     static constexpr int R1 = R1_;
     static constexpr int T = N / R1;           // threads per line
     static constexpr int LINES = 256 / T;      // lines per 256 threads
-    // radix of stage s: R1 while R1 still divides what is left, then the (smaller) remainder
+    __host__ __device__ static constexpr int gcd(int a, int b) { return b == 0 ? a : gcd(b, a % b); }
+    // radix of stage s: R1 for stage 0, then the largest divisor of R1 that divides what is left
+    // (every later radix divides R1, so each thread runs a whole number of butterflies)
     __host__ __device__ static constexpr int radix(int s) {
-        int left = N;
+        int left = N / R1;
         int r = R1;
-        for (int i = 0; i <= s; ++i) {
-            r = left >= R1 ? R1 : left;
+        for (int i = 1; i <= s; ++i) {
+            r = gcd(R1, left);
             left /= r;
         }
         return r;
@@ -40,11 +42,11 @@ struct RegPlan {
     }
     __host__ __device__ static constexpr int stages() {
         int n = 0;
-        while (before(n) < N) ++n;
+        while (n < 32 && before(n) < N && radix(n) > 1) ++n;
         return n;
     }
     static constexpr int NSTAGES = stages();
-    static_assert((N & (N - 1)) == 0 && N % R1 == 0 && T >= 1 && T <= 256 && 256 % T == 0, "register plan");
+    static_assert(N % R1 == 0 && T >= 1 && T <= 256 && 256 % T == 0, "register plan");
     static_assert(before(NSTAGES) == N && NSTAGES >= 2, "register plan stages");
 };
 

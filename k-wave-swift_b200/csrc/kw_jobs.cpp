@@ -62,7 +62,7 @@ const Engine::Map& Engine::map_cols(int axis, int ncomp, int sim_only, bool op, 
         const int inner = axis == 0 ? h.B * h.Cp : h.Cp;
         const int outer = axis == 0 ? 1 : h.A;
         int tiles;
-        if (sclass && has_two_stage_col(sclass)) {   // register-plan kernels: columns of one plane
+        if (sclass && (op ? has_colop(sclass) : has_colp(sclass))) {   // register-plan kernels: columns of one plane
             const int tw = op ? colop_lines(n) : colr_lines(n);
             tiles = outer * ((inner + tw - 1) / tw);
         } else {
@@ -174,9 +174,9 @@ void Engine::issue_job(const SpecJob& job, int sim_only) {
             const double bytes = sum_sims(in_class, bytes_of);
             const long long tiles = sc ? (op ? 4 : 2) : (op ? 5 : 3);
             const size_t smem = (size_t)(tiles * te * sizeof(float2));
-            if (sc && has_two_stage_col(sc) && op)
+            if (sc && op && has_colop(sc))
                 timed(std::string(label) + job.name, bytes, [&] { launch_colop(st(), d_sims_, d_t_, m.d, m.n, cj, sc); });
-            else if (sc && has_two_stage_col(sc))
+            else if (sc && !op && has_colp(sc))
                 timed(std::string(label) + job.name, bytes,
                       [&] { launch_colp(st(), d_sims_, d_t_, m.d, m.n, cj, sc, d_flag_ + 1); });
             else

@@ -61,12 +61,12 @@ void launch_col(cudaStream_t st, const SimDev* d_sims, const int* d_t, const Blo
                 const ColJob& job, size_t smem, int size_class);
 void launch_row_c2r(cudaStream_t st, const SimDev* d_sims, const int* d_t, const BlockWork* map, int nmap,
                     const RowC2RJob& job, size_t smem, int size_class);
-// register-resident operator column pass for has_two_stage_col(n) lengths; one CTA per map entry,
+// register-resident operator column pass for has_colop(n) lengths; one CTA per map entry,
 // whose tile indexes colop_lines(n) consecutive columns (the pass's outer extent is 1)
 void init_colop_attributes(int optin);
 void launch_colop(cudaStream_t st, const SimDev* d_sims, const int* d_t, const BlockWork* map, int nmap,
                   const ColJob& job, int n);
-// TMA-fed warp-specialised in-place column pass for has_two_stage_col(n) lengths (persistent grid);
+// TMA-fed warp-specialised in-place column pass for has_colp(n) lengths (persistent grid);
 // tiles are colr_lines(n) columns of one plane; `err` receives a KernelError code if a wait times out
 void init_colp_attributes();
 void launch_colp(cudaStream_t st, const SimDev* d_sims, const int* d_t, const BlockWork* map, int nmap,

@@ -1,5 +1,5 @@
 // kw_pass_colop.cu — the operator column pass: the last forward pass of a spectral job (along A in
-// 3D, along B in 2D) for the register-plan lengths (has_two_stage_col: N = 16 ... 256).
+// 3D, along B in 2D) for the register-plan lengths (has_colop: N = 16 ... 1024).
 //
 // A CTA owns TW = colop_lines(N) consecutive spectrum columns; thread t of line l loads rows
 // t + T r straight from HBM (consecutive lanes read consecutive columns), transforms forward
@@ -17,7 +17,7 @@ namespace kw {
 template <int N>
 __global__ void __launch_bounds__(256) k_colop(const SimDev* __restrict__ sims, const int* __restrict__ d_t,
                                                const BlockWork* __restrict__ map, int nmap, ColJob job) {
-    using P = RegPlan<N, colop_r1(N)>;
+    using P = RegPlan<N, reg_r1(N)>;
     using Lay = ColLayout<P, N>;
     constexpr int R1 = P::R1, T = P::T, TW = P::LINES;
     __shared__ float2 sh[Lay::SLOTS];
@@ -116,15 +116,13 @@ __global__ void __launch_bounds__(256) k_colop(const SimDev* __restrict__ sims, 
 
 template <int N>
 static size_t colop_park_bytes(const ColJob& job) {
-    return job.fanout && job.nout > 1 ? (size_t)colop_r1(N) * 256 * sizeof(float2) : 0;
+    return job.fanout && job.nout > 1 ? (size_t)reg_r1(N) * 256 * sizeof(float2) : 0;
 }
 
 void init_colop_attributes(int optin) {
-    set_max_smem((const void*)k_colop<16>, optin);
-    set_max_smem((const void*)k_colop<32>, optin);
-    set_max_smem((const void*)k_colop<64>, optin);
-    set_max_smem((const void*)k_colop<128>, optin);
-    set_max_smem((const void*)k_colop<256>, optin);
+#define KW_SET(n) set_max_smem((const void*)k_colop<n>, optin);
+    KW_COLOP_SIZES(KW_SET)
+#undef KW_SET
 }
 
 void launch_colop(cudaStream_t st, const SimDev* d_sims, const int* d_t, const BlockWork* map, int nmap,
@@ -133,7 +131,7 @@ void launch_colop(cudaStream_t st, const SimDev* d_sims, const int* d_t, const B
     switch (n) {
 #define KW_CASE(n) \
     case n: k_colop<n><<<nmap, 256, colop_park_bytes<n>(job), st>>>(d_sims, d_t, map, nmap, job); break;
-        KW_CASE(16) KW_CASE(32) KW_CASE(64) KW_CASE(128) KW_CASE(256)
+        KW_COLOP_SIZES(KW_CASE)
 #undef KW_CASE
         default: break;
     }

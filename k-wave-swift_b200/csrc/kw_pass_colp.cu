@@ -20,7 +20,7 @@ namespace kw {
 
 template <int N>
 struct ColpCfg {
-    using P = RegPlan<N, colr_r1(N)>;
+    using P = RegPlan<N, reg_r1(N)>;
     static constexpr int TW = P::LINES;
     static constexpr int STAGE = N * TW * 8;   // one tile: TW columns by N rows
     static constexpr int EXCH = ColLayout<P, N>::SLOTS * 8;
@@ -139,8 +139,9 @@ static void colp_attr() {
 }
 
 void init_colp_attributes() {
-    colp_attr<16, false>(); colp_attr<32, false>(); colp_attr<64, false>(); colp_attr<128, false>(); colp_attr<256, false>();
-    colp_attr<16, true>(); colp_attr<32, true>(); colp_attr<64, true>(); colp_attr<128, true>(); colp_attr<256, true>();
+#define KW_SET(n) colp_attr<n, false>(); colp_attr<n, true>();
+    KW_COLP_SIZES(KW_SET)
+#undef KW_SET
 }
 
 template <int N, bool INV>
@@ -163,11 +164,10 @@ template <bool INV>
 static void launch_dir(cudaStream_t st, const SimDev* d_sims, const int* d_t, const BlockWork* map, int nmap,
                        const ColJob& job, int n, int* err) {
     switch (n) {
-        case 16: launch_one<16, INV>(st, d_sims, d_t, map, nmap, job, err); break;
-        case 32: launch_one<32, INV>(st, d_sims, d_t, map, nmap, job, err); break;
-        case 64: launch_one<64, INV>(st, d_sims, d_t, map, nmap, job, err); break;
-        case 128: launch_one<128, INV>(st, d_sims, d_t, map, nmap, job, err); break;
-        case 256: launch_one<256, INV>(st, d_sims, d_t, map, nmap, job, err); break;
+#define KW_CASE(n) \
+    case n: launch_one<n, INV>(st, d_sims, d_t, map, nmap, job, err); break;
+        KW_COLP_SIZES(KW_CASE)
+#undef KW_CASE
         default: break;
     }
 }

@@ -1,5 +1,5 @@
-// kw_pass_rowr.cu — register-resident row passes for even rows whose half length M = C / 2 is a
-// power of two in [16, 2048] (has_reg_row).
+// kw_pass_rowr.cu — register-resident row passes for even rows whose half length M = C / 2 has a
+// register plan (has_reg_row: powers of two 16 ... 2048 and 12 * 2^k up to 1536).
 //
 // A 256-thread CTA owns 256 / T consecutive rows; the T threads of a row are consecutive lanes, so
 // every load and store walks the row contiguously. Thread t of a row holds the packed values
@@ -24,7 +24,7 @@ namespace kw {
 template <int M>
 __global__ void __launch_bounds__(256) k_rowr_r2c(const SimDev* __restrict__ sims, const int* __restrict__ d_t,
                                                   const BlockWork* __restrict__ map, int nmap, RowR2CJob job) {
-    using P = RegPlan<M, colr_r1(M)>;
+    using P = RegPlan<M, reg_r1(M)>;
     using Lay = RowLayout<P, M>;
     constexpr int R1 = P::R1, T = P::T, TW = P::LINES;
     __shared__ float2 sh[Lay::SLOTS];
@@ -290,14 +290,9 @@ static size_t rowr_park_bytes(int ncomp) { return (size_t)(ncomp > 1 ? ncomp - 1
 
 template <int EPI>
 static void set_rowr_attrs(int optin) {
-    set_max_smem((const void*)k_rowr_c2r<16, EPI>, optin);
-    set_max_smem((const void*)k_rowr_c2r<32, EPI>, optin);
-    set_max_smem((const void*)k_rowr_c2r<64, EPI>, optin);
-    set_max_smem((const void*)k_rowr_c2r<128, EPI>, optin);
-    set_max_smem((const void*)k_rowr_c2r<256, EPI>, optin);
-    set_max_smem((const void*)k_rowr_c2r<512, EPI>, optin);
-    set_max_smem((const void*)k_rowr_c2r<1024, EPI>, optin);
-    set_max_smem((const void*)k_rowr_c2r<2048, EPI>, optin);
+#define KW_SET(m) set_max_smem((const void*)k_rowr_c2r<m, EPI>, optin);
+    KW_REG_ROW_SIZES(KW_SET)
+#undef KW_SET
 }
 
 void init_rowr_attributes(int optin) {
@@ -309,14 +304,10 @@ void launch_rowr_r2c(cudaStream_t st, const SimDev* d_sims, const int* d_t, cons
                      const RowR2CJob& job, int M) {
     if (nmap <= 0) return;
     switch (M) {
-        case 16: k_rowr_r2c<16><<<nmap, 256, 0, st>>>(d_sims, d_t, map, nmap, job); break;
-        case 32: k_rowr_r2c<32><<<nmap, 256, 0, st>>>(d_sims, d_t, map, nmap, job); break;
-        case 64: k_rowr_r2c<64><<<nmap, 256, 0, st>>>(d_sims, d_t, map, nmap, job); break;
-        case 128: k_rowr_r2c<128><<<nmap, 256, 0, st>>>(d_sims, d_t, map, nmap, job); break;
-        case 256: k_rowr_r2c<256><<<nmap, 256, 0, st>>>(d_sims, d_t, map, nmap, job); break;
-        case 512: k_rowr_r2c<512><<<nmap, 256, 0, st>>>(d_sims, d_t, map, nmap, job); break;
-        case 1024: k_rowr_r2c<1024><<<nmap, 256, 0, st>>>(d_sims, d_t, map, nmap, job); break;
-        case 2048: k_rowr_r2c<2048><<<nmap, 256, 0, st>>>(d_sims, d_t, map, nmap, job); break;
+#define KW_CASE(m) \
+    case m: k_rowr_r2c<m><<<nmap, 256, 0, st>>>(d_sims, d_t, map, nmap, job); break;
+        KW_REG_ROW_SIZES(KW_CASE)
+#undef KW_CASE
         default: break;
     }
 }
@@ -341,14 +332,10 @@ void launch_rowr_c2r(cudaStream_t st, const SimDev* d_sims, const int* d_t, cons
                      const RowC2RJob& job, int M) {
     if (nmap <= 0) return;
     switch (M) {
-        case 16: launch_c2r_m<16>(st, d_sims, d_t, map, nmap, job); break;
-        case 32: launch_c2r_m<32>(st, d_sims, d_t, map, nmap, job); break;
-        case 64: launch_c2r_m<64>(st, d_sims, d_t, map, nmap, job); break;
-        case 128: launch_c2r_m<128>(st, d_sims, d_t, map, nmap, job); break;
-        case 256: launch_c2r_m<256>(st, d_sims, d_t, map, nmap, job); break;
-        case 512: launch_c2r_m<512>(st, d_sims, d_t, map, nmap, job); break;
-        case 1024: launch_c2r_m<1024>(st, d_sims, d_t, map, nmap, job); break;
-        case 2048: launch_c2r_m<2048>(st, d_sims, d_t, map, nmap, job); break;
+#define KW_CASE(m) \
+    case m: launch_c2r_m<m>(st, d_sims, d_t, map, nmap, job); break;
+        KW_REG_ROW_SIZES(KW_CASE)
+#undef KW_CASE
         default: break;
     }
 }

@@ -34,8 +34,8 @@ static PFN_cuTensorMapEncodeTiled_v12000 encode_tiled() {
 
 // true when the column pass along `layout_axis` runs the TMA-fed kernel for this simulation
 bool colp_enabled(const SimHost& h, int layout_axis) {
-    if (layout_axis == 0) return h.dim == 3 && has_two_stage_col(h.A);
-    return h.dim >= 2 && has_two_stage_col(h.B);
+    if (layout_axis == 0) return h.dim == 3 && has_colp(h.A);
+    return h.dim == 3 && has_colp(h.B);
 }
 
 void Engine::build_tensor_maps(SimHost& h, SimDev& v) {

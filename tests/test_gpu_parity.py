@@ -137,6 +137,41 @@ def test_odd_sizes_and_generic_radix():
     compare(run_gpu(b), ref)
 
 
+def _reg_case(shape, seed, pml):
+    """Heterogeneous nonlinear power-law case with an additive plane source, for the kernel lengths
+    of the register-resident passes (radix-12 and long power-of-two lines)."""
+    rng = np.random.default_rng(seed)
+    dim = len(shape)
+    dx = 1e-4
+    c = (1500 + 60 * rng.standard_normal(shape)).astype(np.float32)
+    rho = (1000 + 40 * rng.standard_normal(shape)).astype(np.float32)
+    args = []
+    for n in shape:
+        args += [n, dx]
+    g = KWaveGrid(*args)
+    g.makeTime(float(c.max()), cfl=0.3)
+    g.setTime(40, g.dt)
+    pm = np.zeros(shape, np.float32)
+    sl = tuple([slice(pml + 1, n - pml - 1) for n in shape[:-1]] + [pml + 2])
+    pm[sl] = 1
+    sig = (toneBurst(1 / g.dt, 2e6, 2) * 1e5).astype(np.float32)
+    sm = np.zeros(shape, np.float32)
+    sm[tuple([slice(None)] * (dim - 1) + [pml + 8])] = 1   # within reach of the source in 40 steps
+    med = KWaveMedium(c, rho, alphaCoeff=0.5, alphaPower=1.5, alphaMode=1, bOnA=5.0)
+    return DescBuilder(g, med, KWaveSource(pMask=pm, p=sig, pMode=SourceMode.additive),
+                       KWaveSensor(mask=sm, record=RecordField.p | RecordField.pFinal), SimulationOptions(pmlSize=pml))
+
+
+@pytest.mark.parametrize("shape", [(96, 192), (384, 48), (1024, 64), (32, 4096), (48, 24, 96), (24, 192, 40),
+                                   (16, 32, 32)])
+def test_register_plan_lengths(shape):
+    # radix-12 plans (24 ... 768), long rows (C = 4096: half length 2048) and long operator
+    # columns (1024); in 3D the TMA-fed in-place pass runs along B
+    b = _reg_case(shape, sum(shape), 6)
+    ref, _ = oracle.run(b)
+    compare(run_gpu(b), ref)
+
+
 def test_batch_equals_individual_runs():
     rng = np.random.default_rng(3)
     builders = []
