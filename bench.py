@@ -135,6 +135,8 @@ def run_reference(args) -> None:
     if rank != 0:
         return
     threads = os.cpu_count() or 1
+    if args.workload == BATCH:
+        return run_reference_batch(args, threads)
     b = workload(args.workload, 1)
     steps = max(1, min(args.steps or args.ref_steps, args.ref_steps))
     r = cpu_sample(b, steps, threads)
@@ -150,6 +152,144 @@ def run_reference(args) -> None:
         "e2e": {"value": r["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
+
+
+BATCH = "batch2d_64"
+
+
+def run_reference_batch(args, threads: int) -> None:
+    """The FP64 oracle on this host over a bounded sample of the batch: the first steps of one
+    simulation of each grid size."""
+    from kwave import workloads
+    builders = workloads.batch2d()
+    seen, work, secs = set(), 0.0, 0.0
+    steps = max(1, min(args.steps or args.ref_steps, args.ref_steps)) * 5
+    for b in builders:
+        n = b.grid.shape[0]
+        if n in seen:
+            continue
+        seen.add(n)
+        r = cpu_sample(b, steps, threads)
+        work += b.grid.totalGridPoints * steps
+        secs += r["seconds"]
+    value = work / secs
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": steps, "warmup": 0, "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": BATCH, "sims": len(builders), "sizes": sorted(seen), "l2": "small grids (L2-resident)"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+                         "sample": f"first {steps} steps of one simulation per grid size {sorted(seen)}, FP64, "
+                                   f"{threads} threads, time loop only"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_batch(args) -> None:
+    """C3: 64 independent uneven 2D forwards, all in one engine (one launch per pass and size class,
+    the steady step a CUDA graph) against the same 64 run one after another through the
+    single-simulation path. Work = sum over simulations of grid points x time steps."""
+    import torch
+
+    from kwave import workloads
+    from kwave.runtime import Context
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    builders = workloads.batch2d()
+    W = args.warmup
+    work = float(sum(b.grid.totalGridPoints * b.grid.nt for b in builders))
+    ctx = Context(local)
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    ctx.set_stream(stream.cuda_stream)
+
+    def ev():
+        return torch.cuda.Event(enable_timing=True)
+
+    # batched: warm up W steps, restart, then time the whole batch (max nt steps)
+    batch = ctx.create_batch(builders)
+    batch.step(W)
+    batch.reset()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    gpu_id = "GPU-" + str(torch.cuda.get_device_properties(local).uuid)
+    steps = max(b.grid.nt for b in builders)
+    e0, e1 = ev(), ev()
+    with ClockSampler(gpu_id) as clk:
+        e0.record(stream)
+        batch.step(steps)
+        e1.record(stream)
+        torch.cuda.synchronize()
+    ms_batch = e0.elapsed_time(e1)
+    batch.close()
+
+    # plain: one simulation at a time (each warmed up W steps, reset, then timed over its nt steps)
+    ms_plain = 0.0
+    for b in builders:
+        sim = ctx.create_sim(b)
+        sim.step(W)
+        sim.reset()
+        torch.cuda.synchronize()
+        a, z = ev(), ev()
+        a.record(stream)
+        sim.step(b.grid.nt)
+        z.record(stream)
+        torch.cuda.synchronize()
+        ms_plain += a.elapsed_time(z)
+        sim.close()
+
+    # end to end through the public API from host buffers: create + run + sensor data, batched
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    batch = ctx.create_batch(builders)
+    batch.run()
+    outs = [batch.output(i, "p", b.grid.nt, 256) for i, b in enumerate(builders)]
+    t1 = time.perf_counter()
+    batch.close()
+    h2d = sum(sum(a.nbytes for a in b.keep) for b in builders)
+    d2h = sum(o.nbytes for o in outs if o is not None)
+
+    if dist:
+        t = torch.tensor([ms_batch, ms_plain], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_batch, ms_plain = float(t[0]), float(t[1])
+    if rank == 0:
+        peak, peak_kind = measured_peak_gbs()
+        sizes = sorted({b.grid.shape[0] for b in builders})
+        value = work * world / (ms_batch / 1e3)
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": steps, "warmup": W,
+            "ms_per_step": ms_batch / steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32", "data": "synthetic",
+            "config": {"workload": BATCH, "sims": len(builders), "sizes": sizes,
+                       "grid_pt_steps": work, "l2": "small grids (each simulation's fields are L2-resident)",
+                       "parallelism": f"replicas{world}"},
+            "plain": {"value": work * world / (ms_plain / 1e3), "unit": UNIT, "ms": ms_plain,
+                      "what": "the same simulations run one after another through the single-simulation path"},
+            "batched_over_plain": ms_plain / ms_batch,
+            "roofline": None,
+            "cpu_baseline": None,
+            "e2e": {"value": work * world / (t1 - t0), "unit": UNIT, "h2d_bytes_per_step": h2d / steps,
+                    "d2h_bytes_per_step": d2h / steps, "seconds": t1 - t0},
+            "clocks": clk.summary(),
+            "peak_gbs": peak, "peak_source": peak_kind,
+        }
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
 
 
 def run_ours(args) -> None:
@@ -306,6 +446,8 @@ def main() -> None:
         args.warmup = 3
     if args.impl == "reference":
         run_reference(args)
+    elif args.workload == BATCH:
+        run_batch(args)
     else:
         run_ours(args)
 
