@@ -307,6 +307,46 @@ KW_API int kw_batch_output_size(const kw_batch* batch, int index, int field, siz
 KW_API int kw_batch_get_output(kw_batch* batch, int index, int field, float* dst, size_t count);
 KW_API void kw_batch_destroy(kw_batch* batch);
 
+/* ---- adjoint gradient of a sensor-data misfit --------------------------------------------------
+ * Gradients of L = 1/2 sum_t sum_q (p_q(t) - data_q(t))^2 (p_q: the pressure the forward
+ * kw_sim_run records at sensor point q) with respect to the sound speed c0 (one value per grid
+ * point) and the initial pressure p0, by the exact discrete adjoint of the time step: every
+ * operator of the step transposed in reverse order. The reference has no adjoint; this is the
+ * kspaceFirstOrderAdjoint entry a Swift adapter would expose next to kspaceFirstOrder
+ * (Sources/KWave/Solver/KSpaceFirstOrder.swift:79-107 is the forward it differentiates).
+ * The reverse sweep needs the forward states in reverse order; they are recomputed segment by
+ * segment from checkpoints (policy below). c_ref (kappa, PML) and dt are held fixed.
+ * Supported: 1D/2D/3D, heterogeneous c0/rho0, lossless / Stokes / power law (with or without
+ * dispersion), B/A, source.p0 and k-space corrected additive pressure sources, binary or
+ * Cartesian sensors. KW_ERR_UNSUPPORTED: velocity sources, Dirichlet or uncorrected pressure
+ * sources, directivity, smoothC0 / smoothRho0 maps, grad_p0 with smoothP0, grad_rho0. */
+typedef enum kw_checkpoint_policy {
+    KW_CHECKPOINT_SQRT = 0,      /* ceil(sqrt(nt)) steps between checkpoints, segments recomputed */
+    KW_CHECKPOINT_INTERVAL = 1,  /* checkpoint_interval steps between checkpoints */
+    KW_CHECKPOINT_BUDGET = 2,    /* keep every state when that fits memory_budget bytes, else the
+                                    interval that needs the least memory */
+    KW_CHECKPOINT_STORE_ALL = 3  /* keep every state of the forward run (no recompute) */
+} kw_checkpoint_policy;
+
+typedef struct kw_adjoint_desc {
+    int abi_version;              /* KW_ABI_VERSION */
+    const float* data;            /* observed sensor pressure [n_sensor][nt], the p output's layout */
+    int policy;                   /* kw_checkpoint_policy */
+    int checkpoint_interval;      /* KW_CHECKPOINT_INTERVAL */
+    double memory_budget;         /* KW_CHECKPOINT_BUDGET, bytes of device memory for states */
+    float* grad_c0;               /* out: dL/dc0 on the grid (same layout as sound_speed), or NULL */
+    float* grad_p0;               /* out: dL/dp0 on the grid, or NULL (needs source.p0) */
+    float* grad_rho0;             /* must be NULL (not implemented) */
+    double misfit;                /* out: L */
+    double forward_ms;            /* out: device time of the forward run that stores checkpoints */
+    double reverse_ms;            /* out: device time of the reverse sweep (recompute included) */
+    int interval;                 /* out: steps between checkpoints actually used */
+    int checkpoints;              /* out: stored checkpoints (0 when every state was kept) */
+} kw_adjoint_desc;
+
+KW_API void kw_adjoint_desc_init(kw_adjoint_desc* adj);
+KW_API int kw_adjoint_run(kw_context* ctx, const kw_sim_desc* desc, kw_adjoint_desc* adj);
+
 #ifdef __cplusplus
 }
 #endif

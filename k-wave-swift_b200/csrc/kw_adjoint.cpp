@@ -1,0 +1,277 @@
+// kw_adjoint.cpp — host orchestration of the discrete adjoint (equations in kw_adjoint.cu).
+//
+// 1. Forward run of the simulation (sensor p recorded), storing a checkpoint of the state after
+//    every `interval`-th step (u_a, rho_a, S, p, div and S of the step before), or, with
+//    KW_CHECKPOINT_STORE_ALL, the reverse sweep's inputs of every step.
+// 2. Residuals r_t = p_sensor(t) - data(t) and the misfit on the host (FP64).
+// 3. Reverse sweep, segment by segment from the last: restore the segment's checkpoint, rerun its
+//    steps storing p, S, div (absorption) and u_a (B/A) of each step, then walk the segment
+//    backwards through the reverse step. The spectral pieces of a reverse step are ordinary jobs
+//    of the pass kernels (FS_ADJ fields): the transposed absorption filters, D-_a u_a for the B/A
+//    term, the source filter, D+_a and D-_a.
+// 4. The t = 0 override of an initial pressure gives dL/dp0 and its share of dL/dc0.
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "kw_adjoint.h"
+#include "kw_engine.h"
+
+namespace kw {
+
+static KwError err(int code, const std::string& m) { return KwError{code, m}; }
+
+void Engine::adjoint(const kw_sim_desc& din, kw_adjoint_desc& a) {
+    if (a.abi_version != KW_ABI_VERSION) throw err(KW_ERR_INVALID, "adjoint descriptor abi_version mismatch");
+    if (!a.data) throw err(KW_ERR_INVALID, "adjoint: data is required");
+    if (a.grad_rho0) throw err(KW_ERR_UNSUPPORTED, "adjoint: the density gradient is not implemented");
+    if (din.u_mask) throw err(KW_ERR_UNSUPPORTED, "adjoint: velocity sources are not supported");
+    if (din.p_mask && din.p.data && din.p_mode != KW_SOURCE_ADDITIVE)
+        throw err(KW_ERR_UNSUPPORTED, "adjoint: only the k-space corrected additive pressure source is supported");
+    if (din.directivity_angle) throw err(KW_ERR_UNSUPPORTED, "adjoint: directivity is not supported");
+    if ((din.smooth_c0 && din.sound_speed.len > 1) || (din.smooth_rho0 && din.density.len > 1))
+        throw err(KW_ERR_UNSUPPORTED, "adjoint: smoothC0 / smoothRho0 maps are not supported");
+    if (a.grad_p0 && !din.p0) throw err(KW_ERR_INVALID, "adjoint: grad_p0 needs source.p0");
+    if (a.grad_p0 && din.smooth_p0) throw err(KW_ERR_UNSUPPORTED, "adjoint: grad_p0 with smoothP0 is not supported");
+    if (din.sensor_kind != KW_SENSOR_BINARY && din.sensor_kind != KW_SENSOR_CARTESIAN)
+        throw err(KW_ERR_INVALID, "adjoint: a sensor is required");
+    kw_sim_desc d = din;
+    d.record = KW_RECORD_P;   // the reverse sweep reads the p series only
+    create(&d, 1);
+    SimHost& h = sims_[0];
+    SimDev& v = h.dev;
+    const int D = h.dim, nt = h.nt;
+    const long long N = h.N;
+    const size_t fb = (size_t)N * sizeof(float);
+    const int npts = v.sensor.npts;
+    if (npts <= 0) throw err(KW_ERR_INVALID, "adjoint: the sensor has no points");
+    const bool absorb = v.absorb >= 1, powerlaw = v.absorb >= 2, disp = v.absorb == 3, nonlin = v.nonlinear != 0;
+    const bool has_p0 = v.has_p0 != 0;
+    const bool psrc = v.has_p && v.psrc.mode == KW_SOURCE_ADDITIVE;
+    float y = std::isnan(d.alpha_power) ? 1.5f : (float)d.alpha_power;
+    if (d.alpha_mode == KW_ABSORPTION_STOKES) y = 2.f;
+
+    // ---- work fields ----
+    for (int k = 0; k < ADJ_COUNT; ++k) v.adj[k] = (float*)dalloc(fb);
+    double* gc = (double*)dalloc((size_t)N * sizeof(double));
+    check(cudaMemcpyAsync(d_sims_, &v, sizeof(SimDev), cudaMemcpyHostToDevice, st()), "upload sim");
+
+    // ---- checkpoint policy ----
+    const int ck_fields = 2 * D + 3 + (absorb ? 1 : 0);   // u_a, rho_a, S, p, S(t-1), div
+    const int tp_fields = 2 + (absorb ? 1 : 0) + (nonlin ? D : 0);   // p, S, div, u_a
+    bool store_all = a.policy == KW_CHECKPOINT_STORE_ALL;
+    int K = 1;
+    if (a.policy == KW_CHECKPOINT_SQRT) K = (int)std::ceil(std::sqrt((double)nt));
+    else if (a.policy == KW_CHECKPOINT_INTERVAL) K = a.checkpoint_interval;
+    else if (a.policy == KW_CHECKPOINT_BUDGET) {
+        const double all = (double)nt * tp_fields * fb;
+        if (all <= a.memory_budget) store_all = true;
+        else {
+            // memory(K) = ceil(nt / K) checkpoints + K tape slots
+            double best = 1e300;
+            for (int k = 1; k <= nt; ++k) {
+                const double m = (double)((nt + k - 1) / k) * ck_fields * fb + (double)k * tp_fields * fb;
+                if (m < best) { best = m; K = k; }
+            }
+            if (best > a.memory_budget) throw err(KW_ERR_OOM, "adjoint: the smallest checkpoint schedule needs more than memory_budget");
+        }
+    } else if (!store_all) throw err(KW_ERR_INVALID, "adjoint: unknown checkpoint policy");
+    if (store_all) K = nt;
+    if (K < 1 || K > nt) throw err(KW_ERR_INVALID, "adjoint: checkpoint_interval must be in [1, nt]");
+    const int nck = store_all ? 0 : (nt + K - 1) / K;
+    a.interval = K;
+    a.checkpoints = nck;
+
+    // tape: K slots of tp_fields fields; checkpoints: nck of ck_fields fields
+    auto alloc_fields = [&](size_t count) {
+        std::vector<float*> f(count);
+        for (auto& x : f) x = (float*)dalloc(fb);
+        return f;
+    };
+    std::vector<float*> tape = alloc_fields((size_t)K * tp_fields);
+    std::vector<float*> ck = alloc_fields((size_t)nck * ck_fields);
+    auto tslot = [&](int slot, int f) { return tape[(size_t)slot * tp_fields + f]; };   // f: 0 p, 1 S, 2 div, then u_a
+    const int TF_DIV = 2, TF_U = absorb ? 3 : 2;
+    auto ckf = [&](int c, int f) { return ck[(size_t)c * ck_fields + f]; };   // u_a, rho_a, S, p, S(t-1), div
+    auto cpy = [&](float* dst, const float* src) {
+        check(cudaMemcpyAsync(dst, src, fb, cudaMemcpyDeviceToDevice, st()), "adjoint copy");
+    };
+    auto zero = [&](float* x) { check(cudaMemsetAsync(x, 0, fb, st()), "adjoint zero"); };
+    auto tape_now = [&](int slot) {
+        cpy(tslot(slot, 0), v.p);
+        cpy(tslot(slot, 1), v.rho_sum);
+        if (absorb) cpy(tslot(slot, TF_DIV), v.div_term);
+        if (nonlin) for (int b = 0; b < D; ++b) cpy(tslot(slot, TF_U + b), v.u[b]);
+    };
+
+    cudaEvent_t e0, e1, e2;
+    check(cudaEventCreate(&e0), "event");
+    check(cudaEventCreate(&e1), "event");
+    check(cudaEventCreate(&e2), "event");
+
+    // ---- 1. forward ----
+    reset();
+    check(cudaEventRecord(e0, st()), "event");
+    std::vector<float*> sprev_all;   // store-all: S(t-1) of step 0 is zero
+    for (int t = 0; t < nt; ++t) {
+        const bool ck_step = !store_all && t % K == 0;
+        if (ck_step) {
+            const int c = t / K;
+            if (t == 0) zero(ckf(c, 2 * D + 2));
+            else cpy(ckf(c, 2 * D + 2), v.rho_sum);
+        }
+        step(1);
+        if (ck_step) {
+            const int c = t / K;
+            for (int b = 0; b < D; ++b) { cpy(ckf(c, b), v.u[b]); cpy(ckf(c, D + b), v.rho[b]); }
+            cpy(ckf(c, 2 * D), v.rho_sum);
+            cpy(ckf(c, 2 * D + 1), v.p);
+            if (absorb) cpy(ckf(c, 2 * D + 3), v.div_term);
+        }
+        if (store_all) tape_now(t);
+    }
+    check(cudaEventRecord(e1, st()), "event");
+
+    // ---- 2. residuals and misfit ----
+    std::vector<float> ps((size_t)nt * npts);
+    check(cudaMemcpyAsync(ps.data(), v.sensor.p_series, ps.size() * sizeof(float), cudaMemcpyDeviceToHost, st()), "series");
+    check(cudaStreamSynchronize(st()), "sync");
+    check_kernel_error();
+    std::vector<float> resid((size_t)nt * npts);   // [t][q]
+    double L = 0;
+    for (int t = 0; t < nt; ++t)
+        for (int q = 0; q < npts; ++q) {
+            const double r = (double)ps[(size_t)t * npts + q] - (double)a.data[(size_t)q * nt + t];
+            resid[(size_t)t * npts + q] = (float)r;
+            L += 0.5 * r * r;
+        }
+    a.misfit = L;
+    float* d_resid = upload(resid);
+
+    // ---- 3. reverse sweep ----
+    for (int k = 0; k < ADJ_COUNT; ++k) zero(v.adj[k]);
+    check(cudaMemsetAsync(gc, 0, (size_t)N * sizeof(double), st()), "zero");
+    AdjStepArgs A{};
+    A.pt = v.adj[ADJ_PT];
+    A.st = v.adj[ADJ_ST];
+    A.sprev = v.adj[ADJ_SPREV];
+    A.divt = v.adj[ADJ_DIVT];
+    A.a1 = v.adj[ADJ_A1];
+    A.a2 = v.adj[ADJ_A2];
+    A.q1 = v.adj[ADJ_Q1];
+    A.q2 = v.adj[ADJ_Q2];
+    A.lam_p = v.adj[ADJ_LP];
+    for (int b = 0; b < kMaxComp; ++b) {
+        const int bb = b < D ? b : 0;
+        A.dd[b] = v.adj[ADJ_DD + bb];
+        A.lam_u[b] = v.adj[ADJ_LU + bb];
+        A.lam_r[b] = v.adj[ADJ_LR + bb];
+        A.w[b] = v.adj[ADJ_W + bb];
+        A.e[b] = v.adj[ADJ_E + bb];
+    }
+    A.gc = gc;
+    A.y = y;
+
+    auto job = [&](int in, int out, int nin, auto opf, const char* name) {
+        SpecJob j;
+        j.in_field = FS_ADJ + in;
+        j.nin = nin;
+        j.nout = nin;
+        for (int c = 0; c < nin; ++c) j.op[c] = opf(c);
+        j.spec_in = 0;
+        j.spec_out = 0;
+        j.epi = EPI_STORE;
+        j.out_field = FS_ADJ + out;
+        j.name = name;
+        issue_job(j, -1);
+    };
+    auto radial = [](int r) { return [r](int c) { return OpSpec{AO_NONE, 0, (int8_t)r, (int8_t)c}; }; };
+    auto deriv = [](int ao) { return [ao](int c) { return OpSpec{(int8_t)ao, (int8_t)c, RT_KAPPA, (int8_t)c}; }; };
+
+    // one reverse step t: tape slot `slot`, S(t-1) in `sprev` (nullptr: zero state before step 0)
+    auto reverse_step = [&](int t, int slot, const float* sprev) {
+        launch_set_step(st(), d_t_, t);   // the pass kernels gate on t < nt
+        launch_adj_residual(st(), d_sims_, npts, d_resid, t, v.adj[ADJ_LP]);
+        cpy(v.adj[ADJ_PT], tslot(slot, 0));
+        cpy(v.adj[ADJ_ST], tslot(slot, 1));
+        if (sprev) cpy(v.adj[ADJ_SPREV], sprev);
+        else zero(v.adj[ADJ_SPREV]);
+        if (absorb) cpy(v.adj[ADJ_DIVT], tslot(slot, TF_DIV));
+        if (powerlaw) {
+            launch_adj_pre(st(), d_sims_, N, v.adj[ADJ_LP], v.adj[ADJ_X1], v.adj[ADJ_X2]);
+            job(ADJ_X1, ADJ_A1, 2, radial(RT_NU1), "adj_nu1");
+            if (disp) job(ADJ_X2, ADJ_A2, 2, radial(RT_NU2), "adj_nu2");
+        }
+        if (nonlin) {
+            for (int b = 0; b < D; ++b) cpy(v.adj[ADJ_UT + b], tslot(slot, TF_U + b));
+            job(ADJ_UT, ADJ_DD, D, deriv(AO_DNEG), "adj_du");
+        }
+        const bool src_on = psrc && t < v.psrc.len;
+        A.sig = src_on ? v.adj[ADJ_SIG] : nullptr;
+        launch_adj_eos(st(), d_sims_, N, A);
+        if (src_on) {
+            job(ADJ_SIG, ADJ_GSIG, 1, radial(RT_SKAPPA), "adj_src");
+            launch_adj_src(st(), d_sims_, v.psrc.nsrc, v.adj[ADJ_GSIG], t, gc);
+        }
+        job(ADJ_W, ADJ_E, D, deriv(AO_DPOS), "adj_dpos");
+        launch_adj_vel(st(), d_sims_, N, A);
+        job(ADJ_W, ADJ_E, D, deriv(AO_DNEG), "adj_dneg");
+        launch_adj_sum(st(), d_sims_, N, A);
+    };
+
+    const int t_stop = has_p0 ? 1 : 0;
+    if (store_all) {
+        for (int t = nt - 1; t >= t_stop; --t) reverse_step(t, t, t > 0 ? tslot(t - 1, 1) : nullptr);
+    } else {
+        for (int c = nck - 1; c >= 0; --c) {
+            const int t0 = c * K, t1 = std::min(t0 + K, nt);
+            if (t1 - 1 < t_stop) continue;
+            // restore the state after step t0 and rerun the segment, storing each step
+            for (int b = 0; b < D; ++b) { cpy(v.u[b], ckf(c, b)); cpy(v.rho[b], ckf(c, D + b)); }
+            cpy(v.rho_sum, ckf(c, 2 * D));
+            cpy(v.p, ckf(c, 2 * D + 1));
+            if (absorb) cpy(v.div_term, ckf(c, 2 * D + 3));
+            tape_now(0);
+            launch_set_step(st(), d_t_, t0 + 1);
+            t_ = t0 + 1;
+            for (int t = t0 + 1; t < t1; ++t) {
+                step(1);
+                tape_now(t - t0);
+            }
+            for (int t = t1 - 1; t >= std::max(t0, t_stop); --t)
+                reverse_step(t, t - t0, t > t0 ? tslot(t - t0 - 1, 1) : (t > 0 ? ckf(c, 2 * D + 2) : nullptr));
+        }
+    }
+    if (has_p0) {
+        // t = 0 override: p = p0, rho_a = p0 / (D c^2), u_a = dtor_a / 2 D+_a p0
+        launch_set_step(st(), d_t_, 0);
+        launch_adj_residual(st(), d_sims_, npts, d_resid, 0, v.adj[ADJ_LP]);
+        launch_adj_half_dtor(st(), d_sims_, N, A);
+        job(ADJ_W, ADJ_E, D, deriv(AO_DNEG), "adj_p0");
+        float* gp = a.grad_p0 ? v.adj[ADJ_GSIG] : nullptr;
+        launch_adj_p0(st(), d_sims_, N, A, h.p0s, gp);
+        if (gp) {
+            check(cudaMemcpyAsync(a.grad_p0, gp, fb, cudaMemcpyDeviceToHost, st()), "grad p0");
+        }
+    } else if (a.grad_p0) {
+        std::memset(a.grad_p0, 0, fb);
+    }
+    check(cudaEventRecord(e2, st()), "event");
+    if (a.grad_c0) {
+        launch_adj_store_grad(st(), gc, v.adj[ADJ_SIG], N);
+        check(cudaMemcpyAsync(a.grad_c0, v.adj[ADJ_SIG], fb, cudaMemcpyDeviceToHost, st()), "grad c0");
+    }
+    check(cudaGetLastError(), "adjoint launch");
+    check(cudaStreamSynchronize(st()), "adjoint sync");
+    check_kernel_error();
+    float f_ms = 0, r_ms = 0;
+    cudaEventElapsedTime(&f_ms, e0, e1);
+    cudaEventElapsedTime(&r_ms, e1, e2);
+    a.forward_ms = f_ms;
+    a.reverse_ms = r_ms;
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaEventDestroy(e2);
+}
+
+}  // namespace kw

@@ -1,0 +1,200 @@
+// kw_adjoint.cu — pointwise and sparse kernels of the discrete adjoint of the time step
+// (host orchestration in kw_adjoint.cpp; the spectral operators run through the ordinary pass
+// kernels with FS_ADJ fields).
+//
+// Forward step t (kw_engine.cpp issue_step), per grid point, with d_a = D+_a p(t-1) for the
+// velocity and d_a = D-_a u_a(t) for the density (D+-_a = Re F^-1(i k_a e^{+-i k_a dx_a/2} kappa F .)):
+//   u_a   = sg_a (sg_a u_a - dtor_a D+_a p(t-1))
+//   rho_a = pm_a (pm_a rho_a - dt rho0 nl d_a),   nl = (2 S(t-1) + rho0) / rho0 (B/A) or 1
+//   rho_a += (1 / dx_a) G(src),  G = Re F^-1(cos(c_ref dt |k| / 2) F .),  src = sig 2 dt / (D c) at the mask
+//   S = sum_a rho_a,  div = rho0 sum_a d_a
+//   p = c^2 (S + tau A1(div) - eta A2(S) + B/A S^2 / (2 rho0))   (power law; Stokes: tau div)
+// Reverse (lambda_x = dL/dx of the state after step t):
+//   lambda_p += Sample^T r_t
+//   dL/dc  += lambda_p (2 p / c + c ((y-1) tau A1(div) - y eta A2(S)))      (Stokes: + c tau div)
+//   lE = c^2 lambda_p;  lS = lE + lE B/A S / rho0 - A2(eta lE);  ldiv = A1(tau lE) (Stokes: tau lE)
+//   L_a = lambda_rho_a + lS;  source: dL/dc_i += G(sum_a L_a / dx_a)_i sig (-scale_i / c_i)
+//   w_a = rho0 ldiv - pm_a dt rho0 nl L_a
+//   lambda_rho_a <- pm_a^2 L_a - 2 dt sum_b pm_b d_b L_b   (the B/A term through nl)
+//   mu_a = lambda_u_a - D+_a w_a                            ((D-_a)^T = -D+_a)
+//   lambda_u_a <- sg_a^2 mu_a;  lambda_p <- sum_a D-_a(sg_a dtor_a mu_a)
+#include "kw_adjoint.h"
+#include "kw_device.cuh"
+
+namespace kw {
+
+__device__ __forceinline__ int layout_coord(const SimDev& S, long long i, int a) {
+    const int L = a + 3 - S.dim;
+    const long long ic = i % S.C;
+    const long long r = i / S.C;
+    const int ib = (int)(r % S.B);
+    const int ia = (int)(r / S.B);
+    return L == 0 ? ia : (L == 1 ? ib : (int)ic);
+}
+
+__global__ void k_set_step(int* d_t, int t) { *d_t = t; }
+
+// lambda_p += Sample^T r_t (binary: one point; Cartesian: multilinear corners, which can coincide)
+__global__ void k_adj_residual(const SimDev* __restrict__ sims, const float* __restrict__ resid, int t,
+                               float* __restrict__ lam_p) {
+    const SimDev& S = sims[0];
+    const SensorDev& sn = S.sensor;
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= sn.npts) return;
+    const float r = resid[(long long)t * sn.npts + q];
+    for (int c = 0; c < sn.ncorners; ++c) {
+        const int i = __ldg(sn.idx + q * sn.ncorners + c);
+        const float w = sn.kind == 2 ? __ldg(sn.w + q * sn.ncorners + c) : 1.f;
+        atomicAdd(lam_p + i, w * r);
+    }
+}
+
+// inputs of the transposed absorption filters: tau c^2 lambda_p and eta c^2 lambda_p
+__global__ void k_adj_pre(const SimDev* __restrict__ sims, const float* __restrict__ lam_p, float* __restrict__ x1,
+                          float* __restrict__ x2) {
+    const SimDev& S = sims[0];
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= S.N) return;
+    const float lE = S.c2.at(i) * lam_p[i];
+    x1[i] = S.tau.at(i) * lE;
+    if (S.absorb == 3) x2[i] = S.eta.at(i) * lE;
+}
+
+__global__ void k_adj_eos(const SimDev* __restrict__ sims, AdjStepArgs A) {
+    const SimDev& S = sims[0];
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= S.N) return;
+    const int D = S.dim;
+    const float c2 = S.c2.at(i);
+    const float c = sqrtf(c2);
+    const float lp = A.lam_p[i];
+    const float sv = A.st[i];
+    const float r0 = S.rho0.at(i);
+    double dpdc = 2.0 * (double)A.pt[i] / c;
+    if (S.absorb == 1) dpdc += (double)c * S.tau.at(i) * A.divt[i];
+    if (S.absorb >= 2) dpdc += (double)c * (A.y - 1.f) * S.tau.at(i) * A.q1[i];
+    if (S.absorb == 3) dpdc -= (double)c * A.y * S.eta.at(i) * A.q2[i];
+    A.gc[i] += (double)lp * dpdc;
+    const float lE = c2 * lp;
+    float lS = lE;
+    if (S.nonlinear) lS += lE * S.bona.at(i) * sv / r0;
+    if (S.absorb == 3) lS -= A.a2[i];
+    float ldiv = 0.f;
+    if (S.absorb == 1) ldiv = S.tau.at(i) * lE;
+    else if (S.absorb >= 2) ldiv = A.a1[i];
+    const float nl = S.nonlinear ? (2.f * A.sprev[i] + r0) / r0 : 1.f;
+    const float dtr = S.dt * r0;
+    float lam[kMaxComp], pm[kMaxComp];
+    float lsprev = 0.f, sig = 0.f;
+#pragma unroll
+    for (int a = 0; a < kMaxComp; ++a) {
+        if (a >= D) break;
+        pm[a] = __ldg(S.ax[a].pml + layout_coord(S, i, a));
+        lam[a] = A.lam_r[a][i] + lS;
+        A.w[a][i] = r0 * ldiv - pm[a] * dtr * nl * lam[a];
+        if (S.nonlinear) lsprev += -2.f * S.dt * pm[a] * A.dd[a][i] * lam[a];
+        sig += lam[a] * S.ax[a].inv_d;
+    }
+#pragma unroll
+    for (int a = 0; a < kMaxComp; ++a) {
+        if (a >= D) break;
+        A.lam_r[a][i] = pm[a] * pm[a] * lam[a] + lsprev;
+    }
+    if (A.sig) A.sig[i] = sig;
+}
+
+// dL/dc at the additive source points: G(sigma)_i sig (-scale_i / c_i)
+__global__ void k_adj_src(const SimDev* __restrict__ sims, const float* __restrict__ gsig, int t, double* __restrict__ gc) {
+    const SimDev& S = sims[0];
+    const SourceDev& s = S.psrc;
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= s.nsrc || t >= s.len) return;
+    const float sg = __ldg(s.signal + (long long)(s.rows == 1 ? 0 : q) * s.len + t);
+    const int i = __ldg(s.idx + q);
+    const float c = sqrtf(S.c2.at(i));
+    gc[i] += (double)gsig[i] * sg * (-(double)__ldg(s.scale[0] + q) / c);
+}
+
+// mu_a = lambda_u_a - e_a; lambda_u_a <- sg_a^2 mu_a; w_a <- sg_a dtor_a mu_a
+__global__ void k_adj_vel(const SimDev* __restrict__ sims, AdjStepArgs A) {
+    const SimDev& S = sims[0];
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= S.N) return;
+    for (int a = 0; a < S.dim; ++a) {
+        const float mu = A.lam_u[a][i] - A.e[a][i];
+        const float sg = __ldg(S.ax[a].pml_sg + layout_coord(S, i, a));
+        A.lam_u[a][i] = sg * sg * mu;
+        A.w[a][i] = sg * S.dtor[a].at(i) * mu;
+    }
+}
+
+__global__ void k_adj_sum(const SimDev* __restrict__ sims, AdjStepArgs A) {
+    const SimDev& S = sims[0];
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= S.N) return;
+    float s = A.e[0][i];
+    for (int a = 1; a < S.dim; ++a) s += A.e[a][i];
+    A.lam_p[i] = s;
+}
+
+// the t = 0 override of an initial pressure: w_a = dtor_a / 2 lambda_u_a (then e_a = D-_a w_a)
+__global__ void k_adj_half_dtor(const SimDev* __restrict__ sims, AdjStepArgs A) {
+    const SimDev& S = sims[0];
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= S.N) return;
+    for (int a = 0; a < S.dim; ++a) A.w[a][i] = (S.dtor[a].at(i) / 2.f) * A.lam_u[a][i];
+}
+
+// dL/dp0 = lambda_p + sum_a lambda_rho_a / (D c^2) + sum_a (D+_a)^T(w_a) (= - e_a);
+// dL/dc += sum_a lambda_rho_a p0 (-2 / (D c^3))
+__global__ void k_adj_p0(const SimDev* __restrict__ sims, AdjStepArgs A, const float* __restrict__ p0s,
+                         float* __restrict__ gp) {
+    const SimDev& S = sims[0];
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= S.N) return;
+    const float c2 = S.c2.at(i);
+    const float dd = S.dim == 1 ? 1.f : (float)S.dim;
+    float lrs = 0.f, es = 0.f;
+    for (int a = 0; a < S.dim; ++a) { lrs += A.lam_r[a][i]; es += A.e[a][i]; }
+    if (gp) gp[i] = A.lam_p[i] + lrs / (dd * c2) - es;
+    A.gc[i] += (double)lrs * p0s[i] * (-2.0 / ((double)dd * c2 * sqrtf(c2)));
+}
+
+__global__ void k_adj_store_grad(const double* __restrict__ gc, float* __restrict__ out, long long n) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) out[i] = (float)gc[i];
+}
+
+// ---------------------------------------------------------------------------------------------
+static unsigned blocks(long long n) { return (unsigned)((n + 255) / 256); }
+
+void launch_set_step(cudaStream_t st, int* d_t, int t) { k_set_step<<<1, 1, 0, st>>>(d_t, t); }
+void launch_adj_residual(cudaStream_t st, const SimDev* d_sims, int npts, const float* resid, int t, float* lam_p) {
+    if (npts > 0) k_adj_residual<<<blocks(npts), 256, 0, st>>>(d_sims, resid, t, lam_p);
+}
+void launch_adj_pre(cudaStream_t st, const SimDev* d_sims, long long N, const float* lam_p, float* x1, float* x2) {
+    k_adj_pre<<<blocks(N), 256, 0, st>>>(d_sims, lam_p, x1, x2);
+}
+void launch_adj_eos(cudaStream_t st, const SimDev* d_sims, long long N, const AdjStepArgs& a) {
+    k_adj_eos<<<blocks(N), 256, 0, st>>>(d_sims, a);
+}
+void launch_adj_src(cudaStream_t st, const SimDev* d_sims, int nsrc, const float* gsig, int t, double* gc) {
+    if (nsrc > 0) k_adj_src<<<blocks(nsrc), 256, 0, st>>>(d_sims, gsig, t, gc);
+}
+void launch_adj_vel(cudaStream_t st, const SimDev* d_sims, long long N, const AdjStepArgs& a) {
+    k_adj_vel<<<blocks(N), 256, 0, st>>>(d_sims, a);
+}
+void launch_adj_sum(cudaStream_t st, const SimDev* d_sims, long long N, const AdjStepArgs& a) {
+    k_adj_sum<<<blocks(N), 256, 0, st>>>(d_sims, a);
+}
+void launch_adj_half_dtor(cudaStream_t st, const SimDev* d_sims, long long N, const AdjStepArgs& a) {
+    k_adj_half_dtor<<<blocks(N), 256, 0, st>>>(d_sims, a);
+}
+void launch_adj_p0(cudaStream_t st, const SimDev* d_sims, long long N, const AdjStepArgs& a, const float* p0s, float* gp) {
+    k_adj_p0<<<blocks(N), 256, 0, st>>>(d_sims, a, p0s, gp);
+}
+void launch_adj_store_grad(cudaStream_t st, const double* gc, float* out, long long n) {
+    k_adj_store_grad<<<blocks(n), 256, 0, st>>>(gc, out, n);
+}
+
+}  // namespace kw

@@ -223,6 +223,22 @@ int kw_spectral_derivative_noalloc(kw_context* ctx, int dim, int nx, int ny, int
     });
 }
 
+void kw_adjoint_desc_init(kw_adjoint_desc* a) {
+    if (!a) return;
+    std::memset(a, 0, sizeof(*a));
+    a->abi_version = KW_ABI_VERSION;
+    a->policy = KW_CHECKPOINT_SQRT;
+}
+
+int kw_adjoint_run(kw_context* ctx, const kw_sim_desc* desc, kw_adjoint_desc* adj) {
+    if (!ctx || !desc || !adj) return KW_ERR_INVALID;
+    return guarded(ctx, [&]() {
+        kw::Engine eng(&ctx->c);
+        eng.adjoint(*desc, *adj);
+        return KW_OK;
+    });
+}
+
 int kw_batch_create(kw_context* ctx, const kw_sim_desc* descs, int count, kw_batch** out) {
     if (!ctx || !descs || count <= 0 || !out) return KW_ERR_INVALID;
     *out = nullptr;

@@ -18,6 +18,7 @@ namespace kw {
 
 constexpr int kMaxStages = 16;
 constexpr int kMaxComp = 3;
+constexpr int kAdjFields = 32;
 
 // FFT plan of one complex transform length n (a Stockham sequence of radix stages).
 struct FFTPlanDev {
@@ -184,6 +185,7 @@ struct SimDev {
     float* src_buf[kMaxComp];   // sparse scratch fields for additive sources (zero off-mask)
     float* tmp[kMaxComp];       // real scratch fields (collocated velocity etc.)
     float2* spec[4];
+    float* adj[kAdjFields];     // adjoint work fields (kw_adjoint.cpp), unused by a forward run
 
     // medium
     float dt;              // time step (FP32, multiplies rho0 like the reference's dt * rho0)

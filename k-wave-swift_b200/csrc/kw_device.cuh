@@ -26,7 +26,8 @@ __device__ __forceinline__ float* field_ptr(const SimDev& S, int sel, int comp) 
         case FS_DIV: return S.div_term;
         case FS_SRCBUF: return S.src_buf[comp];
         case FS_WORK: return comp == 0 ? S.div_term : S.rho_sum;   // power-law inputs
-        default: return S.tmp[comp];
+        case FS_TMP: return S.tmp[comp];
+        default: return S.adj[sel - FS_ADJ + comp];
     }
 }
 

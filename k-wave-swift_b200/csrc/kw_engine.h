@@ -78,6 +78,8 @@ public:
     // Standalone staggered spectral derivative of a device field (kw_derivative.cpp).
     void create_derivative(int dim, const int* n, const double* d, int axis, int shift, const float* in, float* out);
     void run_derivative();
+    // Discrete adjoint of a single simulation's misfit (kw_adjoint.cpp).
+    void adjoint(const kw_sim_desc& d, kw_adjoint_desc& a);
     // Take every device buffer from [base, base + bytes) instead of cudaMalloc (call before create).
     void set_arena(void* base, size_t bytes) {
         arena_ = static_cast<char*>(base);

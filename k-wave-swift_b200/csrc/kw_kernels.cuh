@@ -8,7 +8,8 @@ namespace kw {
 // Which real field a pass reads or writes.
 enum FieldSel {
     FS_P = 0, FS_U, FS_RHO, FS_RHO_SUM, FS_DIV, FS_SRCBUF, FS_TMP,
-    FS_WORK   // power-law absorption inputs: component 0 = rho0 div u, component 1 = rho_sum
+    FS_WORK,  // power-law absorption inputs: component 0 = rho0 div u, component 1 = rho_sum
+    FS_ADJ    // adjoint work fields: FS_ADJ + k selects adj[k + component]
 };
 
 // A launch may be gated on a source being active at the current step.

@@ -4,15 +4,15 @@ The solver runs in libkwave_cuda.so (hand-written CUDA for sm_100a behind a C AB
 include/kwave_cuda.h). This package mirrors the reference's Swift API over that ABI.
 """
 from .abi import FIELDS
-from .api import (AbsorptionMode, DescBuilder, DeviceKind, DirectivityPattern, KWaveError,
+from .api import (AbsorptionMode, AdjointOutput, DescBuilder, DeviceKind, DirectivityPattern, KWaveError,
                   KWaveGrid, KWaveMedium, KWaveSensor, KWaveSource, RecordField,
                   SimulationOptions, SimulationOutput, SourceMode, kspaceFirstOrder,
-                  wavenumberVector)
+                  kspaceFirstOrderAdjoint, wavenumberVector)
 from .shapes import gaussian, makeBall, makeCartCircle, makeCircle, makeDisc, toneBurst
 
 __all__ = [
-    "AbsorptionMode", "DescBuilder", "DeviceKind", "DirectivityPattern", "FIELDS", "KWaveError",
+    "AbsorptionMode", "AdjointOutput", "DescBuilder", "DeviceKind", "DirectivityPattern", "FIELDS", "KWaveError",
     "KWaveGrid", "KWaveMedium", "KWaveSensor", "KWaveSource", "RecordField", "SimulationOptions",
-    "SimulationOutput", "SourceMode", "gaussian", "kspaceFirstOrder", "makeBall",
+    "SimulationOutput", "SourceMode", "gaussian", "kspaceFirstOrder", "kspaceFirstOrderAdjoint", "makeBall",
     "makeCartCircle", "makeCircle", "makeDisc", "toneBurst", "wavenumberVector",
 ]

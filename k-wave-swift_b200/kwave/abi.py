@@ -103,6 +103,26 @@ class kw_kernel_timing(C.Structure):
     _fields_ = [("name", C.c_char * 48), ("ms", C.c_double), ("bytes", C.c_double)]
 
 
+class kw_adjoint_desc(C.Structure):
+    _fields_ = [
+        ("abi_version", C.c_int),
+        ("data", C.POINTER(C.c_float)),
+        ("policy", C.c_int),
+        ("checkpoint_interval", C.c_int),
+        ("memory_budget", C.c_double),
+        ("grad_c0", C.POINTER(C.c_float)),
+        ("grad_p0", C.POINTER(C.c_float)),
+        ("grad_rho0", C.POINTER(C.c_float)),
+        ("misfit", C.c_double),
+        ("forward_ms", C.c_double),
+        ("reverse_ms", C.c_double),
+        ("interval", C.c_int),
+        ("checkpoints", C.c_int),
+    ]
+
+
+KW_CHECKPOINT_SQRT, KW_CHECKPOINT_INTERVAL, KW_CHECKPOINT_BUDGET, KW_CHECKPOINT_STORE_ALL = 0, 1, 2, 3
+
 # Every symbol include/kwave_cuda.h declares, with its ctypes signature.
 P = C.c_void_p
 SIGNATURES = {
@@ -129,6 +149,8 @@ SIGNATURES = {
                                          C.c_int, C.c_int, P, P]),
     "kw_spectral_derivative_noalloc": (C.c_int, [P, C.c_int, C.c_int, C.c_int, C.c_int, C.c_double, C.c_double,
                                                  C.c_double, C.c_int, C.c_int, P, P]),
+    "kw_adjoint_desc_init": (None, [C.POINTER(kw_adjoint_desc)]),
+    "kw_adjoint_run": (C.c_int, [P, C.POINTER(kw_sim_desc), C.POINTER(kw_adjoint_desc)]),
     "kw_batch_create": (C.c_int, [P, C.POINTER(kw_sim_desc), C.c_int, C.POINTER(P)]),
     "kw_batch_run": (C.c_int, [P, C.POINTER(kw_callbacks)]),
     "kw_batch_reset": (C.c_int, [P]),

@@ -80,6 +80,27 @@ class Context:
     def create_batch(self, builders: Sequence[DescBuilder]) -> "Batch":
         return Batch(self, builders)
 
+    def adjoint(self, builder: DescBuilder, data: np.ndarray, grad_c0: bool = True, grad_p0: bool = False,
+                policy: int = abi.KW_CHECKPOINT_SQRT, interval: int = 0, memory_budget: float = 0.0) -> dict:
+        """kw_adjoint_run: misfit 1/2 sum (p_sensor - data)^2 and its gradients (see the header)."""
+        d = np.ascontiguousarray(data, dtype=np.float32)
+        shape = builder.shape
+        a = abi.kw_adjoint_desc()
+        self.lib.kw_adjoint_desc_init(C.byref(a))
+        a.data = d.ctypes.data_as(C.POINTER(C.c_float))
+        a.policy = int(policy)
+        a.checkpoint_interval = int(interval)
+        a.memory_budget = float(memory_budget)
+        gc = np.zeros(shape, np.float32) if grad_c0 else None
+        gp = np.zeros(shape, np.float32) if grad_p0 else None
+        if gc is not None:
+            a.grad_c0 = gc.ctypes.data_as(C.POINTER(C.c_float))
+        if gp is not None:
+            a.grad_p0 = gp.ctypes.data_as(C.POINTER(C.c_float))
+        _check(self.lib, self.h, self.lib.kw_adjoint_run(self.h, C.byref(builder.desc), C.byref(a)))
+        return {"misfit": a.misfit, "grad_c0": gc, "grad_p0": gp, "forward_ms": a.forward_ms,
+                "reverse_ms": a.reverse_ms, "interval": a.interval, "checkpoints": a.checkpoints}
+
 
 def _callbacks(progress, monitor, interval, shape):
     keep = []

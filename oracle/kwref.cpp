@@ -325,6 +325,423 @@ static vecd stagger_density(const Shape& s, const vecd& rho, int a) {
     return out;
 }
 
+/* ======================================================================================
+ * The model: everything kspaceFirstOrder precomputes before its time loop (KSFO:203-442),
+ * shared by the forward run and the discrete adjoint.
+ * ====================================================================================== */
+struct DirEntry { vecd weight; std::vector<int> rows; std::vector<size_t> gather; };
+
+struct Model {
+    Shape s;
+    size_t N = 0;
+    int ndim = 1;
+    double dt = 0;
+    int nt = 0;
+    vecd c0, rho0, c2, dtRho0;
+    double cRef = 0;
+    std::vector<vecd> kv;
+    vecd kmag, kappa, skappa;
+    std::vector<vecc> ddPos, ddNeg, colloc;
+    std::vector<vecd> pml, pmlSg, dtOverRho;
+    std::vector<SourceOp> pOp, uOp;
+    std::vector<bool> hasP, hasU;
+    bool hasP0 = false;
+    vecd p0f;
+    bool absorb = false, stokes = false, dispersion = false;
+    double y = 1.5;
+    vecd tau, eta, nabla1, nabla2;
+    bool nonlinear = false;
+    vecd bona;
+    unsigned rec = 0;
+    bool recordP = false, recordU = false, recordUFinal = false;
+    bool haveSampler = false;
+    int nPts = 0, nCorners = 1;
+    std::vector<size_t> sIdx;
+    vecd sW;
+    bool directivity = false;
+    std::vector<DirEntry> dirEntries;
+};
+
+// The fields the time loop carries (KSFO:438-442) plus the step's intermediates.
+struct State {
+    vecd p, rhoTot, divU;
+    std::vector<vecd> u, rho, dU;
+    void init(const Model& m) {
+        p.assign(m.N, 0.0);
+        rhoTot.assign(m.N, 0.0);
+        divU.assign(m.N, 0.0);
+        u.assign(m.ndim, vecd(m.N, 0.0));
+        rho.assign(m.ndim, vecd(m.N, 0.0));
+        dU.assign(m.ndim, vecd(m.N, 0.0));
+    }
+};
+
+// Re F^-1(H F x) for a full-grid multiplier H(i) (the reference's fftn(...).realPart() chain)
+template <class HF>
+static void apply_op(const Model& m, const vecd& x, vecd& out, HF H) {
+    vecc w = to_complex(x);
+    fftn(m.s, w, false);
+#pragma omp parallel for schedule(static)
+    for (long long i = 0; i < (long long)m.N; ++i) w[i] *= H((size_t)i);
+    fftn(m.s, w, true);
+    out.resize(m.N);
+    for (size_t i = 0; i < m.N; ++i) out[i] = w[i].real();
+}
+
+static int build_model(const kw_sim_desc* d, Model& m) {
+    Shape& s = m.s;
+    s.dim = d->dim;
+    if (s.dim < 1 || s.dim > 3) { g_err = "dim must be 1, 2 or 3"; return KW_ERR_INVALID; }
+    const int ns[3] = {d->nx, d->ny, d->nz};
+    const double ds[3] = {d->dx, d->dy, d->dz};
+    for (int a = 0; a < s.dim; ++a) { s.n[a] = ns[a]; s.d[a] = ds[a]; if (ns[a] < 1) { g_err = "bad size"; return KW_ERR_INVALID; } }
+    s.finish();
+    const size_t N = s.N;
+    m.N = N;
+    const int ndim = s.dim;
+    m.ndim = ndim;
+    const double dt = d->dt;
+    m.dt = dt;
+    m.nt = d->nt;
+    if (m.nt <= 0) { g_err = "call grid.makeTime(...) before running the solver"; return KW_ERR_INVALID; }
+    if (!d->p0 && !d->p_mask && !d->u_mask) { g_err = "solver requires source.p0 or a time-varying p/u source"; return KW_ERR_INVALID; }
+    if (!grid_sized(d->sound_speed, N) || !grid_sized(d->density, N)) { g_err = "soundSpeed/density must be scalar or grid-shaped"; return KW_ERR_INVALID; }
+    if (d->pml_size < 0) { g_err = "bad pml size"; return KW_ERR_INVALID; }
+    for (int a = 0; a < ndim; ++a) if (d->pml_size > s.n[a]) { g_err = "pml larger than grid"; return KW_ERR_INVALID; }
+
+    // ---- medium (KSFO:367-373) ----
+    const bool c0Map = d->sound_speed.len > 1, rho0Map = d->density.len > 1;
+    m.c0 = expand(d->sound_speed, N);
+    m.rho0 = expand(d->density, N);
+    if (d->smooth_c0 && c0Map) m.c0 = smooth_field(s, m.c0);
+    if (d->smooth_rho0 && rho0Map) m.rho0 = smooth_field(s, m.rho0);
+    const vecd& c0 = m.c0;
+    const vecd& rho0 = m.rho0;
+    double cRef = 0;
+    for (size_t i = 0; i < N; ++i) cRef = std::max(cRef, c0[i]);   // referenceSoundSpeed KSFO:786-788
+    if (!c0Map) cRef = c0[0];
+    if (!std::isnan(d->c_ref)) cRef = d->c_ref;
+    m.cRef = cRef;
+
+    // ---- k-space operators (KSFO:376-383, 764-769) ----
+    m.kv.resize(ndim);
+    for (int a = 0; a < ndim; ++a) m.kv[a] = wavenumber_vector(s.n[a], s.d[a]);
+    m.kmag.resize(N); m.kappa.resize(N); m.skappa.resize(N);
+    for (size_t i = 0; i < N; ++i) {
+        double k2 = 0;
+        for (int a = 0; a < ndim; ++a) { const double k = m.kv[a][s.idx(i, a)]; k2 += k * k; }
+        m.kmag[i] = std::sqrt(k2);
+        const double arg = m.kmag[i] * (cRef * dt / 2.0);
+        m.kappa[i] = arg == 0.0 ? 1.0 : std::sin(arg) / arg;
+        m.skappa[i] = std::cos(arg);
+    }
+    m.ddPos.resize(ndim); m.ddNeg.resize(ndim); m.colloc.resize(ndim);
+    const cd I(0, 1);
+    for (int a = 0; a < ndim; ++a) {
+        const int n = s.n[a];
+        m.ddPos[a].resize(n); m.ddNeg[a].resize(n); m.colloc[a].resize(n);
+        for (int i = 0; i < n; ++i) {
+            const double k = m.kv[a][i], th = k * (s.d[a] / 2.0);
+            m.ddPos[a][i] = I * k * (std::cos(th) + 1.0 * I * std::sin(th));
+            m.ddNeg[a][i] = I * k * (std::cos(th) - 1.0 * I * std::sin(th));
+            m.colloc[a][i] = std::cos(th) - I * std::sin(th);   // REC:101-104
+        }
+    }
+
+    // ---- PML (KSFO:385-397) ----
+    m.pml.resize(ndim); m.pmlSg.resize(ndim);
+    for (int a = 0; a < ndim; ++a) {
+        m.pml[a] = pml_profile(s.n[a], s.d[a], dt, cRef, d->pml_size, d->pml_alpha, false);
+        m.pmlSg[a] = pml_profile(s.n[a], s.d[a], dt, cRef, d->pml_size, d->pml_alpha, true);
+    }
+
+    // ---- staggered density etc. (KSFO:399-402) ----
+    m.c2.resize(N); m.dtRho0.resize(N);
+    for (size_t i = 0; i < N; ++i) { m.c2[i] = c0[i] * c0[i]; m.dtRho0[i] = dt * rho0[i]; }
+    m.dtOverRho.resize(ndim);
+    for (int a = 0; a < ndim; ++a) {
+        vecd sg = rho0Map ? stagger_density(s, rho0, a) : rho0;
+        m.dtOverRho[a].resize(N);
+        for (size_t i = 0; i < N; ++i) m.dtOverRho[a][i] = dt / sg[i];
+    }
+
+    // ---- sources (KSFO:404-423, 129-201) ----
+    const double nd = (double)ndim;
+    // makeSourceOp KSFO:192-201: no op when the mask or the signal is absent or the mask is empty.
+    auto make_op = [&](const float* mask, const kw_signal& sig, int mode, bool isP, int a, SourceOp& op) -> int {
+        if (!mask || !sig.data) return 0;
+        op.idx = flat_nonzero(mask, N);
+        if (op.idx.empty()) return 0;
+        const int rows = sig.rows, len = sig.len;
+        if ((rows != 1 && rows != (int)op.idx.size()) || len < 0) return -1;
+        op.signal.assign(rows, vecd(len));
+        for (int r = 0; r < rows; ++r)
+            for (int t = 0; t < len; ++t) op.signal[r][t] = sig.data[(size_t)r * len + t];
+        op.mode = mode;
+        op.scale.resize(op.idx.size());
+        for (size_t q = 0; q < op.idx.size(); ++q) {
+            const double c = c0[op.idx[q]];   // soundSpeedSamples KSFO:791-794
+            if (isP) op.scale[q] = mode == KW_SOURCE_DIRICHLET ? 1.0 / (nd * c * c) : 2.0 * dt / (nd * c * s.d[a]);
+            else op.scale[q] = mode == KW_SOURCE_DIRICHLET ? 1.0 : 2.0 * c * dt / s.d[a];
+        }
+        return 1;
+    };
+    m.pOp.assign(ndim, SourceOp()); m.uOp.assign(ndim, SourceOp());
+    m.hasP.assign(ndim, false); m.hasU.assign(ndim, false);
+    const kw_signal* usig[3] = {&d->ux, &d->uy, &d->uz};
+    for (int a = 0; a < ndim; ++a) {
+        const int rp = make_op(d->p_mask, d->p, d->p_mode, true, a, m.pOp[a]);
+        const int ru = make_op(d->u_mask, *usig[a], d->u_mode, false, a, m.uOp[a]);
+        if (rp < 0 || ru < 0) { g_err = "source signal rows must be 1 or the number of source points"; return KW_ERR_INVALID; }
+        m.hasP[a] = rp > 0; m.hasU[a] = ru > 0;
+    }
+
+    // ---- p0 (KSFO:425-430) ----
+    m.hasP0 = d->p0 != nullptr;
+    if (m.hasP0) {
+        m.p0f.assign(d->p0, d->p0 + N);
+        if (d->smooth_p0) m.p0f = smooth_field(s, m.p0f);
+    }
+
+    // ---- absorption (KSFO:812-882) and nonlinearity (KSFO:889-907) ----
+    if (d->alpha_coeff.data && d->alpha_mode != KW_ABSORPTION_NONE) {
+        if (!grid_sized(d->alpha_coeff, N)) { g_err = "alphaCoeff must be scalar or grid-shaped"; return KW_ERR_INVALID; }
+        m.absorb = true;
+        double y = std::isnan(d->alpha_power) ? 1.5 : d->alpha_power;
+        if (d->alpha_mode == KW_ABSORPTION_STOKES) y = 2.0;
+        m.y = y;
+        const double np1 = db2neper(1.0, y);
+        vecd alphaNp = expand(d->alpha_coeff, N);
+        for (auto& v : alphaNp) v *= np1;
+        m.stokes = d->alpha_mode == KW_ABSORPTION_STOKES || std::fabs(y - 2.0) < 1e-10;
+        m.tau.resize(N);
+        if (m.stokes) {
+            for (size_t i = 0; i < N; ++i) m.tau[i] = -2.0 * alphaNp[i] * c0[i];
+        } else {
+            m.nabla1.resize(N);
+            for (size_t i = 0; i < N; ++i) {
+                m.tau[i] = -2.0 * alphaNp[i] * std::pow(c0[i], y - 1.0);
+                m.nabla1[i] = m.kmag[i] == 0.0 ? 0.0 : std::pow(m.kmag[i], y - 2.0);
+            }
+        }
+        if (!m.stokes && d->alpha_mode != KW_ABSORPTION_NO_DISPERSION) {
+            m.dispersion = true;
+            m.eta.resize(N); m.nabla2.resize(N);
+            const double tn = std::tan(M_PI * y / 2.0);
+            for (size_t i = 0; i < N; ++i) {
+                m.eta[i] = 2.0 * alphaNp[i] * std::pow(c0[i], y) * tn;
+                m.nabla2[i] = m.kmag[i] == 0.0 ? 0.0 : std::pow(m.kmag[i], y - 1.0);
+            }
+        }
+    }
+    if (d->b_on_a.data) {
+        if (!grid_sized(d->b_on_a, N)) { g_err = "bOnA must be scalar or grid-shaped"; return KW_ERR_INVALID; }
+        m.bona = expand(d->b_on_a, N);
+        double mx = 0;
+        for (double v : m.bona) mx = std::max(mx, std::fabs(v));
+        m.nonlinear = mx != 0.0;
+    }
+
+    // ---- sensor (REC:8-97) ----
+    const unsigned rec = d->record;
+    m.rec = rec;
+    m.recordP = (rec & (KW_RECORD_P | KW_RECORD_P_MAX | KW_RECORD_P_MIN | KW_RECORD_P_RMS | KW_RECORD_I_AVG)) != 0;
+    m.recordU = (rec & (KW_RECORD_UX | KW_RECORD_UY | KW_RECORD_UZ | KW_RECORD_U_MAX | KW_RECORD_U_RMS | KW_RECORD_I_AVG)) != 0;
+    m.recordUFinal = (rec & KW_RECORD_U_FINAL) != 0;
+    if (d->sensor_kind == KW_SENSOR_BINARY && d->sensor_mask) {
+        m.haveSampler = true;
+        m.sIdx = flat_nonzero(d->sensor_mask, N);
+        m.nPts = (int)m.sIdx.size();
+        m.sW.assign(m.sIdx.size(), 1.0);
+    } else if (d->sensor_kind == KW_SENSOR_CARTESIAN && d->sensor_mask) {
+        m.haveSampler = true;
+        const int nPts = d->sensor_points;
+        m.nPts = nPts;
+        m.nCorners = 1 << ndim;
+        const int nCorners = m.nCorners;
+        m.sIdx.resize((size_t)nPts * nCorners);
+        m.sW.resize((size_t)nPts * nCorners);
+        for (int p = 0; p < nPts; ++p) {
+            int i0[3]; double frac[3];
+            for (int a = 0; a < ndim; ++a) {
+                const double g = (double)d->sensor_mask[(size_t)a * nPts + p] / s.d[a] + (double)(s.n[a] / 2);
+                if (!(g >= 0 && g <= (double)(s.n[a] - 1))) { g_err = "Cartesian sensor point outside grid bounds"; return KW_ERR_INVALID; }
+                const double f = std::floor(g);
+                i0[a] = (int)f; frac[a] = g - f;
+            }
+            for (int c = 0; c < nCorners; ++c) {
+                size_t flat = 0; double w = 1.0;
+                for (int a = 0; a < ndim; ++a) {
+                    const int bit = (c >> a) & 1;
+                    const int ai = std::min(i0[a] + bit, s.n[a] - 1);
+                    w *= bit == 1 ? frac[a] : (1.0 - frac[a]);
+                    flat = flat * (size_t)s.n[a] + (size_t)ai;
+                }
+                m.sIdx[(size_t)p * nCorners + c] = flat;
+                m.sW[(size_t)p * nCorners + c] = w;
+            }
+        }
+    }
+
+    // 2D directivity (Directivity.swift:41-79): per unique angle, a k-space weight.
+    m.directivity = ndim == 2 && d->sensor_kind == KW_SENSOR_BINARY && d->sensor_mask && d->directivity_angle && m.nPts > 0;
+    if (m.directivity) {
+        std::vector<double> rowAngle(m.nPts);
+        for (int r = 0; r < m.nPts; ++r) rowAngle[r] = (double)d->directivity_angle[m.sIdx[r]];
+        std::vector<double> uniq(rowAngle);
+        std::sort(uniq.begin(), uniq.end());
+        uniq.erase(std::unique(uniq.begin(), uniq.end()), uniq.end());
+        const double elem = std::isnan(d->directivity_size) ? 10.0 * std::max(s.d[0], s.d[1]) : d->directivity_size;
+        for (double th : uniq) {
+            DirEntry e; e.weight.resize(N);
+            for (size_t i = 0; i < N; ++i) {
+                const double kx = m.kv[0][s.idx(i, 0)], ky = m.kv[1][s.idx(i, 1)];
+                if (d->directivity_pattern == KW_DIRECTIVITY_PRESSURE) {
+                    const double kt = std::cos(th) * ky - std::sin(th) * kx;
+                    const double x = kt * (elem / 2.0);
+                    e.weight[i] = x == 0.0 ? 1.0 : std::sin(M_PI * x) / (M_PI * x);
+                } else {
+                    const double kn = std::sin(th) * ky + std::cos(th) * kx;
+                    e.weight[i] = m.kmag[i] == 0.0 ? 0.0 : kn / m.kmag[i];
+                }
+            }
+            for (int r = 0; r < m.nPts; ++r) if (rowAngle[r] == th) { e.rows.push_back(r); e.gather.push_back(m.sIdx[r]); }
+            m.dirEntries.push_back(std::move(e));
+        }
+    }
+    return KW_OK;
+}
+
+// SourceOp.apply (KSFO:155-174)
+static void apply_source(const Model& m, const SourceOp& op, vecd& field, int t) {
+    if (t >= op.len()) return;
+    const size_t N = m.N;
+    vecd vals(op.idx.size());
+    for (size_t q = 0; q < op.idx.size(); ++q)
+        vals[q] = (op.signal.size() == 1 ? op.signal[0][t] : op.signal[q][t]) * op.scale[q];
+    if (op.mode == KW_SOURCE_DIRICHLET) {
+        for (size_t q = 0; q < op.idx.size(); ++q) field[op.idx[q]] = vals[q];
+    } else if (op.mode == KW_SOURCE_ADDITIVE_NO_CORRECTION) {
+        vecd buf(N, 0.0);
+        for (size_t q = 0; q < op.idx.size(); ++q) buf[op.idx[q]] = vals[q];
+        for (size_t i = 0; i < N; ++i) field[i] += buf[i];
+    } else {
+        vecc B(N, cd(0, 0));
+        for (size_t q = 0; q < op.idx.size(); ++q) B[op.idx[q]] = vals[q];
+        fftn(m.s, B, false);
+        for (size_t i = 0; i < N; ++i) B[i] *= m.skappa[i];
+        fftn(m.s, B, true);
+        for (size_t i = 0; i < N; ++i) field[i] += B[i].real();
+    }
+}
+
+// One time step t (KSFO:444-521): velocity, sources, density, sources, equation of state, and
+// for t = 0 with an initial pressure the override of the whole state.
+static void forward_step(const Model& m, State& st, int t, vecc& spec, vecc& work) {
+    const Shape& s = m.s;
+    const size_t N = m.N;
+    const int ndim = m.ndim;
+    // velStep (KSFO:448-455): u_a = pml_sg * (pml_sg * u_a - dt/rho_sg * Re ifft(ddPos_a kappa fft(p)))
+    spec = to_complex(st.p);
+    fftn(s, spec, false);
+    for (int a = 0; a < ndim; ++a) {
+#pragma omp parallel for schedule(static)
+        for (long long i = 0; i < (long long)N; ++i) work[i] = m.ddPos[a][s.idx(i, a)] * m.kappa[i] * spec[i];
+        fftn(s, work, true);
+#pragma omp parallel for schedule(static)
+        for (long long i = 0; i < (long long)N; ++i) {
+            const double sg = m.pmlSg[a][s.idx(i, a)];
+            st.u[a][i] = sg * (sg * st.u[a][i] - m.dtOverRho[a][i] * work[i].real());
+        }
+    }
+    for (int a = 0; a < ndim; ++a) if (m.hasU[a]) apply_source(m, m.uOp[a], st.u[a], t);   // KSFO:497-501
+
+    // rhoStep (KSFO:457-465): nl factor from the previous split densities
+    vecd nl;
+    if (m.nonlinear) {
+        nl.resize(N);
+        for (size_t i = 0; i < N; ++i) {
+            double sum = 0;
+            for (int a = 0; a < ndim; ++a) sum += st.rho[a][i];
+            nl[i] = (2.0 * sum + m.rho0[i]) / m.rho0[i];
+        }
+    }
+    for (int a = 0; a < ndim; ++a) {
+        work = to_complex(st.u[a]);
+        fftn(s, work, false);
+#pragma omp parallel for schedule(static)
+        for (long long i = 0; i < (long long)N; ++i) work[i] *= m.ddNeg[a][s.idx(i, a)] * m.kappa[i];
+        fftn(s, work, true);
+#pragma omp parallel for schedule(static)
+        for (long long i = 0; i < (long long)N; ++i) {
+            const double du = work[i].real();
+            st.dU[a][i] = du;
+            const double mass = m.nonlinear ? m.dtRho0[i] * du * nl[i] : m.dtRho0[i] * du;
+            const double pm = m.pml[a][s.idx(i, a)];
+            st.rho[a][i] = pm * (pm * st.rho[a][i] - mass);
+        }
+    }
+    for (int a = 0; a < ndim; ++a) if (m.hasP[a]) apply_source(m, m.pOp[a], st.rho[a], t);   // KSFO:503-508
+
+    // eosStep (KSFO:467-474)
+    for (size_t i = 0; i < N; ++i) {
+        double sum = 0, dsum = 0;
+        for (int a = 0; a < ndim; ++a) { sum += st.rho[a][i]; dsum += st.dU[a][i]; }
+        st.rhoTot[i] = sum; st.divU[i] = dsum;
+    }
+    vecd eos(st.rhoTot);
+    if (m.absorb) {   // PowerLawAbsorption.eosTerm KSFO:836-845
+        if (!m.stokes) {
+            for (size_t i = 0; i < N; ++i) work[i] = cd(m.rho0[i] * st.divU[i], 0.0);
+            fftn(s, work, false);
+            for (size_t i = 0; i < N; ++i) work[i] *= m.nabla1[i];
+            fftn(s, work, true);
+            for (size_t i = 0; i < N; ++i) eos[i] += m.tau[i] * work[i].real();
+        } else {
+            for (size_t i = 0; i < N; ++i) eos[i] += m.tau[i] * m.rho0[i] * st.divU[i];
+        }
+        if (m.dispersion) {
+            work = to_complex(st.rhoTot);
+            fftn(s, work, false);
+            for (size_t i = 0; i < N; ++i) work[i] *= m.nabla2[i];
+            fftn(s, work, true);
+            for (size_t i = 0; i < N; ++i) eos[i] -= m.eta[i] * work[i].real();
+        }
+    }
+    if (m.nonlinear)
+        for (size_t i = 0; i < N; ++i) eos[i] += m.bona[i] * (st.rhoTot[i] * st.rhoTot[i]) / (2.0 * m.rho0[i]);
+    for (size_t i = 0; i < N; ++i) st.p[i] = m.c2[i] * eos[i];
+
+    // t = 0 override for an initial pressure (KSFO:514-521; 1D divides by c^2 only, :323)
+    if (t == 0 && m.hasP0) {
+        st.p = m.p0f;
+        for (int a = 0; a < ndim; ++a)
+            for (size_t i = 0; i < N; ++i) st.rho[a][i] = ndim == 1 ? m.p0f[i] / m.c2[i] : m.p0f[i] / ((double)ndim * m.c2[i]);
+        spec = to_complex(st.p);
+        fftn(s, spec, false);
+        for (int a = 0; a < ndim; ++a) {
+            for (size_t i = 0; i < N; ++i) work[i] = m.ddPos[a][s.idx(i, a)] * m.kappa[i] * spec[i];
+            fftn(s, work, true);
+            for (size_t i = 0; i < N; ++i) st.u[a][i] = (m.dtOverRho[a][i] / 2.0) * work[i].real();
+        }
+        for (size_t i = 0; i < N; ++i) {
+            double sum = 0;
+            for (int a = 0; a < ndim; ++a) sum += st.rho[a][i];
+            st.rhoTot[i] = sum;
+        }
+    }
+}
+
+// sensor gather (REC:37-45): binary mask or multilinear Cartesian weights
+static void sample_field(const Model& m, const vecd& f, vecd& dst) {
+    dst.assign(m.nPts, 0.0);
+    for (int p = 0; p < m.nPts; ++p) {
+        double acc = 0;
+        for (int c = 0; c < m.nCorners; ++c) acc += f[m.sIdx[(size_t)p * m.nCorners + c]] * m.sW[(size_t)p * m.nCorners + c];
+        dst[p] = acc;
+    }
+}
+
 extern "C" {
 
 const char* kwref_last_error(void) { return g_err.c_str(); }
@@ -392,383 +809,57 @@ int kwref_run(const kw_sim_desc* d, int nthreads, int max_steps, kwref_result** 
 #ifdef _OPENMP
     if (nthreads > 0) omp_set_num_threads(nthreads);
 #endif
-    Shape s;
-    s.dim = d->dim;
-    if (s.dim < 1 || s.dim > 3) { g_err = "dim must be 1, 2 or 3"; return KW_ERR_INVALID; }
-    const int ns[3] = {d->nx, d->ny, d->nz};
-    const double ds[3] = {d->dx, d->dy, d->dz};
-    for (int a = 0; a < s.dim; ++a) { s.n[a] = ns[a]; s.d[a] = ds[a]; if (ns[a] < 1) { g_err = "bad size"; return KW_ERR_INVALID; } }
-    s.finish();
-    const size_t N = s.N;
-    const int ndim = s.dim;
-    const double dt = d->dt;
-    const int nt = d->nt;
-    if (nt <= 0) { g_err = "call grid.makeTime(...) before running the solver"; return KW_ERR_INVALID; }
-    if (!d->p0 && !d->p_mask && !d->u_mask) { g_err = "solver requires source.p0 or a time-varying p/u source"; return KW_ERR_INVALID; }
-    if (!grid_sized(d->sound_speed, N) || !grid_sized(d->density, N)) { g_err = "soundSpeed/density must be scalar or grid-shaped"; return KW_ERR_INVALID; }
-    if (d->pml_size < 0) { g_err = "bad pml size"; return KW_ERR_INVALID; }
-    for (int a = 0; a < ndim; ++a) if (d->pml_size > s.n[a]) { g_err = "pml larger than grid"; return KW_ERR_INVALID; }
+    Model m;
+    const int st0 = build_model(d, m);
+    if (st0 != KW_OK) return st0;
+    const Shape& s = m.s;
+    const size_t N = m.N;
+    const int ndim = m.ndim;
+    const int nt = m.nt;
+    const int nPts = m.nPts;
+    const unsigned rec = m.rec;
 
     auto* R = new kwref_result();
     R->s = s; R->nt = nt; R->record = d->record;
     R->fields.assign(KW_FIELD_COUNT, vecd());
     R->present.assign(KW_FIELD_COUNT, 0);
+    R->nsensor = m.haveSampler ? nPts : 0;
 
-    // ---- medium (KSFO:367-373) ----
-    const bool c0Map = d->sound_speed.len > 1, rho0Map = d->density.len > 1;
-    vecd c0 = expand(d->sound_speed, N), rho0 = expand(d->density, N);
-    if (d->smooth_c0 && c0Map) c0 = smooth_field(s, c0);
-    if (d->smooth_rho0 && rho0Map) rho0 = smooth_field(s, rho0);
-    double cRef = 0;
-    for (size_t i = 0; i < N; ++i) cRef = std::max(cRef, c0[i]);   // referenceSoundSpeed KSFO:786-788
-    if (!c0Map) cRef = c0[0];
-    if (!std::isnan(d->c_ref)) cRef = d->c_ref;
-
-    // ---- k-space operators (KSFO:376-383, 764-769) ----
-    std::vector<vecd> kv(ndim);
-    for (int a = 0; a < ndim; ++a) kv[a] = wavenumber_vector(s.n[a], s.d[a]);
-    vecd kmag(N), kappa(N), skappa(N);
-    for (size_t i = 0; i < N; ++i) {
-        double k2 = 0;
-        for (int a = 0; a < ndim; ++a) { const double k = kv[a][s.idx(i, a)]; k2 += k * k; }
-        kmag[i] = std::sqrt(k2);
-        const double arg = kmag[i] * (cRef * dt / 2.0);
-        kappa[i] = arg == 0.0 ? 1.0 : std::sin(arg) / arg;
-        skappa[i] = std::cos(arg);
-    }
-    std::vector<vecc> ddPos(ndim), ddNeg(ndim), colloc(ndim);
-    const cd I(0, 1);
-    for (int a = 0; a < ndim; ++a) {
-        const int n = s.n[a];
-        ddPos[a].resize(n); ddNeg[a].resize(n); colloc[a].resize(n);
-        for (int i = 0; i < n; ++i) {
-            const double k = kv[a][i], th = k * (s.d[a] / 2.0);
-            ddPos[a][i] = I * k * (std::cos(th) + 1.0 * I * std::sin(th));
-            ddNeg[a][i] = I * k * (std::cos(th) - 1.0 * I * std::sin(th));
-            colloc[a][i] = std::cos(th) - I * std::sin(th);   // REC:101-104
-        }
-    }
-
-    // ---- PML (KSFO:385-397) ----
-    std::vector<vecd> pml(ndim), pmlSg(ndim);
-    for (int a = 0; a < ndim; ++a) {
-        pml[a] = pml_profile(s.n[a], s.d[a], dt, cRef, d->pml_size, d->pml_alpha, false);
-        pmlSg[a] = pml_profile(s.n[a], s.d[a], dt, cRef, d->pml_size, d->pml_alpha, true);
-    }
-
-    // ---- staggered density etc. (KSFO:399-402) ----
-    vecd c2(N), dtRho0(N);
-    for (size_t i = 0; i < N; ++i) { c2[i] = c0[i] * c0[i]; dtRho0[i] = dt * rho0[i]; }
-    std::vector<vecd> dtOverRho(ndim);
-    for (int a = 0; a < ndim; ++a) {
-        vecd sg = rho0Map ? stagger_density(s, rho0, a) : rho0;
-        dtOverRho[a].resize(N);
-        for (size_t i = 0; i < N; ++i) dtOverRho[a][i] = dt / sg[i];
-    }
-
-    // ---- sources (KSFO:404-423, 129-201) ----
-    const double nd = (double)ndim;
-    // makeSourceOp KSFO:192-201: no op when the mask or the signal is absent or the mask is empty.
-    auto make_op = [&](const float* mask, const kw_signal& sig, int mode, bool isP, int a, SourceOp& op) -> int {
-        if (!mask || !sig.data) return 0;
-        op.idx = flat_nonzero(mask, N);
-        if (op.idx.empty()) return 0;
-        const int rows = sig.rows, len = sig.len;
-        if ((rows != 1 && rows != (int)op.idx.size()) || len < 0) return -1;
-        op.signal.assign(rows, vecd(len));
-        for (int r = 0; r < rows; ++r)
-            for (int t = 0; t < len; ++t) op.signal[r][t] = sig.data[(size_t)r * len + t];
-        op.mode = mode;
-        op.scale.resize(op.idx.size());
-        for (size_t q = 0; q < op.idx.size(); ++q) {
-            const double c = c0[op.idx[q]];   // soundSpeedSamples KSFO:791-794
-            if (isP) op.scale[q] = mode == KW_SOURCE_DIRICHLET ? 1.0 / (nd * c * c) : 2.0 * dt / (nd * c * s.d[a]);
-            else op.scale[q] = mode == KW_SOURCE_DIRICHLET ? 1.0 : 2.0 * c * dt / s.d[a];
-        }
-        return 1;
-    };
-    std::vector<SourceOp> pOp(ndim), uOp(ndim);
-    std::vector<bool> hasP(ndim, false), hasU(ndim, false);
-    const kw_signal* usig[3] = {&d->ux, &d->uy, &d->uz};
-    for (int a = 0; a < ndim; ++a) {
-        const int rp = make_op(d->p_mask, d->p, d->p_mode, true, a, pOp[a]);
-        const int ru = make_op(d->u_mask, *usig[a], d->u_mode, false, a, uOp[a]);
-        if (rp < 0 || ru < 0) { delete R; g_err = "source signal rows must be 1 or the number of source points"; return KW_ERR_INVALID; }
-        hasP[a] = rp > 0; hasU[a] = ru > 0;
-    }
-    auto apply_op = [&](const SourceOp& op, vecd& field, int t) {     // SourceOp.apply KSFO:155-174
-        if (t >= op.len()) return;
-        vecd vals(op.idx.size());
-        for (size_t q = 0; q < op.idx.size(); ++q)
-            vals[q] = (op.signal.size() == 1 ? op.signal[0][t] : op.signal[q][t]) * op.scale[q];
-        if (op.mode == KW_SOURCE_DIRICHLET) {
-            for (size_t q = 0; q < op.idx.size(); ++q) field[op.idx[q]] = vals[q];
-        } else if (op.mode == KW_SOURCE_ADDITIVE_NO_CORRECTION) {
-            vecd buf(N, 0.0);
-            for (size_t q = 0; q < op.idx.size(); ++q) buf[op.idx[q]] = vals[q];
-            for (size_t i = 0; i < N; ++i) field[i] += buf[i];
-        } else {
-            vecc B(N, cd(0, 0));
-            for (size_t q = 0; q < op.idx.size(); ++q) B[op.idx[q]] = vals[q];
-            fftn(s, B, false);
-            for (size_t i = 0; i < N; ++i) B[i] *= skappa[i];
-            fftn(s, B, true);
-            for (size_t i = 0; i < N; ++i) field[i] += B[i].real();
-        }
-    };
-
-    // ---- p0 (KSFO:425-430) ----
-    bool hasP0 = d->p0 != nullptr;
-    vecd p0f;
-    if (hasP0) {
-        p0f.assign(d->p0, d->p0 + N);
-        if (d->smooth_p0) p0f = smooth_field(s, p0f);
-    }
-
-    // ---- absorption (KSFO:812-882) and nonlinearity (KSFO:889-907) ----
-    bool absorb = false, stokes = false, dispersion = false;
-    vecd tau, eta, nabla1, nabla2;
-    if (d->alpha_coeff.data && d->alpha_mode != KW_ABSORPTION_NONE) {
-        if (!grid_sized(d->alpha_coeff, N)) { delete R; g_err = "alphaCoeff must be scalar or grid-shaped"; return KW_ERR_INVALID; }
-        absorb = true;
-        double y = std::isnan(d->alpha_power) ? 1.5 : d->alpha_power;
-        if (d->alpha_mode == KW_ABSORPTION_STOKES) y = 2.0;
-        const double np1 = db2neper(1.0, y);
-        vecd alphaNp = expand(d->alpha_coeff, N);
-        for (auto& v : alphaNp) v *= np1;
-        stokes = d->alpha_mode == KW_ABSORPTION_STOKES || std::fabs(y - 2.0) < 1e-10;
-        tau.resize(N);
-        if (stokes) {
-            for (size_t i = 0; i < N; ++i) tau[i] = -2.0 * alphaNp[i] * c0[i];
-        } else {
-            nabla1.resize(N);
-            for (size_t i = 0; i < N; ++i) {
-                tau[i] = -2.0 * alphaNp[i] * std::pow(c0[i], y - 1.0);
-                nabla1[i] = kmag[i] == 0.0 ? 0.0 : std::pow(kmag[i], y - 2.0);
-            }
-        }
-        if (!stokes && d->alpha_mode != KW_ABSORPTION_NO_DISPERSION) {
-            dispersion = true;
-            eta.resize(N); nabla2.resize(N);
-            const double tn = std::tan(M_PI * y / 2.0);
-            for (size_t i = 0; i < N; ++i) {
-                eta[i] = 2.0 * alphaNp[i] * std::pow(c0[i], y) * tn;
-                nabla2[i] = kmag[i] == 0.0 ? 0.0 : std::pow(kmag[i], y - 1.0);
-            }
-        }
-    }
-    bool nonlinear = false;
-    vecd bona;
-    if (d->b_on_a.data) {
-        if (!grid_sized(d->b_on_a, N)) { delete R; g_err = "bOnA must be scalar or grid-shaped"; return KW_ERR_INVALID; }
-        bona = expand(d->b_on_a, N);
-        double mx = 0;
-        for (double v : bona) mx = std::max(mx, std::fabs(v));
-        nonlinear = mx != 0.0;
-    }
-
-    // ---- sensor (REC:8-97) ----
-    const unsigned rec = d->record;
-    const bool recordP = (rec & (KW_RECORD_P | KW_RECORD_P_MAX | KW_RECORD_P_MIN | KW_RECORD_P_RMS | KW_RECORD_I_AVG)) != 0;
-    const bool recordU = (rec & (KW_RECORD_UX | KW_RECORD_UY | KW_RECORD_UZ | KW_RECORD_U_MAX | KW_RECORD_U_RMS | KW_RECORD_I_AVG)) != 0;
-    const bool recordUFinal = (rec & KW_RECORD_U_FINAL) != 0;
-    bool haveSampler = false;
-    int nPts = 0, nCorners = 1;
-    std::vector<size_t> sIdx;
-    vecd sW;
-    if (d->sensor_kind == KW_SENSOR_BINARY && d->sensor_mask) {
-        haveSampler = true;
-        sIdx = flat_nonzero(d->sensor_mask, N);
-        nPts = (int)sIdx.size();
-        sW.assign(sIdx.size(), 1.0);
-    } else if (d->sensor_kind == KW_SENSOR_CARTESIAN && d->sensor_mask) {
-        haveSampler = true;
-        nPts = d->sensor_points;
-        nCorners = 1 << ndim;
-        sIdx.resize((size_t)nPts * nCorners);
-        sW.resize((size_t)nPts * nCorners);
-        for (int p = 0; p < nPts; ++p) {
-            int i0[3]; double frac[3];
-            for (int a = 0; a < ndim; ++a) {
-                const double g = (double)d->sensor_mask[(size_t)a * nPts + p] / s.d[a] + (double)(s.n[a] / 2);
-                if (!(g >= 0 && g <= (double)(s.n[a] - 1))) { delete R; g_err = "Cartesian sensor point outside grid bounds"; return KW_ERR_INVALID; }
-                const double f = std::floor(g);
-                i0[a] = (int)f; frac[a] = g - f;
-            }
-            for (int c = 0; c < nCorners; ++c) {
-                size_t flat = 0; double w = 1.0;
-                for (int a = 0; a < ndim; ++a) {
-                    const int bit = (c >> a) & 1;
-                    const int ai = std::min(i0[a] + bit, s.n[a] - 1);
-                    w *= bit == 1 ? frac[a] : (1.0 - frac[a]);
-                    flat = flat * (size_t)s.n[a] + (size_t)ai;
-                }
-                sIdx[(size_t)p * nCorners + c] = flat;
-                sW[(size_t)p * nCorners + c] = w;
-            }
-        }
-    }
-    R->nsensor = haveSampler ? nPts : 0;
-
-    // 2D directivity (Directivity.swift:41-79): per unique angle, a k-space weight.
-    struct DirEntry { vecd weight; std::vector<int> rows; std::vector<size_t> gather; };
-    std::vector<DirEntry> dirEntries;
-    const bool directivity = ndim == 2 && d->sensor_kind == KW_SENSOR_BINARY && d->sensor_mask && d->directivity_angle && nPts > 0;
-    if (directivity) {
-        std::vector<double> rowAngle(nPts);
-        for (int r = 0; r < nPts; ++r) rowAngle[r] = (double)d->directivity_angle[sIdx[r]];
-        std::vector<double> uniq(rowAngle);
-        std::sort(uniq.begin(), uniq.end());
-        uniq.erase(std::unique(uniq.begin(), uniq.end()), uniq.end());
-        const double elem = std::isnan(d->directivity_size) ? 10.0 * std::max(s.d[0], s.d[1]) : d->directivity_size;
-        for (double th : uniq) {
-            DirEntry e; e.weight.resize(N);
-            for (size_t i = 0; i < N; ++i) {
-                const double kx = kv[0][s.idx(i, 0)], ky = kv[1][s.idx(i, 1)];
-                if (d->directivity_pattern == KW_DIRECTIVITY_PRESSURE) {
-                    const double kt = std::cos(th) * ky - std::sin(th) * kx;
-                    const double x = kt * (elem / 2.0);
-                    e.weight[i] = x == 0.0 ? 1.0 : std::sin(M_PI * x) / (M_PI * x);
-                } else {
-                    const double kn = std::sin(th) * ky + std::cos(th) * kx;
-                    e.weight[i] = kmag[i] == 0.0 ? 0.0 : kn / kmag[i];
-                }
-            }
-            for (int r = 0; r < nPts; ++r) if (rowAngle[r] == th) { e.rows.push_back(r); e.gather.push_back(sIdx[r]); }
-            dirEntries.push_back(std::move(e));
-        }
-    }
-
-    auto sample = [&](const vecd& f, vecd& dst) {
-        dst.assign(nPts, 0.0);
-        for (int p = 0; p < nPts; ++p) {
-            double acc = 0;
-            for (int c = 0; c < nCorners; ++c) acc += f[sIdx[(size_t)p * nCorners + c]] * sW[(size_t)p * nCorners + c];
-            dst[p] = acc;
-        }
-    };
-
-    // ---- state (KSFO:438-442) ----
-    vecd p(N, 0.0), rhoTot(N), divU(N);
-    std::vector<vecd> u(ndim, vecd(N, 0.0)), rho(ndim, vecd(N, 0.0)), dU(ndim, vecd(N, 0.0));
+    State st;
+    st.init(m);
     std::vector<vecd> pRec, uRec[3];
-
     const int steps = max_steps >= 0 ? std::min(max_steps, nt) : nt;
     auto t0 = std::chrono::steady_clock::now();
     vecc spec(N), work(N);
     for (int t = 0; t < steps; ++t) {
-        // velStep (KSFO:448-455): u_a = pml_sg * (pml_sg * u_a - dt/rho_sg * Re ifft(ddPos_a kappa fft(p)))
-        spec = to_complex(p);
-        fftn(s, spec, false);
-        for (int a = 0; a < ndim; ++a) {
-#pragma omp parallel for schedule(static)
-            for (long long i = 0; i < (long long)N; ++i) work[i] = ddPos[a][s.idx(i, a)] * kappa[i] * spec[i];
-            fftn(s, work, true);
-#pragma omp parallel for schedule(static)
-            for (long long i = 0; i < (long long)N; ++i) {
-                const double sg = pmlSg[a][s.idx(i, a)];
-                u[a][i] = sg * (sg * u[a][i] - dtOverRho[a][i] * work[i].real());
-            }
-        }
-        for (int a = 0; a < ndim; ++a) if (hasU[a]) apply_op(uOp[a], u[a], t);   // KSFO:497-501
-
-        // rhoStep (KSFO:457-465): nl factor from the previous split densities
-        vecd nl;
-        if (nonlinear) {
-            nl.resize(N);
-            for (size_t i = 0; i < N; ++i) {
-                double sum = 0;
-                for (int a = 0; a < ndim; ++a) sum += rho[a][i];
-                nl[i] = (2.0 * sum + rho0[i]) / rho0[i];
-            }
-        }
-        for (int a = 0; a < ndim; ++a) {
-            work = to_complex(u[a]);
-            fftn(s, work, false);
-#pragma omp parallel for schedule(static)
-            for (long long i = 0; i < (long long)N; ++i) work[i] *= ddNeg[a][s.idx(i, a)] * kappa[i];
-            fftn(s, work, true);
-#pragma omp parallel for schedule(static)
-            for (long long i = 0; i < (long long)N; ++i) {
-                const double du = work[i].real();
-                dU[a][i] = du;
-                const double mass = nonlinear ? dtRho0[i] * du * nl[i] : dtRho0[i] * du;
-                const double pm = pml[a][s.idx(i, a)];
-                rho[a][i] = pm * (pm * rho[a][i] - mass);
-            }
-        }
-        for (int a = 0; a < ndim; ++a) if (hasP[a]) apply_op(pOp[a], rho[a], t);   // KSFO:503-508
-
-        // eosStep (KSFO:467-474)
-        for (size_t i = 0; i < N; ++i) {
-            double sum = 0, dsum = 0;
-            for (int a = 0; a < ndim; ++a) { sum += rho[a][i]; dsum += dU[a][i]; }
-            rhoTot[i] = sum; divU[i] = dsum;
-        }
-        vecd eos(rhoTot);
-        if (absorb) {   // PowerLawAbsorption.eosTerm KSFO:836-845
-            if (!stokes) {
-                for (size_t i = 0; i < N; ++i) work[i] = cd(rho0[i] * divU[i], 0.0);
-                fftn(s, work, false);
-                for (size_t i = 0; i < N; ++i) work[i] *= nabla1[i];
-                fftn(s, work, true);
-                for (size_t i = 0; i < N; ++i) eos[i] += tau[i] * work[i].real();
-            } else {
-                for (size_t i = 0; i < N; ++i) eos[i] += tau[i] * rho0[i] * divU[i];
-            }
-            if (dispersion) {
-                work = to_complex(rhoTot);
-                fftn(s, work, false);
-                for (size_t i = 0; i < N; ++i) work[i] *= nabla2[i];
-                fftn(s, work, true);
-                for (size_t i = 0; i < N; ++i) eos[i] -= eta[i] * work[i].real();
-            }
-        }
-        if (nonlinear)
-            for (size_t i = 0; i < N; ++i) eos[i] += bona[i] * (rhoTot[i] * rhoTot[i]) / (2.0 * rho0[i]);
-        for (size_t i = 0; i < N; ++i) p[i] = c2[i] * eos[i];
-
-        // t = 0 override for an initial pressure (KSFO:514-521; 1D divides by c^2 only, :323)
-        if (t == 0 && hasP0) {
-            p = p0f;
-            for (int a = 0; a < ndim; ++a)
-                for (size_t i = 0; i < N; ++i) rho[a][i] = ndim == 1 ? p0f[i] / c2[i] : p0f[i] / ((double)ndim * c2[i]);
-            spec = to_complex(p);
-            fftn(s, spec, false);
-            for (int a = 0; a < ndim; ++a) {
-                for (size_t i = 0; i < N; ++i) work[i] = ddPos[a][s.idx(i, a)] * kappa[i] * spec[i];
-                fftn(s, work, true);
-                for (size_t i = 0; i < N; ++i) u[a][i] = (dtOverRho[a][i] / 2.0) * work[i].real();
-            }
-        }
-
+        forward_step(m, st, t, spec, work);
         // sampling (KSFO:523-540)
-        if (haveSampler) {
-            if (recordP) {
+        if (m.haveSampler) {
+            if (m.recordP) {
                 vecd sp;
-                if (directivity) {
+                if (m.directivity) {
                     sp.assign(nPts, 0.0);
-                    vecc P = to_complex(p);
+                    vecc P = to_complex(st.p);
                     fftn(s, P, false);
-                    for (auto& e : dirEntries) {
+                    for (auto& e : m.dirEntries) {
                         for (size_t i = 0; i < N; ++i) work[i] = P[i] * e.weight[i];
                         fftn(s, work, true);
                         for (size_t q = 0; q < e.rows.size(); ++q) sp[e.rows[q]] = work[e.gather[q]].real();
                     }
                 } else {
-                    sample(p, sp);
+                    sample_field(m, st.p, sp);
                 }
                 pRec.push_back(sp);
             }
-            if (recordU) {
+            if (m.recordU) {
                 for (int a = 0; a < ndim; ++a) {
-                    work = to_complex(u[a]);
+                    work = to_complex(st.u[a]);
                     fftn(s, work, false);
-                    for (size_t i = 0; i < N; ++i) work[i] *= colloc[a][s.idx(i, a)];
+                    for (size_t i = 0; i < N; ++i) work[i] *= m.colloc[a][s.idx(i, a)];
                     fftn(s, work, true);
                     vecd uc(N), su;
                     for (size_t i = 0; i < N; ++i) uc[i] = work[i].real();
-                    sample(uc, su);
+                    sample_field(m, uc, su);
                     uRec[a].push_back(su);
                 }
             }
@@ -779,7 +870,7 @@ int kwref_run(const kw_sim_desc* d, int nthreads, int max_steps, kwref_result** 
 
     // ---- finalizeRecording (REC:129-168) ----
     auto put = [&](int f, vecd v) { R->fields[f] = std::move(v); R->present[f] = 1; };
-    put(KW_FIELD_P_FINAL, p);
+    put(KW_FIELD_P_FINAL, st.p);
     const int T = steps;
     auto series = [&](const std::vector<vecd>& recs) {   // MLX.stacked(axis: 1) -> [nPts, T]
         vecd v((size_t)nPts * T);
@@ -787,13 +878,13 @@ int kwref_run(const kw_sim_desc* d, int nthreads, int max_steps, kwref_result** 
             for (int q = 0; q < nPts; ++q) v[(size_t)q * T + t] = recs[t][q];
         return v;
     };
-    const bool haveP = haveSampler && recordP && T > 0;
-    const bool haveU = haveSampler && recordU && T > 0;
+    const bool haveP = m.haveSampler && m.recordP && T > 0;
+    const bool haveU = m.haveSampler && m.recordU && T > 0;
     vecd Pser, User[3];
     if (haveP) Pser = series(pRec);
     if (haveU) for (int a = 0; a < ndim; ++a) User[a] = series(uRec[a]);
-    auto reduce_max = [&](const vecd& S) { vecd r(nPts); for (int q = 0; q < nPts; ++q) { double m = -INFINITY; for (int t = 0; t < T; ++t) m = std::max(m, S[(size_t)q * T + t]); r[q] = m; } return r; };
-    auto reduce_min = [&](const vecd& S) { vecd r(nPts); for (int q = 0; q < nPts; ++q) { double m = INFINITY; for (int t = 0; t < T; ++t) m = std::min(m, S[(size_t)q * T + t]); r[q] = m; } return r; };
+    auto reduce_max = [&](const vecd& S) { vecd r(nPts); for (int q = 0; q < nPts; ++q) { double mx = -INFINITY; for (int t = 0; t < T; ++t) mx = std::max(mx, S[(size_t)q * T + t]); r[q] = mx; } return r; };
+    auto reduce_min = [&](const vecd& S) { vecd r(nPts); for (int q = 0; q < nPts; ++q) { double mn = INFINITY; for (int t = 0; t < T; ++t) mn = std::min(mn, S[(size_t)q * T + t]); r[q] = mn; } return r; };
     auto reduce_rms = [&](const vecd& S) { vecd r(nPts); for (int q = 0; q < nPts; ++q) { double a = 0; for (int t = 0; t < T; ++t) a += S[(size_t)q * T + t] * S[(size_t)q * T + t]; r[q] = std::sqrt(a / T); } return r; };
     if (haveP) {
         if (rec & KW_RECORD_P) put(KW_FIELD_P, Pser);
@@ -833,9 +924,193 @@ int kwref_run(const kw_sim_desc* d, int nthreads, int max_steps, kwref_result** 
             }
         }
     }
-    if (recordUFinal && (rec & KW_RECORD_U_FINAL))
-        for (int a = 0; a < ndim; ++a) put(KW_FIELD_UX_FINAL + a, u[a]);
+    if (m.recordUFinal && (rec & KW_RECORD_U_FINAL))
+        for (int a = 0; a < ndim; ++a) put(KW_FIELD_UX_FINAL + a, st.u[a]);
     *out = R;
+    return KW_OK;
+}
+
+/* ======================================================================================
+ * Discrete adjoint (FP64), the reference for the device gradient.
+ *
+ * L = 1/2 sum_t sum_q (p_q(t) - data_q(t))^2 over the sensor series of forward_step. The
+ * reverse sweep transposes every operator of the step in reverse order: the sensor gather, the
+ * equation of state (c^2, tau, eta, B/A; the power-law filters |k|^(y-2), |k|^(y-1) are
+ * symmetric), the k-space corrected additive pressure source (symmetric cos filter), the PML
+ * density update (nl from the previous densities), the staggered derivatives (the transpose of
+ * Re F^-1(H F .) is Re F^-1(conj(H) F .)), the PML velocity update, and finally the t = 0
+ * override of an initial pressure. Gradients: dL/dc0 (pointwise field) and dL/dp0 (the
+ * initial pressure after smoothing). The whole forward is kept in memory, so this is for small
+ * grids. Unsupported (KW_ERR_UNSUPPORTED): velocity sources, Dirichlet or uncorrected pressure
+ * sources, directivity, smoothing of c0.
+ * ====================================================================================== */
+int kwref_adjoint(const kw_sim_desc* d, const double* data, int nthreads, double* misfit, double* grad_c0,
+                  double* grad_p0) {
+    if (!d || !data) { g_err = "null argument"; return KW_ERR_INVALID; }
+#ifdef _OPENMP
+    if (nthreads > 0) omp_set_num_threads(nthreads);
+#endif
+    Model m;
+    const int st0 = build_model(d, m);
+    if (st0 != KW_OK) return st0;
+    for (int a = 0; a < m.ndim; ++a) {
+        if (m.hasU[a]) { g_err = "adjoint: velocity sources are not supported"; return KW_ERR_UNSUPPORTED; }
+        if (m.hasP[a] && m.pOp[a].mode != KW_SOURCE_ADDITIVE) { g_err = "adjoint: only the k-space corrected additive pressure source is supported"; return KW_ERR_UNSUPPORTED; }
+    }
+    if (m.directivity) { g_err = "adjoint: directivity is not supported"; return KW_ERR_UNSUPPORTED; }
+    if (d->smooth_c0 && d->sound_speed.len > 1) { g_err = "adjoint: smoothC0 is not supported"; return KW_ERR_UNSUPPORTED; }
+    if (!m.haveSampler || m.nPts == 0) { g_err = "adjoint: a sensor is required"; return KW_ERR_INVALID; }
+    const Shape& s = m.s;
+    const size_t N = m.N;
+    const int ndim = m.ndim, nt = m.nt, nPts = m.nPts;
+
+    // ---- forward, keeping what the reverse sweep reads ----
+    State st;
+    st.init(m);
+    std::vector<vecd> P(nt), Ssum(nt), Div(nt), Y(nt);
+    std::vector<std::vector<vecd>> DU(nt);
+    vecc spec(N), work(N);
+    for (int t = 0; t < nt; ++t) {
+        forward_step(m, st, t, spec, work);
+        P[t] = st.p;
+        Ssum[t] = st.rhoTot;
+        Div[t] = st.divU;
+        if (m.nonlinear) DU[t] = st.dU;
+        sample_field(m, st.p, Y[t]);
+    }
+    double L = 0;
+    std::vector<vecd> Rs(nt, vecd(nPts));
+    for (int t = 0; t < nt; ++t)
+        for (int q = 0; q < nPts; ++q) {
+            const double r = Y[t][q] - data[(size_t)q * nt + t];
+            Rs[t][q] = r;
+            L += 0.5 * r * r;
+        }
+    if (misfit) *misfit = L;
+
+    // ---- reverse sweep ----
+    vecd gc(N, 0.0), lp(N, 0.0), tmp, tmp2;
+    std::vector<vecd> lu(ndim, vecd(N, 0.0)), lr(ndim, vecd(N, 0.0));
+    const double y = m.y;
+    auto scatter_residual = [&](int t) {
+        for (int q = 0; q < nPts; ++q)
+            for (int c = 0; c < m.nCorners; ++c)
+                lp[m.sIdx[(size_t)q * m.nCorners + c]] += m.sW[(size_t)q * m.nCorners + c] * Rs[t][q];
+    };
+    const int t_stop = m.hasP0 ? 1 : 0;
+    for (int t = nt - 1; t >= t_stop; --t) {
+        scatter_residual(t);
+        const vecd& p = P[t];
+        const vecd& S = Ssum[t];
+        // equation of state: p = c^2 (S + tau A1(rho0 div) - eta A2(S) + B/A S^2 / (2 rho0))
+        vecd q1, q2;
+        if (m.absorb && !m.stokes) {
+            vecd x(N);
+            for (size_t i = 0; i < N; ++i) x[i] = m.rho0[i] * Div[t][i];
+            apply_op(m, x, q1, [&](size_t i) { return cd(m.nabla1[i], 0.0); });
+        }
+        if (m.dispersion) apply_op(m, S, q2, [&](size_t i) { return cd(m.nabla2[i], 0.0); });
+        vecd lE(N), lS(N), lDiv(N, 0.0);
+        for (size_t i = 0; i < N; ++i) {
+            const double c = m.c0[i];
+            double dpdc = 2.0 * p[i] / c;
+            if (m.absorb) {
+                if (m.stokes) dpdc += m.c2[i] * (m.tau[i] / c) * m.rho0[i] * Div[t][i];
+                else {
+                    dpdc += m.c2[i] * ((y - 1.0) * m.tau[i] / c) * q1[i];
+                    if (m.dispersion) dpdc -= m.c2[i] * (y * m.eta[i] / c) * q2[i];
+                }
+            }
+            gc[i] += lp[i] * dpdc;
+            lE[i] = m.c2[i] * lp[i];
+            lS[i] = lE[i] + (m.nonlinear ? lE[i] * m.bona[i] * S[i] / m.rho0[i] : 0.0);
+        }
+        if (m.dispersion) {
+            vecd x(N);
+            for (size_t i = 0; i < N; ++i) x[i] = m.eta[i] * lE[i];
+            apply_op(m, x, tmp, [&](size_t i) { return cd(m.nabla2[i], 0.0); });
+            for (size_t i = 0; i < N; ++i) lS[i] -= tmp[i];
+        }
+        if (m.absorb) {
+            if (m.stokes) {
+                for (size_t i = 0; i < N; ++i) lDiv[i] = m.tau[i] * m.rho0[i] * lE[i];
+            } else {
+                vecd x(N);
+                for (size_t i = 0; i < N; ++i) x[i] = m.tau[i] * lE[i];
+                apply_op(m, x, tmp, [&](size_t i) { return cd(m.nabla1[i], 0.0); });
+                for (size_t i = 0; i < N; ++i) lDiv[i] = m.rho0[i] * tmp[i];
+            }
+        }
+        // adjoint of the split densities after the source
+        std::vector<vecd> Lam(ndim, vecd(N));
+        for (int a = 0; a < ndim; ++a)
+            for (size_t i = 0; i < N; ++i) Lam[a][i] = lr[a][i] + lS[i];
+        // additive source: rho_a += Re F^-1(cos F(buf_a)), buf_a = sig * 2 dt / (d c dx_a) at the mask
+        for (int a = 0; a < ndim; ++a) {
+            const SourceOp& op = m.pOp[a];
+            if (!m.hasP[a] || t >= op.len()) continue;
+            apply_op(m, Lam[a], tmp, [&](size_t i) { return cd(m.skappa[i], 0.0); });
+            for (size_t q = 0; q < op.idx.size(); ++q) {
+                const size_t i = op.idx[q];
+                const double sig = op.signal.size() == 1 ? op.signal[0][t] : op.signal[q][t];
+                gc[i] += tmp[i] * sig * (-op.scale[q] / m.c0[i]);
+            }
+        }
+        // density update: rho_a = pml_a (pml_a rho_a - dt rho0 nl du_a), nl = (2 S(t-1) + rho0) / rho0
+        std::vector<vecd> lDu(ndim, vecd(N));
+        vecd lSprev(N, 0.0);
+        for (size_t i = 0; i < N; ++i) {
+            double nl = 1.0;
+            if (m.nonlinear) nl = (2.0 * (t > 0 ? Ssum[t - 1][i] : 0.0) + m.rho0[i]) / m.rho0[i];
+            for (int a = 0; a < ndim; ++a) {
+                const double pm = m.pml[a][s.idx(i, a)];
+                lDu[a][i] = lDiv[i] - pm * m.dtRho0[i] * nl * Lam[a][i];
+                if (m.nonlinear) lSprev[i] += -2.0 * m.dt * pm * DU[t][a][i] * Lam[a][i];
+            }
+            for (int a = 0; a < ndim; ++a) {
+                const double pm = m.pml[a][s.idx(i, a)];
+                lr[a][i] = pm * pm * Lam[a][i] + lSprev[i];
+            }
+        }
+        // du_a = D-_a u_a (the new u): mu_a = lambda_u_a + D-_a^T lDu_a
+        for (int a = 0; a < ndim; ++a) {
+            apply_op(m, lDu[a], tmp, [&](size_t i) { return std::conj(m.ddNeg[a][s.idx(i, a)]) * m.kappa[i]; });
+            for (size_t i = 0; i < N; ++i) lu[a][i] += tmp[i];
+        }
+        // velocity update: u_a = pml_sg (pml_sg u_a - dt/rho_sg D+_a p(t-1))
+        vecd lpNew(N, 0.0);
+        for (int a = 0; a < ndim; ++a) {
+            vecd x(N);
+            for (size_t i = 0; i < N; ++i) {
+                const double sg = m.pmlSg[a][s.idx(i, a)];
+                x[i] = -sg * m.dtOverRho[a][i] * lu[a][i];
+                lu[a][i] = sg * sg * lu[a][i];
+            }
+            apply_op(m, x, tmp, [&](size_t i) { return std::conj(m.ddPos[a][s.idx(i, a)]) * m.kappa[i]; });
+            for (size_t i = 0; i < N; ++i) lpNew[i] += tmp[i];
+        }
+        lp = lpNew;
+    }
+    vecd gp(N, 0.0);
+    if (m.hasP0) {
+        // t = 0 override: p = p0, rho_a = p0 / (d c^2), u_a = dt/rho_sg / 2 D+_a p0
+        scatter_residual(0);
+        const double dd = ndim == 1 ? 1.0 : (double)ndim;
+        for (size_t i = 0; i < N; ++i) {
+            double lrs = 0;
+            for (int a = 0; a < ndim; ++a) lrs += lr[a][i];
+            gp[i] = lp[i] + lrs / (dd * m.c2[i]);
+            gc[i] += lrs * m.p0f[i] * (-2.0 / (dd * m.c2[i] * m.c0[i]));
+        }
+        for (int a = 0; a < ndim; ++a) {
+            vecd x(N);
+            for (size_t i = 0; i < N; ++i) x[i] = m.dtOverRho[a][i] / 2.0 * lu[a][i];
+            apply_op(m, x, tmp, [&](size_t i) { return std::conj(m.ddPos[a][s.idx(i, a)]) * m.kappa[i]; });
+            for (size_t i = 0; i < N; ++i) gp[i] += tmp[i];
+        }
+    }
+    if (grad_c0) for (size_t i = 0; i < N; ++i) grad_c0[i] = gc[i];
+    if (grad_p0) for (size_t i = 0; i < N; ++i) grad_p0[i] = gp[i];
     return KW_OK;
 }
 

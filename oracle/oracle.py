@@ -44,6 +44,9 @@ def lib():
                                         C.c_double, C.c_int, C.POINTER(C.c_double)]
         L.kwref_smooth.argtypes = [C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_double), C.POINTER(C.c_double)]
         L.kwref_smoothing_window.argtypes = [C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_double)]
+        L.kwref_adjoint.restype = C.c_int
+        L.kwref_adjoint.argtypes = [C.POINTER(abi.kw_sim_desc), C.POINTER(C.c_double), C.c_int,
+                                    C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_double)]
         L.kwref_db2neper.restype = C.c_double
         L.kwref_db2neper.argtypes = [C.c_double, C.c_double]
         _lib = L
@@ -91,6 +94,21 @@ def run(builder, nthreads: int = 0, max_steps: int = -1):
         return out, L.kwref_loop_seconds(h)
     finally:
         L.kwref_free(h)
+
+
+def adjoint(builder, data: np.ndarray, nthreads: int = 0):
+    """FP64 discrete adjoint: (misfit, dL/dc0, dL/dp0) of L = 1/2 sum (p_sensor - data)^2, with
+    `data` shaped like the p series [n_sensor, nt]."""
+    L = lib()
+    d = np.ascontiguousarray(data, dtype=np.float64)
+    shape = builder.shape
+    gc = np.zeros(int(np.prod(shape)))
+    gp = np.zeros(int(np.prod(shape)))
+    mis = C.c_double()
+    st = L.kwref_adjoint(C.byref(builder.desc), _dp(d), int(nthreads), C.byref(mis), _dp(gc), _dp(gp))
+    if st != 0:
+        raise OracleError(f"status {st}: {L.kwref_last_error().decode()}")
+    return mis.value, gc.reshape(shape), gp.reshape(shape)
 
 
 def fft(x: np.ndarray, inverse: bool = False) -> np.ndarray:

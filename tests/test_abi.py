@@ -68,6 +68,28 @@ def test_descriptor_layout_matches_c(lib):
     assert int(vals[-1]) == C.sizeof(abi.kw_array)
 
 
+def test_adjoint_descriptor_layout_matches_c(lib):
+    fields = [f for f, _ in abi.kw_adjoint_desc._fields_]
+    src = ["#include <stdio.h>", "#include <stddef.h>", f'#include "{HEADER}"', "int main(void){",
+           'printf("%zu\\n", sizeof(kw_adjoint_desc));']
+    for f in fields:
+        src.append(f'printf("%zu\\n", offsetof(kw_adjoint_desc, {f}));')
+    src.append("return 0; }")
+    with tempfile.TemporaryDirectory() as d:
+        c = os.path.join(d, "t.c")
+        open(c, "w").write("\n".join(src))
+        exe = os.path.join(d, "t")
+        subprocess.run(["gcc", c, "-o", exe], check=True)
+        vals = subprocess.run([exe], capture_output=True, text=True, check=True).stdout.split()
+    assert int(vals[0]) == C.sizeof(abi.kw_adjoint_desc)
+    for i, f in enumerate(fields):
+        assert int(vals[1 + i]) == getattr(abi.kw_adjoint_desc, f).offset, f
+    abi.bind(lib)
+    a = abi.kw_adjoint_desc()
+    lib.kw_adjoint_desc_init(C.byref(a))
+    assert a.abi_version == abi.KW_ABI_VERSION and a.policy == abi.KW_CHECKPOINT_SQRT
+
+
 def test_desc_init_defaults(lib):
     abi.bind(lib)
     d = abi.kw_sim_desc()

@@ -1,0 +1,70 @@
+"""Device discrete adjoint (kw_adjoint_run through the C ABI) against the FP64 oracle adjoint and
+FP64 central finite differences of the oracle's misfit.
+
+Tolerances (FP32 device arithmetic): misfit relative error <= 1e-3; gradient fields relative L2
+<= 2e-3 against the FP64 adjoint; directional derivatives within 1e-3 of the finite differences;
+the checkpoint policies agree to 1e-5.
+"""
+import numpy as np
+import pytest
+
+import oracle
+from adjoint_cases import builder, fd_misfit_diff, problem
+from cases import rel_l2
+from kwave import KWaveError, abi
+from kwave.runtime import Context
+
+pytestmark = pytest.mark.gpu
+
+CASES = [
+    ((48, 40), dict(absorb="powerlaw", nonlinear=False, cartesian=True, nt=60)),
+    ((40, 36), dict(absorb="none", nonlinear=True, cartesian=False, nt=50)),
+    ((40, 36), dict(absorb="stokes", nonlinear=False, cartesian=True, nt=50)),
+    ((36, 32), dict(absorb="nodispersion", nonlinear=True, cartesian=False, nt=40, no_p0=True)),
+    ((96,), dict(absorb="powerlaw", nonlinear=True, cartesian=False, nt=60)),
+    ((20, 18, 16), dict(absorb="powerlaw", nonlinear=True, cartesian=True, nt=30)),
+]
+
+
+def gpu_adjoint(shape, c, p0, data, kw, **opt):
+    return Context.default().adjoint(builder(shape, c, p0, **kw), data, grad_c0=True, grad_p0=p0 is not None, **opt)
+
+
+@pytest.mark.parametrize("shape,kw", CASES)
+def test_device_adjoint_matches_fp64_adjoint_and_differences(shape, kw):
+    c, p0, data, kw = problem(shape, **kw)
+    L, gc, gp = oracle.adjoint(builder(shape, c, p0, **kw), data)
+    r = gpu_adjoint(shape, c, p0, data, kw)
+    assert abs(r["misfit"] - L) <= 1e-3 * L, (r["misfit"], L)
+    assert rel_l2(r["grad_c0"], gc) < 2e-3, rel_l2(r["grad_c0"], gc)
+    if p0 is not None:
+        assert rel_l2(r["grad_p0"], gp) < 2e-3, rel_l2(r["grad_p0"], gp)
+    rng = np.random.default_rng(3)
+    for _ in range(2):
+        dL, dx = fd_misfit_diff(shape, c, p0, data, rng.standard_normal(shape), 0.1, "c", kw)
+        assert abs(dL - np.sum(r["grad_c0"] * dx)) <= 1e-3 * abs(dL)
+
+
+def test_checkpoint_policies_agree():
+    shape = (40, 36)
+    c, p0, data, kw = problem(shape, absorb="powerlaw", nonlinear=True, nt=45)
+    runs = [gpu_adjoint(shape, c, p0, data, kw, policy=abi.KW_CHECKPOINT_SQRT),
+            gpu_adjoint(shape, c, p0, data, kw, policy=abi.KW_CHECKPOINT_INTERVAL, interval=8),
+            gpu_adjoint(shape, c, p0, data, kw, policy=abi.KW_CHECKPOINT_STORE_ALL),
+            gpu_adjoint(shape, c, p0, data, kw, policy=abi.KW_CHECKPOINT_BUDGET, memory_budget=1e6)]
+    assert runs[0]["interval"] == 7 and runs[0]["checkpoints"] == 7
+    assert runs[2]["checkpoints"] == 0
+    for r in runs[1:]:
+        assert rel_l2(r["grad_c0"], runs[0]["grad_c0"]) < 1e-5
+        assert rel_l2(r["grad_p0"], runs[0]["grad_p0"]) < 1e-5
+        assert abs(r["misfit"] - runs[0]["misfit"]) <= 1e-6 * runs[0]["misfit"]
+
+
+def test_adjoint_rejects_unsupported():
+    shape = (32, 32)
+    c, p0, data, kw = problem(shape, absorb="none")
+    b = builder(shape, c, p0, **kw)
+    b.desc.p_mode = 0   # Dirichlet pressure source
+    with pytest.raises(KWaveError) as e:
+        Context.default().adjoint(b, data)
+    assert e.value.status == abi.KW_ERR_UNSUPPORTED
