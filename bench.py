@@ -137,6 +137,8 @@ def run_reference(args) -> None:
     threads = os.cpu_count() or 1
     if args.workload == BATCH:
         return run_reference_batch(args, threads)
+    if args.workload == ADJ:
+        return run_reference_adjoint(args, threads)
     b = workload(args.workload, 1)
     steps = max(1, min(args.steps or args.ref_steps, args.ref_steps))
     r = cpu_sample(b, steps, threads)
@@ -284,6 +286,119 @@ def run_batch(args) -> None:
                     "d2h_bytes_per_step": d2h / steps, "seconds": t1 - t0},
             "clocks": clk.summary(),
             "peak_gbs": peak, "peak_source": peak_kind,
+        }
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+ADJ = "adjoint2d_512"
+
+
+def run_reference_adjoint(args, threads: int) -> None:
+    """The FP64 oracle adjoint (forward + reverse) on this host over a bounded sample: the first
+    steps of the same 512^2 problem."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    from kwave import workloads
+    steps = max(2, min(args.steps or args.ref_steps, args.ref_steps) * 2)
+    bp, bt = workloads.adjoint2d(512, steps)
+    data, _ = oracle.run(bt, nthreads=threads)
+    t0 = time.perf_counter()
+    oracle.adjoint(bp, data["p"], nthreads=threads)
+    secs = time.perf_counter() - t0
+    value = bp.grid.totalGridPoints * steps / secs
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": steps,
+        "warmup": 0, "ms_per_step": 1e3 * secs / steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": ADJ, "grid": [512, 512], "what": "misfit gradient (forward + adjoint) per time step"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+                         "sample": f"first {steps} steps of the 512^2 adjoint problem: FP64 oracle forward + "
+                                   f"discrete adjoint, {threads} threads"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_adjoint(args) -> None:
+    """C4: the sound-speed gradient of a 512^2 sensor-data misfit by the discrete adjoint with
+    sqrt(nt) checkpointing, against the forward run of the same simulation. Value = grid points x
+    time steps / gradient time (forward with checkpoints + reverse sweep with recompute)."""
+    import numpy as np
+    import torch
+
+    from kwave import abi, workloads
+    from kwave.runtime import Context
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    bp, bt = workloads.adjoint2d()
+    nt, npts = bp.grid.nt, bp.grid.totalGridPoints
+    ctx = Context(local)
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    ctx.set_stream(stream.cuda_stream)
+    # observed data: the forward run at the true sound speed
+    sim = ctx.create_sim(bt)
+    sim.run()
+    data = sim.output("p")
+    sim.close()
+    # forward time of the perturbed model (warm-up, restart, the whole run)
+    sim = ctx.create_sim(bp)
+    sim.step(args.warmup)
+    sim.reset()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    gpu_id = "GPU-" + str(torch.cuda.get_device_properties(local).uuid)
+    with ClockSampler(gpu_id) as clk:
+        e0.record(stream)
+        sim.step(nt)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        fwd_ms = e0.elapsed_time(e1)
+        sim.close()
+        ctx.adjoint(bp, data, policy=abi.KW_CHECKPOINT_SQRT)   # warm-up of the adjoint path
+        t0 = time.perf_counter()
+        r = ctx.adjoint(bp, data, policy=abi.KW_CHECKPOINT_SQRT)
+        e2e_s = time.perf_counter() - t0
+        r_all = ctx.adjoint(bp, data, policy=abi.KW_CHECKPOINT_STORE_ALL)
+    grad_ms = r["forward_ms"] + r["reverse_ms"]
+    all_ms = r_all["forward_ms"] + r_all["reverse_ms"]
+    if dist:
+        t = torch.tensor([grad_ms, fwd_ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        grad_ms, fwd_ms = float(t[0]), float(t[1])
+    if rank == 0:
+        g = r["grad_c0"]
+        line = {
+            "metric": METRIC, "value": npts * nt * world / (grad_ms / 1e3), "unit": UNIT, "n_gpus": world,
+            "steps": nt, "warmup": args.warmup, "ms_per_step": grad_ms / nt, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": ADJ, "grid": [512, 512], "nt": nt, "sensor": "512-point Cartesian ring",
+                       "physics": "power law y=1.1 with dispersion, heterogeneous c0, p0",
+                       "l2": "small grid (fields L2-resident)", "parallelism": f"replicas{world}"},
+            "grad_over_forward": grad_ms / fwd_ms,
+            "forward_ms": fwd_ms,
+            "gradient_ms": {"checkpointed_forward": r["forward_ms"], "reverse_sweep": r["reverse_ms"]},
+            "checkpointing": {"policy": "sqrt(nt)", "interval": r["interval"], "checkpoints": r["checkpoints"]},
+            "store_all": {"gradient_ms": all_ms, "grad_over_forward": all_ms / fwd_ms},
+            "misfit": r["misfit"], "grad_c0_l2": float(np.sqrt(np.sum(g.astype(np.float64) ** 2))),
+            "roofline": None, "cpu_baseline": None,
+            "e2e": {"value": npts * nt * world / e2e_s, "unit": UNIT,
+                    "h2d_bytes_per_step": (sum(a.nbytes for a in bp.keep) + data.nbytes) / nt,
+                    "d2h_bytes_per_step": g.nbytes / nt + npts * 4 / nt, "seconds": e2e_s},
+            "clocks": clk.summary(),
         }
         print(json.dumps(line), flush=True)
     ctx.close()
@@ -448,6 +563,8 @@ def main() -> None:
         run_reference(args)
     elif args.workload == BATCH:
         run_batch(args)
+    elif args.workload == ADJ:
+        run_adjoint(args)
     else:
         run_ours(args)
 

@@ -5,10 +5,11 @@
 //    KW_CHECKPOINT_STORE_ALL, the reverse sweep's inputs of every step.
 // 2. Residuals r_t = p_sensor(t) - data(t) and the misfit on the host (FP64).
 // 3. Reverse sweep, segment by segment from the last: restore the segment's checkpoint, rerun its
-//    steps storing p, S, div (absorption) and u_a (B/A) of each step, then walk the segment
-//    backwards through the reverse step. The spectral pieces of a reverse step are ordinary jobs
-//    of the pass kernels (FS_ADJ fields): the transposed absorption filters, D-_a u_a for the B/A
-//    term, the source filter, D+_a and D-_a.
+//    steps storing p, S, div (Stokes) and u_a (B/A) of each step, then walk the segment backwards
+//    through the reverse step. The spectral pieces of a reverse step are ordinary jobs of the pass
+//    kernels on FS_ADJ fields (the transposed absorption filters with A2(S(t)), D-_a u_a for the
+//    B/A term, the source filter), and D+_a, D-_a whose C2R epilogues carry the velocity adjoint
+//    and the sum into lambda_p (register row kernels; separate kernels otherwise).
 // 4. The t = 0 override of an initial pressure gives dL/dp0 and its share of dL/dc0.
 #include <cmath>
 #include <cstring>
@@ -45,20 +46,28 @@ void Engine::adjoint(const kw_sim_desc& din, kw_adjoint_desc& a) {
     const size_t fb = (size_t)N * sizeof(float);
     const int npts = v.sensor.npts;
     if (npts <= 0) throw err(KW_ERR_INVALID, "adjoint: the sensor has no points");
-    const bool absorb = v.absorb >= 1, powerlaw = v.absorb >= 2, disp = v.absorb == 3, nonlin = v.nonlinear != 0;
+    const bool powerlaw = v.absorb >= 2, disp = v.absorb == 3, nonlin = v.nonlinear != 0;
     const bool has_p0 = v.has_p0 != 0;
     const bool psrc = v.has_p && v.psrc.mode == KW_SOURCE_ADDITIVE;
     float y = std::isnan(d.alpha_power) ? 1.5f : (float)d.alpha_power;
     if (d.alpha_mode == KW_ABSORPTION_STOKES) y = 2.f;
 
     // ---- work fields ----
-    for (int k = 0; k < ADJ_COUNT; ++k) v.adj[k] = (float*)dalloc(fb);
+    for (int k = 0; k < ADJ_COUNT; ++k)
+        if (!adj_is_view(k)) v.adj[k] = (float*)dalloc(fb);
+    // the absorption job of the reverse step has three components, so it needs three spectra
+    // (a 1D simulation allocates two)
+    for (int k = 0; k < 3; ++k)
+        if (!v.spec[k]) v.spec[k] = (float2*)dalloc((size_t)h.Ns * sizeof(float2));
+    // the register row kernels fuse the velocity-adjoint and summing steps into their epilogues
+    const bool fused = h.C % 2 == 0 && has_reg_row(h.M);
     double* gc = (double*)dalloc((size_t)N * sizeof(double));
     check(cudaMemcpyAsync(d_sims_, &v, sizeof(SimDev), cudaMemcpyHostToDevice, st()), "upload sim");
 
     // ---- checkpoint policy ----
-    const int ck_fields = 2 * D + 3 + (absorb ? 1 : 0);   // u_a, rho_a, S, p, S(t-1), div
-    const int tp_fields = 2 + (absorb ? 1 : 0) + (nonlin ? D : 0);   // p, S, div, u_a
+    const bool stokes = v.absorb == 1;   // the Stokes term reads div(t); the power law only p(t), S(t)
+    const int ck_fields = 2 * D + 3 + (stokes ? 1 : 0);   // u_a, rho_a, S, p, S(t-1), div
+    const int tp_fields = 2 + (stokes ? 1 : 0) + (nonlin ? D : 0);   // p, S, div, u_a
     bool store_all = a.policy == KW_CHECKPOINT_STORE_ALL;
     int K = 1;
     if (a.policy == KW_CHECKPOINT_SQRT) K = (int)std::ceil(std::sqrt((double)nt));
@@ -91,18 +100,28 @@ void Engine::adjoint(const kw_sim_desc& din, kw_adjoint_desc& a) {
     std::vector<float*> tape = alloc_fields((size_t)K * tp_fields);
     std::vector<float*> ck = alloc_fields((size_t)nck * ck_fields);
     auto tslot = [&](int slot, int f) { return tape[(size_t)slot * tp_fields + f]; };   // f: 0 p, 1 S, 2 div, then u_a
-    const int TF_DIV = 2, TF_U = absorb ? 3 : 2;
+    const int TF_DIV = 2, TF_U = stokes ? 3 : 2;
     auto ckf = [&](int c, int f) { return ck[(size_t)c * ck_fields + f]; };   // u_a, rho_a, S, p, S(t-1), div
     auto cpy = [&](float* dst, const float* src) {
         check(cudaMemcpyAsync(dst, src, fb, cudaMemcpyDeviceToDevice, st()), "adjoint copy");
     };
     auto zero = [&](float* x) { check(cudaMemsetAsync(x, 0, fb, st()), "adjoint zero"); };
-    auto tape_now = [&](int slot) {
-        cpy(tslot(slot, 0), v.p);
-        cpy(tslot(slot, 1), v.rho_sum);
-        if (absorb) cpy(tslot(slot, TF_DIV), v.div_term);
-        if (nonlin) for (int b = 0; b < D; ++b) cpy(tslot(slot, TF_U + b), v.u[b]);
-    };
+    float* zero_field = (float*)dalloc(fb);   // S(-1): the state before step 0 is zero
+
+    // where step t's forward quantities live while the reverse sweep reads them
+    std::vector<AdjTapeEntry> table(nt);
+    for (int t = 0; t < nt; ++t) {
+        const int slot = store_all ? t : t % K;
+        AdjTapeEntry& e = table[t];
+        e.p = tslot(slot, 0);
+        e.s = tslot(slot, 1);
+        e.div = stokes ? tslot(slot, TF_DIV) : nullptr;
+        for (int b = 0; b < kMaxComp; ++b) e.u[b] = nonlin && b < D ? tslot(slot, TF_U + b) : nullptr;
+        e.sprev = t == 0 ? zero_field : (slot > 0 ? tslot(slot - 1, 1) : ckf(t / K, 2 * D + 2));
+    }
+    const AdjTapeEntry* d_table = upload(table);
+    int* d_rev = (int*)dalloc(sizeof(int));
+    auto tape_now = [&]() { launch_adj_tape(st(), d_sims_, d_t_, d_table, stokes, nonlin, N); };
 
     cudaEvent_t e0, e1, e2;
     check(cudaEventCreate(&e0), "event");
@@ -112,7 +131,6 @@ void Engine::adjoint(const kw_sim_desc& din, kw_adjoint_desc& a) {
     // ---- 1. forward ----
     reset();
     check(cudaEventRecord(e0, st()), "event");
-    std::vector<float*> sprev_all;   // store-all: S(t-1) of step 0 is zero
     for (int t = 0; t < nt; ++t) {
         const bool ck_step = !store_all && t % K == 0;
         if (ck_step) {
@@ -121,14 +139,14 @@ void Engine::adjoint(const kw_sim_desc& din, kw_adjoint_desc& a) {
             else cpy(ckf(c, 2 * D + 2), v.rho_sum);
         }
         step(1);
+        if (store_all) tape_now();
         if (ck_step) {
             const int c = t / K;
             for (int b = 0; b < D; ++b) { cpy(ckf(c, b), v.u[b]); cpy(ckf(c, D + b), v.rho[b]); }
             cpy(ckf(c, 2 * D), v.rho_sum);
             cpy(ckf(c, 2 * D + 1), v.p);
-            if (absorb) cpy(ckf(c, 2 * D + 3), v.div_term);
+            if (stokes) cpy(ckf(c, 2 * D + 3), v.div_term);
         }
-        if (store_all) tape_now(t);
     }
     check(cudaEventRecord(e1, st()), "event");
 
@@ -149,16 +167,16 @@ void Engine::adjoint(const kw_sim_desc& din, kw_adjoint_desc& a) {
     float* d_resid = upload(resid);
 
     // ---- 3. reverse sweep ----
-    for (int k = 0; k < ADJ_COUNT; ++k) zero(v.adj[k]);
+    // the recomputed segments do not sample the sensor: capture the forward step again without it
+    any_recp_ = false;
+    if (graph_exec_) { cudaGraphExecDestroy(graph_exec_); graph_exec_ = nullptr; }
+    if (graph_) { cudaGraphDestroy(graph_); graph_ = nullptr; }
+    for (int k = 0; k < ADJ_COUNT; ++k)
+        if (!adj_is_view(k)) zero(v.adj[k]);
     check(cudaMemsetAsync(gc, 0, (size_t)N * sizeof(double), st()), "zero");
     AdjStepArgs A{};
-    A.pt = v.adj[ADJ_PT];
-    A.st = v.adj[ADJ_ST];
-    A.sprev = v.adj[ADJ_SPREV];
-    A.divt = v.adj[ADJ_DIVT];
     A.a1 = v.adj[ADJ_A1];
     A.a2 = v.adj[ADJ_A2];
-    A.q1 = v.adj[ADJ_Q1];
     A.q2 = v.adj[ADJ_Q2];
     A.lam_p = v.adj[ADJ_LP];
     for (int b = 0; b < kMaxComp; ++b) {
@@ -172,7 +190,7 @@ void Engine::adjoint(const kw_sim_desc& din, kw_adjoint_desc& a) {
     A.gc = gc;
     A.y = y;
 
-    auto job = [&](int in, int out, int nin, auto opf, const char* name) {
+    auto job = [&](int in, int out, int nin, auto opf, int epi, int coupled, const char* name) {
         SpecJob j;
         j.in_field = FS_ADJ + in;
         j.nin = nin;
@@ -180,48 +198,69 @@ void Engine::adjoint(const kw_sim_desc& din, kw_adjoint_desc& a) {
         for (int c = 0; c < nin; ++c) j.op[c] = opf(c);
         j.spec_in = 0;
         j.spec_out = 0;
-        j.epi = EPI_STORE;
+        j.epi = epi;
+        j.coupled = coupled;
         j.out_field = FS_ADJ + out;
         j.name = name;
         issue_job(j, -1);
     };
+    // absorption filters: x1 with |k|^(y-2); x2 and S(t) with |k|^(y-1)
+    auto absorption_op = [](int c) { return OpSpec{AO_NONE, 0, (int8_t)(c == 0 ? RT_NU1 : RT_NU2), (int8_t)c}; };
     auto radial = [](int r) { return [r](int c) { return OpSpec{AO_NONE, 0, (int8_t)r, (int8_t)c}; }; };
     auto deriv = [](int ao) { return [ao](int c) { return OpSpec{(int8_t)ao, (int8_t)c, RT_KAPPA, (int8_t)c}; }; };
 
-    // one reverse step t: tape slot `slot`, S(t-1) in `sprev` (nullptr: zero state before step 0)
-    auto reverse_step = [&](int t, int slot, const float* sprev) {
-        launch_set_step(st(), d_t_, t);   // the pass kernels gate on t < nt
-        launch_adj_residual(st(), d_sims_, npts, d_resid, t, v.adj[ADJ_LP]);
-        cpy(v.adj[ADJ_PT], tslot(slot, 0));
-        cpy(v.adj[ADJ_ST], tslot(slot, 1));
-        if (sprev) cpy(v.adj[ADJ_SPREV], sprev);
-        else zero(v.adj[ADJ_SPREV]);
-        if (absorb) cpy(v.adj[ADJ_DIVT], tslot(slot, TF_DIV));
-        if (powerlaw) {
-            launch_adj_pre(st(), d_sims_, N, v.adj[ADJ_LP], v.adj[ADJ_X1], v.adj[ADJ_X2]);
-            job(ADJ_X1, ADJ_A1, 2, radial(RT_NU1), "adj_nu1");
-            if (disp) job(ADJ_X2, ADJ_A2, 2, radial(RT_NU2), "adj_nu2");
-        }
-        if (nonlin) {
-            for (int b = 0; b < D; ++b) cpy(v.adj[ADJ_UT + b], tslot(slot, TF_U + b));
-            job(ADJ_UT, ADJ_DD, D, deriv(AO_DNEG), "adj_du");
-        }
-        const bool src_on = psrc && t < v.psrc.len;
+    // one reverse step; its step t comes from *d_rev (counted down), so the launches are the same
+    // for every step and run as a CUDA graph (one per variant: additive source active or not)
+    auto reverse_body = [&](bool src_on) {
+        launch_adj_begin(st(), d_sims_, d_t_, d_rev, d_table, d_resid, npts);   // also sets the step counter the pass kernels gate on
+        if (powerlaw) job(ADJ_X1, ADJ_A1, disp ? 3 : 1, absorption_op, EPI_STORE, 0, "adj_abs");
+        if (nonlin) job(ADJ_UTP, ADJ_DD, D, deriv(AO_DNEG), EPI_STORE, 0, "adj_du");
         A.sig = src_on ? v.adj[ADJ_SIG] : nullptr;
-        launch_adj_eos(st(), d_sims_, N, A);
+        launch_adj_eos(st(), d_sims_, N, A, d_rev);
         if (src_on) {
-            job(ADJ_SIG, ADJ_GSIG, 1, radial(RT_SKAPPA), "adj_src");
-            launch_adj_src(st(), d_sims_, v.psrc.nsrc, v.adj[ADJ_GSIG], t, gc);
+            job(ADJ_SIG, ADJ_GSIG, 1, radial(RT_SKAPPA), EPI_STORE, 0, "adj_src");
+            launch_adj_src(st(), d_sims_, v.psrc.nsrc, v.adj[ADJ_GSIG], d_t_, gc);
         }
-        job(ADJ_W, ADJ_E, D, deriv(AO_DPOS), "adj_dpos");
-        launch_adj_vel(st(), d_sims_, N, A);
-        job(ADJ_W, ADJ_E, D, deriv(AO_DNEG), "adj_dneg");
-        launch_adj_sum(st(), d_sims_, N, A);
+        if (fused) {
+            job(ADJ_W, ADJ_E, D, deriv(AO_DPOS), EPI_ADJ_VEL, 0, "adj_vel");
+            job(ADJ_W, ADJ_E, D, deriv(AO_DNEG), EPI_ADJ_SUM, 1, "adj_sum");
+        } else {
+            job(ADJ_W, ADJ_E, D, deriv(AO_DPOS), EPI_STORE, 0, "adj_dpos");
+            launch_adj_vel(st(), d_sims_, N, A);
+            job(ADJ_W, ADJ_E, D, deriv(AO_DNEG), EPI_STORE, 0, "adj_dneg");
+            launch_adj_sum(st(), d_sims_, N, A);
+        }
+    };
+    cudaGraphExec_t rgraph[2] = {nullptr, nullptr};
+    int uses[2] = {0, 0};
+    auto reverse_step = [&](int t) {
+        const int var = psrc && t < v.psrc.len ? 1 : 0;
+        if (uses[var]++ == 0) {   // the first use runs directly (it also creates the tile maps)
+            reverse_body(var == 1);
+            return;
+        }
+        if (!rgraph[var]) {
+            cudaGraph_t g = nullptr;
+            check(cudaStreamBeginCapture(st(), cudaStreamCaptureModeThreadLocal), "begin capture");
+            try {
+                reverse_body(var == 1);
+            } catch (...) {
+                cudaStreamEndCapture(st(), &g);
+                if (g) cudaGraphDestroy(g);
+                throw;
+            }
+            check(cudaStreamEndCapture(st(), &g), "end capture");
+            const cudaError_t e = cudaGraphInstantiate(&rgraph[var], g, 0);
+            cudaGraphDestroy(g);
+            check(e, "graph instantiate");
+        }
+        check(cudaGraphLaunch(rgraph[var], st()), "graph launch");
     };
 
     const int t_stop = has_p0 ? 1 : 0;
+    launch_set_step(st(), d_rev, nt - 1);
     if (store_all) {
-        for (int t = nt - 1; t >= t_stop; --t) reverse_step(t, t, t > 0 ? tslot(t - 1, 1) : nullptr);
+        for (int t = nt - 1; t >= t_stop; --t) reverse_step(t);
     } else {
         for (int c = nck - 1; c >= 0; --c) {
             const int t0 = c * K, t1 = std::min(t0 + K, nt);
@@ -230,24 +269,22 @@ void Engine::adjoint(const kw_sim_desc& din, kw_adjoint_desc& a) {
             for (int b = 0; b < D; ++b) { cpy(v.u[b], ckf(c, b)); cpy(v.rho[b], ckf(c, D + b)); }
             cpy(v.rho_sum, ckf(c, 2 * D));
             cpy(v.p, ckf(c, 2 * D + 1));
-            if (absorb) cpy(v.div_term, ckf(c, 2 * D + 3));
-            tape_now(0);
+            if (stokes) cpy(v.div_term, ckf(c, 2 * D + 3));
             launch_set_step(st(), d_t_, t0 + 1);
             t_ = t0 + 1;
+            tape_now();
             for (int t = t0 + 1; t < t1; ++t) {
                 step(1);
-                tape_now(t - t0);
+                tape_now();
             }
-            for (int t = t1 - 1; t >= std::max(t0, t_stop); --t)
-                reverse_step(t, t - t0, t > t0 ? tslot(t - t0 - 1, 1) : (t > 0 ? ckf(c, 2 * D + 2) : nullptr));
+            for (int t = t1 - 1; t >= std::max(t0, t_stop); --t) reverse_step(t);
         }
     }
     if (has_p0) {
         // t = 0 override: p = p0, rho_a = p0 / (D c^2), u_a = dtor_a / 2 D+_a p0
-        launch_set_step(st(), d_t_, 0);
-        launch_adj_residual(st(), d_sims_, npts, d_resid, 0, v.adj[ADJ_LP]);
+        launch_adj_begin(st(), d_sims_, d_t_, d_rev, d_table, d_resid, npts);   // *d_rev is 0 here: residual r_0
         launch_adj_half_dtor(st(), d_sims_, N, A);
-        job(ADJ_W, ADJ_E, D, deriv(AO_DNEG), "adj_p0");
+        job(ADJ_W, ADJ_E, D, deriv(AO_DNEG), EPI_STORE, 0, "adj_p0");
         float* gp = a.grad_p0 ? v.adj[ADJ_GSIG] : nullptr;
         launch_adj_p0(st(), d_sims_, N, A, h.p0s, gp);
         if (gp) {
@@ -272,6 +309,8 @@ void Engine::adjoint(const kw_sim_desc& din, kw_adjoint_desc& a) {
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     cudaEventDestroy(e2);
+    for (auto& g : rgraph)
+        if (g) cudaGraphExecDestroy(g);
 }
 
 }  // namespace kw

@@ -12,6 +12,7 @@
 // Reverse (lambda_x = dL/dx of the state after step t):
 //   lambda_p += Sample^T r_t
 //   dL/dc  += lambda_p (2 p / c + c ((y-1) tau A1(div) - y eta A2(S)))      (Stokes: + c tau div)
+//             with tau A1(div) - eta A2(S) = p / c^2 - S - B/A S^2 / (2 rho0), so only A2(S) is transformed
 //   lE = c^2 lambda_p;  lS = lE + lE B/A S / rho0 - A2(eta lE);  ldiv = A1(tau lE) (Stokes: tau lE)
 //   L_a = lambda_rho_a + lS;  source: dL/dc_i += G(sum_a L_a / dx_a)_i sig (-scale_i / c_i)
 //   w_a = rho0 ldiv - pm_a dt rho0 nl L_a
@@ -34,10 +35,36 @@ __device__ __forceinline__ int layout_coord(const SimDev& S, long long i, int a)
 
 __global__ void k_set_step(int* d_t, int t) { *d_t = t; }
 
-// lambda_p += Sample^T r_t (binary: one point; Cartesian: multilinear corners, which can coincide)
-__global__ void k_adj_residual(const SimDev* __restrict__ sims, const float* __restrict__ resid, int t,
-                               float* __restrict__ lam_p) {
+__global__ void k_adj_tape(const SimDev* __restrict__ sims, const int* __restrict__ d_t,
+                           const AdjTapeEntry* __restrict__ table, int stokes, int nonlinear) {
     const SimDev& S = sims[0];
+    const AdjTapeEntry e = table[*d_t - 1];
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= S.N) return;
+    e.p[i] = S.p[i];
+    e.s[i] = S.rho_sum[i];
+    if (stokes) e.div[i] = S.div_term[i];
+    if (nonlinear)
+        for (int b = 0; b < S.dim; ++b) e.u[b][i] = S.u[b][i];
+}
+
+// Start of a reverse step: t = *d_rev (counted down by k_adj_eos); thread 0 sets the step counter
+// *d_t = t and points the tape views at table[t]; every thread adds its sensor point's residual:
+// lambda_p += Sample^T r_t (binary: one point; Cartesian: multilinear corners, which can coincide),
+// and x1 = tau c^2 lambda_p, x2 = eta c^2 lambda_p at the same points.
+__global__ void k_adj_begin(SimDev* __restrict__ sims, int* __restrict__ d_t, const int* __restrict__ d_rev,
+                            const AdjTapeEntry* __restrict__ table, const float* __restrict__ resid) {
+    SimDev& S = sims[0];
+    const int t = *d_rev;
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        *d_t = t;
+        const AdjTapeEntry e = table[t];
+        S.adj[ADJ_PTP] = e.p;
+        S.adj[ADJ_STP] = e.s;
+        S.adj[ADJ_SPRP] = e.sprev;
+        S.adj[ADJ_DIVP] = e.div;
+        for (int b = 0; b < kMaxComp; ++b) S.adj[ADJ_UTP + b] = e.u[b];
+    }
     const SensorDev& sn = S.sensor;
     const int q = blockIdx.x * blockDim.x + threadIdx.x;
     if (q >= sn.npts) return;
@@ -45,35 +72,38 @@ __global__ void k_adj_residual(const SimDev* __restrict__ sims, const float* __r
     for (int c = 0; c < sn.ncorners; ++c) {
         const int i = __ldg(sn.idx + q * sn.ncorners + c);
         const float w = sn.kind == 2 ? __ldg(sn.w + q * sn.ncorners + c) : 1.f;
-        atomicAdd(lam_p + i, w * r);
+        const float v = w * r;
+        atomicAdd(S.adj[ADJ_LP] + i, v);
+        if (S.absorb >= 2) {
+            const float c2 = S.c2.at(i);
+            atomicAdd(S.adj[ADJ_X1] + i, S.tau.at(i) * c2 * v);
+            if (S.absorb == 3) atomicAdd(S.adj[ADJ_X2] + i, S.eta.at(i) * c2 * v);
+        }
     }
 }
 
-// inputs of the transposed absorption filters: tau c^2 lambda_p and eta c^2 lambda_p
-__global__ void k_adj_pre(const SimDev* __restrict__ sims, const float* __restrict__ lam_p, float* __restrict__ x1,
-                          float* __restrict__ x2) {
+__global__ void k_adj_eos(const SimDev* __restrict__ sims, AdjStepArgs A, int* __restrict__ d_rev) {
     const SimDev& S = sims[0];
     const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= S.N) return;
-    const float lE = S.c2.at(i) * lam_p[i];
-    x1[i] = S.tau.at(i) * lE;
-    if (S.absorb == 3) x2[i] = S.eta.at(i) * lE;
-}
-
-__global__ void k_adj_eos(const SimDev* __restrict__ sims, AdjStepArgs A) {
-    const SimDev& S = sims[0];
-    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i == 0) *d_rev -= 1;   // every reader of this step's *d_rev (k_adj_begin) has finished
     if (i >= S.N) return;
     const int D = S.dim;
     const float c2 = S.c2.at(i);
     const float c = sqrtf(c2);
     const float lp = A.lam_p[i];
-    const float sv = A.st[i];
+    const float sv = S.adj[ADJ_STP][i];
     const float r0 = S.rho0.at(i);
-    double dpdc = 2.0 * (double)A.pt[i] / c;
-    if (S.absorb == 1) dpdc += (double)c * S.tau.at(i) * A.divt[i];
-    if (S.absorb >= 2) dpdc += (double)c * (A.y - 1.f) * S.tau.at(i) * A.q1[i];
-    if (S.absorb == 3) dpdc -= (double)c * A.y * S.eta.at(i) * A.q2[i];
+    const float pv = S.adj[ADJ_PTP][i];
+    double dpdc = 2.0 * (double)pv / c;
+    if (S.absorb == 1) dpdc += (double)c * S.tau.at(i) * S.adj[ADJ_DIVP][i];
+    if (S.absorb >= 2) {
+        // (y-1) tau A1(div) - y eta A2(S) = (y-1) E - eta A2(S), E = tau A1(div) - eta A2(S) = p / c^2 - S - B/A S^2 / (2 rho0)
+        double E = (double)pv / c2 - sv;
+        if (S.nonlinear) E -= (double)S.bona.at(i) * sv * sv / (2.0 * r0);
+        double term = (double)(A.y - 1.f) * E;
+        if (S.absorb == 3) term -= (double)S.eta.at(i) * A.q2[i];
+        dpdc += (double)c * term;
+    }
     A.gc[i] += (double)lp * dpdc;
     const float lE = c2 * lp;
     float lS = lE;
@@ -82,7 +112,7 @@ __global__ void k_adj_eos(const SimDev* __restrict__ sims, AdjStepArgs A) {
     float ldiv = 0.f;
     if (S.absorb == 1) ldiv = S.tau.at(i) * lE;
     else if (S.absorb >= 2) ldiv = A.a1[i];
-    const float nl = S.nonlinear ? (2.f * A.sprev[i] + r0) / r0 : 1.f;
+    const float nl = S.nonlinear ? (2.f * S.adj[ADJ_SPRP][i] + r0) / r0 : 1.f;
     const float dtr = S.dt * r0;
     float lam[kMaxComp], pm[kMaxComp];
     float lsprev = 0.f, sig = 0.f;
@@ -104,8 +134,10 @@ __global__ void k_adj_eos(const SimDev* __restrict__ sims, AdjStepArgs A) {
 }
 
 // dL/dc at the additive source points: G(sigma)_i sig (-scale_i / c_i)
-__global__ void k_adj_src(const SimDev* __restrict__ sims, const float* __restrict__ gsig, int t, double* __restrict__ gc) {
+__global__ void k_adj_src(const SimDev* __restrict__ sims, const float* __restrict__ gsig, const int* __restrict__ d_t,
+                          double* __restrict__ gc) {
     const SimDev& S = sims[0];
+    const int t = *d_t;
     const SourceDev& s = S.psrc;
     const int q = blockIdx.x * blockDim.x + threadIdx.x;
     if (q >= s.nsrc || t >= s.len) return;
@@ -128,6 +160,8 @@ __global__ void k_adj_vel(const SimDev* __restrict__ sims, AdjStepArgs A) {
     }
 }
 
+// lambda_p = sum_a e_a and the next reverse step's absorption inputs (the fused form is the
+// EPI_ADJ_SUM epilogue of the register row kernels)
 __global__ void k_adj_sum(const SimDev* __restrict__ sims, AdjStepArgs A) {
     const SimDev& S = sims[0];
     const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -135,6 +169,11 @@ __global__ void k_adj_sum(const SimDev* __restrict__ sims, AdjStepArgs A) {
     float s = A.e[0][i];
     for (int a = 1; a < S.dim; ++a) s += A.e[a][i];
     A.lam_p[i] = s;
+    if (S.absorb >= 2) {
+        const float c2 = S.c2.at(i);
+        S.adj[ADJ_X1][i] = S.tau.at(i) * c2 * s;
+        if (S.absorb == 3) S.adj[ADJ_X2][i] = S.eta.at(i) * c2 * s;
+    }
 }
 
 // the t = 0 override of an initial pressure: w_a = dtor_a / 2 lambda_u_a (then e_a = D-_a w_a)
@@ -169,17 +208,19 @@ __global__ void k_adj_store_grad(const double* __restrict__ gc, float* __restric
 static unsigned blocks(long long n) { return (unsigned)((n + 255) / 256); }
 
 void launch_set_step(cudaStream_t st, int* d_t, int t) { k_set_step<<<1, 1, 0, st>>>(d_t, t); }
-void launch_adj_residual(cudaStream_t st, const SimDev* d_sims, int npts, const float* resid, int t, float* lam_p) {
-    if (npts > 0) k_adj_residual<<<blocks(npts), 256, 0, st>>>(d_sims, resid, t, lam_p);
+void launch_adj_begin(cudaStream_t st, SimDev* d_sims, int* d_t, const int* d_rev, const AdjTapeEntry* table,
+                      const float* resid, int npts) {
+    k_adj_begin<<<blocks(npts > 0 ? npts : 1), 256, 0, st>>>(d_sims, d_t, d_rev, table, resid);
 }
-void launch_adj_pre(cudaStream_t st, const SimDev* d_sims, long long N, const float* lam_p, float* x1, float* x2) {
-    k_adj_pre<<<blocks(N), 256, 0, st>>>(d_sims, lam_p, x1, x2);
+void launch_adj_tape(cudaStream_t st, const SimDev* d_sims, const int* d_t, const AdjTapeEntry* table, int stokes,
+                     int nonlinear, long long N) {
+    k_adj_tape<<<blocks(N), 256, 0, st>>>(d_sims, d_t, table, stokes, nonlinear);
 }
-void launch_adj_eos(cudaStream_t st, const SimDev* d_sims, long long N, const AdjStepArgs& a) {
-    k_adj_eos<<<blocks(N), 256, 0, st>>>(d_sims, a);
+void launch_adj_eos(cudaStream_t st, const SimDev* d_sims, long long N, const AdjStepArgs& a, int* d_rev) {
+    k_adj_eos<<<blocks(N), 256, 0, st>>>(d_sims, a, d_rev);
 }
-void launch_adj_src(cudaStream_t st, const SimDev* d_sims, int nsrc, const float* gsig, int t, double* gc) {
-    if (nsrc > 0) k_adj_src<<<blocks(nsrc), 256, 0, st>>>(d_sims, gsig, t, gc);
+void launch_adj_src(cudaStream_t st, const SimDev* d_sims, int nsrc, const float* gsig, const int* d_t, double* gc) {
+    if (nsrc > 0) k_adj_src<<<blocks(nsrc), 256, 0, st>>>(d_sims, gsig, d_t, gc);
 }
 void launch_adj_vel(cudaStream_t st, const SimDev* d_sims, long long N, const AdjStepArgs& a) {
     k_adj_vel<<<blocks(N), 256, 0, st>>>(d_sims, a);

@@ -14,33 +14,40 @@ enum AdjField {
     ADJ_LP = 6,       // lambda_p
     ADJ_W = 7,        // w[a] (job inputs), 3
     ADJ_E = 10,       // e[a] (job outputs), 3
-    ADJ_X1 = 13,      // tau c^2 lambda_p      } job A1 inputs
-    ADJ_DIVT = 14,    // div(t) from the tape  }
-    ADJ_A1 = 15,      // A1(tau c^2 lambda_p)  } job A1 outputs
-    ADJ_Q1 = 16,      // A1(div(t))            }
-    ADJ_X2 = 17,      // eta c^2 lambda_p      } job A2 inputs
-    ADJ_ST = 18,      // S(t) from the tape    }
-    ADJ_A2 = 19,      // A2(eta c^2 lambda_p)  } job A2 outputs
-    ADJ_Q2 = 20,      // A2(S(t))              }
-    ADJ_SIG = 21,     // sum_a L_a / dx_a
-    ADJ_GSIG = 22,    // G(sigma)
-    ADJ_UT = 23,      // u_a(t) from the tape, 3
-    ADJ_DD = 26,      // D-_a u_a(t), 3
-    ADJ_PT = 29,      // p(t) from the tape
-    ADJ_SPREV = 30,   // S(t-1)
-    ADJ_COUNT = 31
+    ADJ_X1 = 13,      // tau c^2 lambda_p      } absorption job inputs: NU1, NU2, NU2
+    ADJ_X2 = 14,      // eta c^2 lambda_p      }
+    ADJ_STP = 15,     // S(t) (points into the tape) }
+    ADJ_A1 = 16,      // A1(tau c^2 lambda_p)  } outputs
+    ADJ_A2 = 17,      // A2(eta c^2 lambda_p)  }
+    ADJ_Q2 = 18,      // A2(S(t))              }
+    ADJ_SIG = 19,     // sum_a L_a / dx_a
+    ADJ_GSIG = 20,    // G(sigma)
+    ADJ_UTP = 21,     // u_a(t) (points into the tape), 3
+    ADJ_DD = 24,      // D-_a u_a(t), 3
+    ADJ_PTP = 27,     // p(t)   (points into the tape)
+    ADJ_SPRP = 28,    // S(t-1) (points into the tape, a checkpoint or a zero field)
+    ADJ_DIVP = 29,    // div(t) (points into the tape; Stokes)
+    ADJ_COUNT = 30
+};
+// entries that point into the tape instead of owning a field
+__host__ __device__ constexpr bool adj_is_view(int k) {
+    return k == ADJ_STP || (k >= ADJ_UTP && k < ADJ_UTP + 3) || k == ADJ_PTP || k == ADJ_SPRP || k == ADJ_DIVP;
+}
+
+// where the reverse sweep finds the forward quantities of step t (one entry per step, device memory)
+struct AdjTapeEntry {
+    float* p;
+    float* s;
+    float* sprev;
+    float* div;
+    float* u[kMaxComp];
 };
 static_assert(ADJ_COUNT <= kAdjFields, "adjoint fields");
 
 // device pointers of one reverse step
 struct AdjStepArgs {
-    const float* pt;
-    const float* st;
-    const float* sprev;
-    const float* divt;
     const float* a1;
     const float* a2;
-    const float* q1;
     const float* q2;
     const float* dd[kMaxComp];
     float* lam_p;
@@ -54,10 +61,17 @@ struct AdjStepArgs {
 };
 
 void launch_set_step(cudaStream_t st, int* d_t, int t);
-void launch_adj_residual(cudaStream_t st, const SimDev* d_sims, int npts, const float* resid, int t, float* lam_p);
-void launch_adj_pre(cudaStream_t st, const SimDev* d_sims, long long N, const float* lam_p, float* x1, float* x2);
-void launch_adj_eos(cudaStream_t st, const SimDev* d_sims, long long N, const AdjStepArgs& a);
-void launch_adj_src(cudaStream_t st, const SimDev* d_sims, int nsrc, const float* gsig, int t, double* gc);
+// A reverse step reads its step t from *d_rev (k_adj_eos counts it down), so that the same
+// launches (a CUDA graph) serve every step. k_adj_begin sets the step counter *d_t = t, points the
+// tape views of the simulation's work fields at table[t] and adds the sensor residual r_t:
+// lambda_p += Sample^T r_t, and x1 = tau c^2 lambda_p, x2 = eta c^2 lambda_p at the same points.
+void launch_adj_begin(cudaStream_t st, SimDev* d_sims, int* d_t, const int* d_rev, const AdjTapeEntry* table,
+                      const float* resid, int npts);
+// after forward step t (*d_t = t + 1): copy p, S, div, u_a into table[t]
+void launch_adj_tape(cudaStream_t st, const SimDev* d_sims, const int* d_t, const AdjTapeEntry* table, int stokes,
+                     int nonlinear, long long N);
+void launch_adj_eos(cudaStream_t st, const SimDev* d_sims, long long N, const AdjStepArgs& a, int* d_rev);
+void launch_adj_src(cudaStream_t st, const SimDev* d_sims, int nsrc, const float* gsig, const int* d_t, double* gc);
 void launch_adj_vel(cudaStream_t st, const SimDev* d_sims, long long N, const AdjStepArgs& a);
 void launch_adj_sum(cudaStream_t st, const SimDev* d_sims, long long N, const AdjStepArgs& a);
 void launch_adj_half_dtor(cudaStream_t st, const SimDev* d_sims, long long N, const AdjStepArgs& a);

@@ -125,6 +125,9 @@ enum Epilogue {
     EPI_ADD_U,           // u_{comp(o)} += d_o                                       (additive u source)
     EPI_ADD_RHO,         // rho_a += d_0 / d_a; rho_sum; EoS                          (additive p source)
     EPI_EOS_ABS,         // p = c2 (rho_sum + tau d_0 - eta d_1 + nonlinear)          (power law)
+    // discrete adjoint (kw_adjoint.cpp; register row kernels only)
+    EPI_ADJ_VEL,         // mu = lambda_u_a - d_a; lambda_u_a = sg_a^2 mu; w_a = sg_a dtor_a mu
+    EPI_ADJ_SUM,         // lambda_p = sum_a d_a; x1 = tau c2 lambda_p; x2 = eta c2 lambda_p
 };
 
 // Source operator of one field variable (SourceOp, KSpaceFirstOrder.swift:129-175).

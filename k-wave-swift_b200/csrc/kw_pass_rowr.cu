@@ -13,6 +13,7 @@
 // one after the other in the same CTA and park the finished ones in shared memory (each thread its
 // own slots). The epilogue reads its field inputs for a few pairs at a time before any store, so
 // their latencies overlap.
+#include "kw_adjoint.h"
 #include "kw_fft_reg.cuh"
 #include "kw_pass_common.cuh"
 
@@ -248,6 +249,58 @@ __global__ void __launch_bounds__(256) k_rowr_c2r(const SimDev* __restrict__ sim
                 if (EPI == EPI_DEN && S.absorb >= 1) st_state(S.div_term, e, dv2);
                 if (S.eos_pointwise) st_state(S.p, e, p2);
             }
+        } else if constexpr (EPI == EPI_ADJ_VEL) {
+            // adjoint of the velocity update (kw_adjoint.cu)
+            const int a = comp0;
+            float* lu = S.adj[ADJ_LU + a];
+            float* w = S.adj[ADJ_W + a];
+            const bool along_row = a == D - 1;
+            const float sgc = along_row ? 0.f : row_const(S.ax[a].pml_sg, a);
+            float2 uu[MB], dr[MB], sg[MB];
+#pragma unroll
+            for (int b = 0; b < MB; ++b) {
+                const int n = t + T * (m0 + b);
+                const long long e = rbase + 2 * n;
+                uu[b] = ld_state(lu, e);
+                dr[b] = ld_medium(S.dtor[a], e);
+                sg[b] = along_row ? row_pair(S.ax[a].pml_sg, n) : make_float2(sgc, sgc);
+            }
+#pragma unroll
+            for (int b = 0; b < MB; ++b) {
+                const float2 d = v[m0 + b];
+                float2 lo, wo;
+#pragma unroll
+                for (int h = 0; h < 2; ++h) {
+                    const float mu = half(uu[b], h) - (h ? d.y : d.x);
+                    half(lo, h) = half(sg[b], h) * half(sg[b], h) * mu;
+                    half(wo, h) = half(sg[b], h) * half(dr[b], h) * mu;
+                }
+                const long long e = rbase + 2 * (t + T * (m0 + b));
+                st_state(lu, e, lo);
+                st_state(w, e, wo);
+            }
+        } else if constexpr (EPI == EPI_ADJ_SUM) {
+            // lambda_p = sum_a d_a and the next reverse step's absorption inputs
+#pragma unroll
+            for (int b = 0; b < MB; ++b) {
+                const int m = m0 + b;
+                const long long e = rbase + 2 * (t + T * m);
+                float2 s2 = dpair(0, m);
+                for (int cc = 1; cc < ncomp; ++cc) {
+                    const float2 dp = dpair(cc, m);
+                    s2.x += dp.x;
+                    s2.y += dp.y;
+                }
+                st_state(S.adj[ADJ_LP], e, s2);
+                if (S.absorb >= 2) {
+                    const float2 c2 = ld_medium(S.c2, e), tau = ld_medium(S.tau, e);
+                    st_state(S.adj[ADJ_X1], e, make_float2(tau.x * c2.x * s2.x, tau.y * c2.y * s2.y));
+                    if (S.absorb == 3) {
+                        const float2 eta = ld_medium(S.eta, e);
+                        st_state(S.adj[ADJ_X2], e, make_float2(eta.x * c2.x * s2.x, eta.y * c2.y * s2.y));
+                    }
+                }
+            }
         } else if constexpr (EPI == EPI_EOS_ABS) {
             // power-law absorption / dispersion (KSpaceFirstOrder.swift:836-845)
             float2 rs[MB], c2[MB], tau[MB], eta[MB], bona[MB], r0[MB];
@@ -298,6 +351,7 @@ static void set_rowr_attrs(int optin) {
 void init_rowr_attributes(int optin) {
     set_rowr_attrs<EPI_DEN>(optin);
     set_rowr_attrs<EPI_EOS_ABS>(optin);
+    set_rowr_attrs<EPI_ADJ_SUM>(optin);
 }
 
 void launch_rowr_r2c(cudaStream_t st, const SimDev* d_sims, const int* d_t, const BlockWork* map, int nmap,
@@ -324,6 +378,8 @@ static void launch_c2r_m(cudaStream_t st, const SimDev* d_sims, const int* d_t, 
         case EPI_DEN: k_rowr_c2r<M, EPI_DEN><<<nmap, 256, smem, st>>>(d_sims, d_t, map, nmap, job); break;
         case EPI_ADD_RHO: k_rowr_c2r<M, EPI_ADD_RHO><<<nmap, 256, smem, st>>>(d_sims, d_t, map, nmap, job); break;
         case EPI_EOS_ABS: k_rowr_c2r<M, EPI_EOS_ABS><<<nmap, 256, smem, st>>>(d_sims, d_t, map, nmap, job); break;
+        case EPI_ADJ_VEL: k_rowr_c2r<M, EPI_ADJ_VEL><<<nmap, 256, smem, st>>>(d_sims, d_t, map, nmap, job); break;
+        case EPI_ADJ_SUM: k_rowr_c2r<M, EPI_ADJ_SUM><<<nmap, 256, smem, st>>>(d_sims, d_t, map, nmap, job); break;
         default: break;
     }
 }

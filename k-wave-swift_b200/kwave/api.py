@@ -241,6 +241,7 @@ class DescBuilder:
         options = options or SimulationOptions()
         self.keep: list[np.ndarray] = []
         self.grid = grid
+        self.medium, self.source, self.sensor, self.options = medium, source, sensor, options
         shape = grid.shape
         N = grid.totalGridPoints
         d = abi.kw_sim_desc()

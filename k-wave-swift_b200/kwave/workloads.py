@@ -7,6 +7,8 @@ configurations (no dataset is involved; numpy.random.default_rng(20261203 + conf
                  plane at z = 30, sensor = full xy plane at z = 200 recording p and pMax
   batch2d_64     64 uneven 2D grids (n in {128,192,256,384,512}), smooth random c0 maps,
                  16-point line source, 256-point Cartesian circle sensor
+  adjoint2d_512  512^2 adjoint gradient: 6 elliptical inclusions, power law y 1.1, smoothed p0
+                 of 10 discs, 512-point Cartesian ring, 1500 steps, c0 perturbed by 1%
 """
 from __future__ import annotations
 
@@ -108,3 +110,47 @@ def batch2d(count: int = 64, sizes=(128, 192, 256, 384, 512), steps: int | None 
         out.append(DescBuilder(g, KWaveMedium(c, 1000.0), KWaveSource(pMask=pm, p=sig, pMode=SourceMode.additive),
                                KWaveSensor(mask=sen, record=RecordField.p), SimulationOptions(pmlSize=20)))
     return out
+
+
+def _ellipses(shape, rng, count, c, s=1.0):
+    nx, ny = shape
+    X, Y = np.meshgrid(np.arange(nx), np.arange(ny), indexing="ij")
+    for _ in range(count):
+        a, b = rng.uniform(10 * s, 60 * s, size=2)
+        th = rng.uniform(0, math.pi)
+        m = 20 + 30 * s
+        cx, cy = rng.uniform(m, nx - m), rng.uniform(m, ny - m)
+        xr = (X - cx) * math.cos(th) + (Y - cy) * math.sin(th)
+        yr = -(X - cx) * math.sin(th) + (Y - cy) * math.cos(th)
+        c[(xr / a) ** 2 + (yr / b) ** 2 <= 1.0] = np.float32(rng.uniform(1420, 1600))
+
+
+def adjoint2d(n: int = 512, steps: int = 1500):
+    """The 2D adjoint-gradient configuration: returns (builder at the perturbed sound speed,
+    builder at the true sound speed). 512^2, dx 0.1 mm, PML 20, `steps` time steps at
+    dt = 0.3 dx / max(c_true); 6 elliptical inclusions (1420-1600 m/s) on 1500 m/s; rho 1000;
+    power law alpha 0.5 dB/(MHz^1.1 cm), y = 1.1; p0 = a smoothed sum of 10 discs; a 512-point
+    Cartesian ring of radius 240 dx recording p. The perturbed speed is c_true (1 + 0.01 N(0,1));
+    c_ref is held at max(c_true) for both."""
+    rng = np.random.default_rng(SEED + 3)
+    dx = 1e-4
+    shape = (n, n)
+    s = n / 512.0
+    c = np.full(shape, 1500.0, np.float32)
+    _ellipses(shape, rng, 6, c, s)
+    p0 = np.zeros(shape, np.float32)
+    for _ in range(10):
+        r = int(rng.integers(3, 13))
+        cx, cy = (int(v) for v in rng.integers(n // 4, 3 * n // 4, size=2))
+        p0 += makeDisc(n, n, cx, cy, r) * np.float32(rng.uniform(0.5, 1.5))
+    p0 = _gauss_smooth_wrap(p0, 1.5).astype(np.float32)   # smooth stand-in: Gaussian sigma 1.5 points
+    c_pert = (c * (1.0 + 0.01 * rng.standard_normal(shape))).astype(np.float32)
+    c_ref = float(c.max())
+    g = KWaveGrid(n, dx, n, dx)
+    g.setTime(steps, 0.3 * dx / c_ref)
+    sen = makeCartCircle(240 * s * dx, max(16, int(512 * s)))
+    def mk(cc):
+        med = KWaveMedium(cc, 1000.0, alphaCoeff=0.5, alphaPower=1.1, alphaMode=AbsorptionMode.powerLaw)
+        return DescBuilder(g, med, KWaveSource(p0=p0), KWaveSensor(mask=sen, record=RecordField.p),
+                           SimulationOptions(pmlSize=20, smoothP0=False, cRef=c_ref))
+    return mk(c_pert), mk(c)
