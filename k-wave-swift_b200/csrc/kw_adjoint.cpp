@@ -61,7 +61,15 @@ void Engine::adjoint(const kw_sim_desc& din, kw_adjoint_desc& a) {
         if (!v.spec[k]) v.spec[k] = (float2*)dalloc((size_t)h.Ns * sizeof(float2));
     // the register row kernels fuse the velocity-adjoint and summing steps into their epilogues
     const bool fused = h.C % 2 == 0 && has_reg_row(h.M);
+    // Folding the reverse equation of state into the absorption job's C2R saves its field traffic
+    // on large grids; on small (L2-resident, launch-bound) grids the separate elementwise kernel
+    // runs on more threads and is faster (2D 512^2: 3.13x against 3.24x forward time).
+    const bool eos_fused = N >= (1LL << 22);
     double* gc = (double*)dalloc((size_t)N * sizeof(double));
+    int* d_rev = (int*)dalloc(sizeof(int));
+    v.adj_gc = gc;
+    v.adj_rev = d_rev;
+    v.adj_y = y;
     check(cudaMemcpyAsync(d_sims_, &v, sizeof(SimDev), cudaMemcpyHostToDevice, st()), "upload sim");
 
     // ---- checkpoint policy ----
@@ -120,7 +128,6 @@ void Engine::adjoint(const kw_sim_desc& din, kw_adjoint_desc& a) {
         e.sprev = t == 0 ? zero_field : (slot > 0 ? tslot(slot - 1, 1) : ckf(t / K, 2 * D + 2));
     }
     const AdjTapeEntry* d_table = upload(table);
-    int* d_rev = (int*)dalloc(sizeof(int));
     auto tape_now = [&]() { launch_adj_tape(st(), d_sims_, d_t_, d_table, stokes, nonlin, N); };
 
     cudaEvent_t e0, e1, e2;
@@ -213,10 +220,14 @@ void Engine::adjoint(const kw_sim_desc& din, kw_adjoint_desc& a) {
     // for every step and run as a CUDA graph (one per variant: additive source active or not)
     auto reverse_body = [&](bool src_on) {
         launch_adj_begin(st(), d_sims_, d_t_, d_rev, d_table, d_resid, npts);   // also sets the step counter the pass kernels gate on
-        if (powerlaw) job(ADJ_X1, ADJ_A1, disp ? 3 : 1, absorption_op, EPI_STORE, 0, "adj_abs");
         if (nonlin) job(ADJ_UTP, ADJ_DD, D, deriv(AO_DNEG), EPI_STORE, 0, "adj_du");
         A.sig = src_on ? v.adj[ADJ_SIG] : nullptr;
-        launch_adj_eos(st(), d_sims_, N, A, d_rev);
+        if (powerlaw && fused && eos_fused) {   // the absorption filters with the reverse EoS as epilogue
+            job(ADJ_X1, ADJ_A1, disp ? 3 : 1, absorption_op, EPI_ADJ_EOS, 1, "adj_eos");
+        } else {
+            if (powerlaw) job(ADJ_X1, ADJ_A1, disp ? 3 : 1, absorption_op, EPI_STORE, 0, "adj_abs");
+            launch_adj_eos(st(), d_sims_, N, A, d_rev);
+        }
         if (src_on) {
             job(ADJ_SIG, ADJ_GSIG, 1, radial(RT_SKAPPA), EPI_STORE, 0, "adj_src");
             launch_adj_src(st(), d_sims_, v.psrc.nsrc, v.adj[ADJ_GSIG], d_t_, gc);

@@ -128,6 +128,7 @@ enum Epilogue {
     // discrete adjoint (kw_adjoint.cpp; register row kernels only)
     EPI_ADJ_VEL,         // mu = lambda_u_a - d_a; lambda_u_a = sg_a^2 mu; w_a = sg_a dtor_a mu
     EPI_ADJ_SUM,         // lambda_p = sum_a d_a; x1 = tau c2 lambda_p; x2 = eta c2 lambda_p
+    EPI_ADJ_EOS,         // the reverse equation of state (kw_adjoint.cu k_adj_eos) with d = A1, A2, A2(S)
 };
 
 // Source operator of one field variable (SourceOp, KSpaceFirstOrder.swift:129-175).
@@ -189,6 +190,9 @@ struct SimDev {
     float* tmp[kMaxComp];       // real scratch fields (collocated velocity etc.)
     float2* spec[4];
     float* adj[kAdjFields];     // adjoint work fields (kw_adjoint.cpp), unused by a forward run
+    double* adj_gc;             // adjoint: dL/dc accumulated in FP64
+    int* adj_rev;               // adjoint: the reverse step counter
+    float adj_y;                // adjoint: absorption power y
 
     // medium
     float dt;              // time step (FP32, multiplies rho0 like the reference's dt * rho0)

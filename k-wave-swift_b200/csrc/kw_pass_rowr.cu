@@ -79,7 +79,7 @@ __global__ void __launch_bounds__(256) k_rowr_c2r(const SimDev* __restrict__ sim
     using Lay = RowLayout<P, M>;
     constexpr int R1 = P::R1, T = P::T, TW = P::LINES;
     // pairs whose inputs are loaded together (the density update reads the most fields)
-    constexpr int MB = (EPI == EPI_DEN || R1 < 4) ? 2 : 4;
+    constexpr int MB = (EPI == EPI_DEN || EPI == EPI_ADJ_EOS || R1 < 4) ? 2 : 4;
     __shared__ float2 sh[Lay::SLOTS];
     extern __shared__ __align__(16) float2 parked[];   // coupled epilogues: [ncomp - 1][R1][256]
     if (blockIdx.x >= nmap) return;
@@ -301,6 +301,82 @@ __global__ void __launch_bounds__(256) k_rowr_c2r(const SimDev* __restrict__ sim
                     }
                 }
             }
+        } else if constexpr (EPI == EPI_ADJ_EOS) {
+            // the reverse equation of state of kw_adjoint.cu (k_adj_eos), with the absorption
+            // filters' outputs d = A1(tau c^2 lambda_p), A2(eta c^2 lambda_p), A2(S(t)) in hand
+            const int tt = *d_t;
+            const bool src_on = S.has_p && S.psrc.mode == 1 && tt < S.psrc.len;   // additive source active
+            if (m0 == 0 && blockIdx.x == 0 && threadIdx.x == 0) *S.adj_rev -= 1;
+            float pmc[kMaxComp - 1];
+#pragma unroll
+            for (int a = 0; a < kMaxComp - 1; ++a)
+                if (a < D - 1) pmc[a] = row_const(S.ax[a].pml, a);
+#pragma unroll
+            for (int b = 0; b < MB; ++b) {
+                const int m = m0 + b;
+                const int n = t + T * m;
+                const long long e = rbase + 2 * n;
+                const float2 lp = ld_state(S.adj[ADJ_LP], e), pv = ld_state(S.adj[ADJ_PTP], e), sv = ld_state(S.adj[ADJ_STP], e);
+                const float2 c2 = ld_medium(S.c2, e), r0 = ld_medium(S.rho0, e), tau = ld_medium(S.tau, e);
+                float2 eta = make_float2(0.f, 0.f), bona = eta, spv = eta;
+                if (S.absorb == 3) eta = ld_medium(S.eta, e);
+                if (S.nonlinear) { bona = ld_medium(S.bona, e); spv = ld_state(S.adj[ADJ_SPRP], e); }
+                float2 lr[kMaxComp], dd[kMaxComp];
+#pragma unroll
+                for (int a = 0; a < kMaxComp; ++a)
+                    if (a < D) {
+                        lr[a] = ld_state(S.adj[ADJ_LR + a], e);
+                        if (S.nonlinear) dd[a] = ld_state(S.adj[ADJ_DD + a], e);
+                    }
+                const float2 pmr = row_pair(S.ax[D - 1].pml, n);
+                const float2 a1 = dpair(0, m);
+                float2 a2 = make_float2(0.f, 0.f), q2 = a2;
+                if (S.absorb == 3) { a2 = dpair(1, m); q2 = dpair(2, m); }
+                double2 gcv = *reinterpret_cast<const double2*>(S.adj_gc + e);
+                float2 lro[kMaxComp], wo[kMaxComp], sg2;
+#pragma unroll
+                for (int h = 0; h < 2; ++h) {
+                    const float cc2 = h ? c2.y : c2.x, c = sqrtf(cc2);
+                    const float lpv = h ? lp.y : lp.x, p_ = h ? pv.y : pv.x, s_ = h ? sv.y : sv.x;
+                    const float rr0 = h ? r0.y : r0.x, ta = h ? tau.y : tau.x, et = h ? eta.y : eta.x;
+                    const float bo = h ? bona.y : bona.x;
+                    double E = (double)p_ / cc2 - s_;
+                    if (S.nonlinear) E -= (double)bo * s_ * s_ / (2.0 * rr0);
+                    double term = (double)(S.adj_y - 1.f) * E;
+                    if (S.absorb == 3) term -= (double)et * (h ? q2.y : q2.x);
+                    const double dpdc = 2.0 * (double)p_ / c + (double)c * term;
+                    if (h) gcv.y += (double)lpv * dpdc; else gcv.x += (double)lpv * dpdc;
+                    const float lE = cc2 * lpv;
+                    float lS = lE;
+                    if (S.nonlinear) lS += lE * bo * s_ / rr0;
+                    if (S.absorb == 3) lS -= h ? a2.y : a2.x;
+                    const float ldiv = h ? a1.y : a1.x;
+                    const float nl = S.nonlinear ? (2.f * (h ? spv.y : spv.x) + rr0) / rr0 : 1.f;
+                    const float dtr = S.dt * rr0;
+                    float lam[kMaxComp], pmv[kMaxComp];
+                    float lsprev = 0.f, sig = 0.f;
+#pragma unroll
+                    for (int a = 0; a < kMaxComp; ++a) {
+                        if (a >= D) break;
+                        pmv[a] = a == D - 1 ? (h ? pmr.y : pmr.x) : pmc[a < kMaxComp - 1 ? a : 0];
+                        lam[a] = (h ? lr[a].y : lr[a].x) + lS;
+                        half(wo[a], h) = rr0 * ldiv - pmv[a] * dtr * nl * lam[a];
+                        if (S.nonlinear) lsprev += -2.f * S.dt * pmv[a] * (h ? dd[a].y : dd[a].x) * lam[a];
+                        sig += lam[a] * S.ax[a].inv_d;
+                    }
+#pragma unroll
+                    for (int a = 0; a < kMaxComp; ++a) {
+                        if (a >= D) break;
+                        half(lro[a], h) = pmv[a] * pmv[a] * lam[a] + lsprev;
+                    }
+                    half(sg2, h) = sig;
+                }
+                *reinterpret_cast<double2*>(S.adj_gc + e) = gcv;
+#pragma unroll
+                for (int a = 0; a < kMaxComp; ++a)
+                    if (a < D) { st_state(S.adj[ADJ_LR + a], e, lro[a]); st_state(S.adj[ADJ_W + a], e, wo[a]); }
+                if (src_on) st_state(S.adj[ADJ_SIG], e, sg2);
+            }
         } else if constexpr (EPI == EPI_EOS_ABS) {
             // power-law absorption / dispersion (KSpaceFirstOrder.swift:836-845)
             float2 rs[MB], c2[MB], tau[MB], eta[MB], bona[MB], r0[MB];
@@ -352,6 +428,7 @@ void init_rowr_attributes(int optin) {
     set_rowr_attrs<EPI_DEN>(optin);
     set_rowr_attrs<EPI_EOS_ABS>(optin);
     set_rowr_attrs<EPI_ADJ_SUM>(optin);
+    set_rowr_attrs<EPI_ADJ_EOS>(optin);
 }
 
 void launch_rowr_r2c(cudaStream_t st, const SimDev* d_sims, const int* d_t, const BlockWork* map, int nmap,
@@ -380,6 +457,7 @@ static void launch_c2r_m(cudaStream_t st, const SimDev* d_sims, const int* d_t, 
         case EPI_EOS_ABS: k_rowr_c2r<M, EPI_EOS_ABS><<<nmap, 256, smem, st>>>(d_sims, d_t, map, nmap, job); break;
         case EPI_ADJ_VEL: k_rowr_c2r<M, EPI_ADJ_VEL><<<nmap, 256, smem, st>>>(d_sims, d_t, map, nmap, job); break;
         case EPI_ADJ_SUM: k_rowr_c2r<M, EPI_ADJ_SUM><<<nmap, 256, smem, st>>>(d_sims, d_t, map, nmap, job); break;
+        case EPI_ADJ_EOS: k_rowr_c2r<M, EPI_ADJ_EOS><<<nmap, 256, smem, st>>>(d_sims, d_t, map, nmap, job); break;
         default: break;
     }
 }
