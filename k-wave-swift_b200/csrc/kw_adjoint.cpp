@@ -12,6 +12,7 @@
 //    and the sum into lambda_p (register row kernels; separate kernels otherwise).
 // 4. The t = 0 override of an initial pressure gives dL/dp0 and its share of dL/dc0.
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <vector>
 
@@ -64,7 +65,9 @@ void Engine::adjoint(const kw_sim_desc& din, kw_adjoint_desc& a) {
     // Folding the reverse equation of state into the absorption job's C2R saves its field traffic
     // on large grids; on small (L2-resident, launch-bound) grids the separate elementwise kernel
     // runs on more threads and is faster (2D 512^2: 3.13x against 3.24x forward time).
-    const bool eos_fused = N >= (1LL << 22);
+    // KW_ADJOINT_FUSED_EOS=1 / 0 forces the choice.
+    bool eos_fused = N >= (1LL << 22);
+    if (const char* f = std::getenv("KW_ADJOINT_FUSED_EOS")) eos_fused = f[0] == '1';
     double* gc = (double*)dalloc((size_t)N * sizeof(double));
     int* d_rev = (int*)dalloc(sizeof(int));
     v.adj_gc = gc;

@@ -46,6 +46,21 @@ def test_device_adjoint_matches_fp64_adjoint_and_differences(shape, kw):
         assert abs(dL - np.sum(r["grad_c0"] * dx)) <= 1e-3 * abs(dL)
 
 
+@pytest.mark.parametrize("shape,kw", [((40, 64), dict(absorb="powerlaw", nonlinear=True, cartesian=True, nt=50)),
+                                      CASES[3], CASES[4], ((16, 20, 32), dict(absorb="powerlaw", nonlinear=False, nt=30))])
+def test_fused_reverse_eos_matches_fp64_adjoint(shape, kw, monkeypatch):
+    # the absorption job's C2R epilogue carries the reverse equation of state (chosen by default
+    # on large grids only; forced here)
+    monkeypatch.setenv("KW_ADJOINT_FUSED_EOS", "1")
+    c, p0, data, kw = problem(shape, **kw)
+    L, gc, gp = oracle.adjoint(builder(shape, c, p0, **kw), data)
+    r = gpu_adjoint(shape, c, p0, data, kw)
+    assert abs(r["misfit"] - L) <= 1e-3 * L
+    assert rel_l2(r["grad_c0"], gc) < 2e-3, rel_l2(r["grad_c0"], gc)
+    if p0 is not None:
+        assert rel_l2(r["grad_p0"], gp) < 2e-3, rel_l2(r["grad_p0"], gp)
+
+
 def test_checkpoint_policies_agree():
     shape = (40, 36)
     c, p0, data, kw = problem(shape, absorb="powerlaw", nonlinear=True, nt=45)
