@@ -137,7 +137,7 @@ def run_reference(args) -> None:
     threads = os.cpu_count() or 1
     if args.workload == BATCH:
         return run_reference_batch(args, threads)
-    if args.workload == ADJ:
+    if args.workload in (ADJ, ADJ3):
         return run_reference_adjoint(args, threads)
     b = workload(args.workload, 1)
     steps = max(1, min(args.steps or args.ref_steps, args.ref_steps))
@@ -295,6 +295,7 @@ def run_batch(args) -> None:
 
 
 ADJ = "adjoint2d_512"
+ADJ3 = "adjoint3d_384"
 
 
 def run_reference_adjoint(args, threads: int) -> None:
@@ -303,8 +304,9 @@ def run_reference_adjoint(args, threads: int) -> None:
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle
     from kwave import workloads
-    steps = max(2, min(args.steps or args.ref_steps, args.ref_steps) * 2)
-    bp, bt = workloads.adjoint2d(512, steps)
+    three_d = args.workload == ADJ3
+    steps = 2 if three_d else max(2, min(args.steps or args.ref_steps, args.ref_steps) * 2)
+    bp, bt = workloads.adjoint3d(384, steps) if three_d else workloads.adjoint2d(512, steps)
     data, _ = oracle.run(bt, nthreads=threads)
     t0 = time.perf_counter()
     oracle.adjoint(bp, data["p"], nthreads=threads)
@@ -314,9 +316,10 @@ def run_reference_adjoint(args, threads: int) -> None:
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": steps,
         "warmup": 0, "ms_per_step": 1e3 * secs / steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": ADJ, "grid": [512, 512], "what": "misfit gradient (forward + adjoint) per time step"},
+        "config": {"workload": args.workload, "grid": list(bp.shape),
+                   "what": "misfit gradient (forward + adjoint) per time step"},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
-                         "sample": f"first {steps} steps of the 512^2 adjoint problem: FP64 oracle forward + "
+                         "sample": f"first {steps} steps of the {args.workload} problem: FP64 oracle forward + "
                                    f"discrete adjoint, {threads} threads"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
@@ -343,7 +346,8 @@ def run_adjoint(args) -> None:
 
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
-    bp, bt = workloads.adjoint2d()
+    three_d = args.workload == ADJ3
+    bp, bt = workloads.adjoint3d() if three_d else workloads.adjoint2d()
     nt, npts = bp.grid.nt, bp.grid.totalGridPoints
     ctx = Context(local)
     stream = torch.cuda.Stream()
@@ -368,13 +372,22 @@ def run_adjoint(args) -> None:
         torch.cuda.synchronize()
         fwd_ms = e0.elapsed_time(e1)
         sim.close()
-        ctx.adjoint(bp, data, policy=abi.KW_CHECKPOINT_SQRT)   # warm-up of the adjoint path
+        if three_d:
+            # the checkpoint schedule sized to the free device memory (less room for the
+            # simulation's own fields and the adjoint's work fields)
+            torch.cuda.empty_cache()
+            free, _ = torch.cuda.mem_get_info()
+            budget = free - 40 * npts * 4 - (4 << 30)
+            opts = dict(policy=abi.KW_CHECKPOINT_BUDGET, memory_budget=float(budget))
+        else:
+            opts = dict(policy=abi.KW_CHECKPOINT_SQRT)
+            ctx.adjoint(bp, data, **opts)   # warm-up of the adjoint path
         t0 = time.perf_counter()
-        r = ctx.adjoint(bp, data, policy=abi.KW_CHECKPOINT_SQRT)
+        r = ctx.adjoint(bp, data, **opts)
         e2e_s = time.perf_counter() - t0
-        r_all = ctx.adjoint(bp, data, policy=abi.KW_CHECKPOINT_STORE_ALL)
+        r_all = None if three_d else ctx.adjoint(bp, data, policy=abi.KW_CHECKPOINT_STORE_ALL)
     grad_ms = r["forward_ms"] + r["reverse_ms"]
-    all_ms = r_all["forward_ms"] + r_all["reverse_ms"]
+    all_ms = r_all["forward_ms"] + r_all["reverse_ms"] if r_all else None
     if dist:
         t = torch.tensor([grad_ms, fwd_ms], device="cuda", dtype=torch.float64)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -385,14 +398,18 @@ def run_adjoint(args) -> None:
             "metric": METRIC, "value": npts * nt * world / (grad_ms / 1e3), "unit": UNIT, "n_gpus": world,
             "steps": nt, "warmup": args.warmup, "ms_per_step": grad_ms / nt, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": ADJ, "grid": [512, 512], "nt": nt, "sensor": "512-point Cartesian ring",
-                       "physics": "power law y=1.1 with dispersion, heterogeneous c0, p0",
-                       "l2": "small grid (fields L2-resident)", "parallelism": f"replicas{world}"},
+            "config": ({"workload": ADJ3, "grid": list(bp.shape), "nt": nt, "sensor": "128x128 receive plane",
+                        "physics": "3 layers + 8 spheres, power law y=1.5 with dispersion, B/A=5, focused 32x32 array",
+                        "l2": "inputs larger than L2", "parallelism": f"replicas{world}"} if three_d else
+                       {"workload": ADJ, "grid": [512, 512], "nt": nt, "sensor": "512-point Cartesian ring",
+                        "physics": "power law y=1.1 with dispersion, heterogeneous c0, p0",
+                        "l2": "small grid (fields L2-resident)", "parallelism": f"replicas{world}"}),
             "grad_over_forward": grad_ms / fwd_ms,
             "forward_ms": fwd_ms,
             "gradient_ms": {"checkpointed_forward": r["forward_ms"], "reverse_sweep": r["reverse_ms"]},
-            "checkpointing": {"policy": "sqrt(nt)", "interval": r["interval"], "checkpoints": r["checkpoints"]},
-            "store_all": {"gradient_ms": all_ms, "grad_over_forward": all_ms / fwd_ms},
+            "checkpointing": {"policy": "memory budget" if three_d else "sqrt(nt)", "interval": r["interval"],
+                              "checkpoints": r["checkpoints"]},
+            "store_all": {"gradient_ms": all_ms, "grad_over_forward": all_ms / fwd_ms} if all_ms else None,
             "misfit": r["misfit"], "grad_c0_l2": float(np.sqrt(np.sum(g.astype(np.float64) ** 2))),
             "roofline": None, "cpu_baseline": None,
             "e2e": {"value": npts * nt * world / e2e_s, "unit": UNIT,
@@ -563,7 +580,7 @@ def main() -> None:
         run_reference(args)
     elif args.workload == BATCH:
         run_batch(args)
-    elif args.workload == ADJ:
+    elif args.workload in (ADJ, ADJ3):
         run_adjoint(args)
     else:
         run_ours(args)

@@ -386,3 +386,23 @@ def kspaceFirstOrderAdjoint(grid: KWaveGrid, medium: KWaveMedium, source: KWaveS
     return AdjointOutput(r["misfit"], r["grad_c0"], r["grad_p0"], r["forward_ms"], r["reverse_ms"],
                          r["interval"], r["checkpoints"])
 
+
+def timeReversal(grid: KWaveGrid, medium: KWaveMedium, sensor: KWaveSensor, recordedPressure: np.ndarray,
+                 compensationFactor: float = 2.0, options: Optional[SimulationOptions] = None) -> np.ndarray:
+    """Time-reversal reconstruction (Sources/KWave/Reconstruction/TimeReversal.swift:20-51): the
+    recorded sensor pressure [n_sensor, nt], flipped in time, is re-injected as a Dirichlet
+    pressure source on the sensor mask; the solver runs forward over the whole grid and the final
+    pressure, scaled by `compensationFactor` and clipped at zero, is the estimate of p0."""
+    if sensor.mask is None:
+        raise KWaveError(abi.KW_ERR_INVALID, "time reversal requires sensor.mask")
+    if grid.nt <= 0:
+        raise KWaveError(abi.KW_ERR_INVALID, "set grid time (makeTime/setTime) before time reversal")
+    rec = np.asarray(recordedPressure, np.float32)
+    if rec.ndim != 2:
+        raise KWaveError(abi.KW_ERR_INVALID, "recordedPressure must be [numSensorPoints, nt]")
+    source = KWaveSource(pMask=np.asarray(sensor.mask, np.float32), p=np.ascontiguousarray(rec[:, ::-1]),
+                         pMode=SourceMode.dirichlet)
+    out = kspaceFirstOrder(grid, medium, source, KWaveSensor(), options)
+    p0 = out.pFinal * np.float32(compensationFactor)
+    return np.maximum(p0, np.float32(0))
+

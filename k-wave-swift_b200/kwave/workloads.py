@@ -9,6 +9,8 @@ configurations (no dataset is involved; numpy.random.default_rng(20261203 + conf
                  16-point line source, 256-point Cartesian circle sensor
   adjoint2d_512  512^2 adjoint gradient: 6 elliptical inclusions, power law y 1.1, smoothed p0
                  of 10 discs, 512-point Cartesian ring, 1500 steps, c0 perturbed by 1%
+  adjoint3d_384  384^3 forward + adjoint: 3 layers + 8 spheres, power law y 1.5, B/A 5, 32x32
+                 focused array at z = 25, 128x128 receive plane, 2000 steps, c0 perturbed by 1%
 """
 from __future__ import annotations
 
@@ -153,4 +155,64 @@ def adjoint2d(n: int = 512, steps: int = 1500):
         med = KWaveMedium(cc, 1000.0, alphaCoeff=0.5, alphaPower=1.1, alphaMode=AbsorptionMode.powerLaw)
         return DescBuilder(g, med, KWaveSource(p0=p0), KWaveSensor(mask=sen, record=RecordField.p),
                            SimulationOptions(pmlSize=20, smoothP0=False, cRef=c_ref))
+    return mk(c_pert), mk(c)
+
+
+def adjoint3d(n: int = 384, steps: int = 2000):
+    """The 3D forward + adjoint configuration: returns (builder at the perturbed sound speed,
+    builder at the true one). 384^3, dx 0.15 mm, PML 20, `steps` time steps; three planar z-layers
+    (c0 1480 / 1560 / 1620 m/s, rho0 1000 / 1050 / 1100, boundaries at z = n/3, 2n/3) with 8 random
+    spheres as in the 256^3 forward; power law alpha 0.75 dB/(MHz^1.5 cm) with dispersion, B/A 5;
+    a 32 x 32 array of single-point elements at pitch 4 on the plane z = 25, each a 1.5 MHz
+    3-cycle burst delayed to focus at the grid centre (one signal row per element); a centred
+    128 x 128 receive plane at z = 25 recording p. The perturbed speed is c_true (1 + 0.01 N(0,1));
+    c_ref is held at max(c_true)."""
+    rng = np.random.default_rng(SEED + 4)
+    s = n / 384.0
+    dx = 1.5e-4
+    shape = (n, n, n)
+    c = np.empty(shape, np.float32)
+    rho = np.empty(shape, np.float32)
+    z1, z2 = n // 3, 2 * n // 3
+    for (lo, hi), cv, rv in (((0, z1), 1480.0, 1000.0), ((z1, z2), 1560.0, 1050.0), ((z2, n), 1620.0, 1100.0)):
+        c[:, :, lo:hi] = cv
+        rho[:, :, lo:hi] = rv
+    _spheres(shape, rng, 8, max(2, int(round(8 * s))), max(3, int(round(30 * s))), int(round(20 * s)),
+             int(round(20 * s)), c, rho, (1400.0, 1650.0), (900.0, 1100.0))
+    c_ref = float(c.max())
+    g = KWaveGrid(n, dx, n, dx, n, dx)
+    g.makeTime(c_ref, cfl=0.3)
+    g.setTime(steps, g.dt)
+    # 32 x 32 elements at pitch 4 (scaled), centred, on z = 25 (scaled)
+    ne = max(2, int(round(32 * s)))
+    pitch = max(1, int(round(4 * s)))
+    z_src = max(1, int(round(25 * s)))
+    off = n // 2 - (ne * pitch) // 2
+    pm = np.zeros(shape, np.float32)
+    pos = []
+    for i in range(ne):
+        for j in range(ne):
+            pm[off + i * pitch, off + j * pitch, z_src] = 1
+            pos.append((off + i * pitch, off + j * pitch, z_src))
+    # rows follow the ascending flat index of the mask: x major, then y (z fixed)
+    pos.sort(key=lambda q: (q[0] * n + q[1]) * n + q[2])
+    centre = np.array([n // 2, n // 2, n // 2], np.float64)
+    dist = np.array([np.linalg.norm((np.array(q) - centre) * dx) for q in pos])
+    delays = (dist.max() - dist) / 1500.0
+    burst = toneBurst(1.0 / g.dt, 1.5e6, 3).astype(np.float64)
+    shift = np.round(delays / g.dt).astype(int)
+    length = len(burst) + int(shift.max())
+    sig = np.zeros((len(pos), length), np.float32)
+    for r, k in enumerate(shift):
+        sig[r, k:k + len(burst)] = burst * 1e5
+    sm = np.zeros(shape, np.float32)
+    h = max(1, int(round(64 * s)))
+    sm[n // 2 - h:n // 2 + h, n // 2 - h:n // 2 + h, z_src] = 1
+    c_pert = (c * (1.0 + 0.01 * rng.standard_normal(shape))).astype(np.float32)
+
+    def mk(cc):
+        med = KWaveMedium(cc, rho, alphaCoeff=0.75, alphaPower=1.5, alphaMode=AbsorptionMode.powerLaw, bOnA=5.0)
+        return DescBuilder(g, med, KWaveSource(pMask=pm, p=sig, pMode=SourceMode.additive),
+                           KWaveSensor(mask=sm, record=RecordField.p),
+                           SimulationOptions(pmlSize=max(4, int(round(20 * s))), cRef=c_ref))
     return mk(c_pert), mk(c)

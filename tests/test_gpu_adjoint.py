@@ -120,3 +120,17 @@ def _with_c(b, c):
     m = b.medium
     return DescBuilder(b.grid, KWaveMedium(c, m.density, alphaCoeff=m.alphaCoeff, alphaPower=m.alphaPower,
                                            alphaMode=m.alphaMode, bOnA=m.bOnA), b.source, b.sensor, b.options)
+
+
+def test_adjoint3d_configuration_replica():
+    """The 384^3 forward + adjoint configuration at 48^3 and 40 steps (same construction, scaled:
+    layers, spheres, focused element array, receive plane): the device gradient against the FP64
+    adjoint, with the memory-budget checkpoint schedule."""
+    from kwave import workloads
+    bp, bt = workloads.adjoint3d(48, 40)
+    data = oracle.run(bt)[0]["p"]
+    L, gc, _ = oracle.adjoint(bp, data)
+    r = Context.default().adjoint(bp, data, grad_c0=True, policy=abi.KW_CHECKPOINT_BUDGET, memory_budget=5e7)
+    assert r["checkpoints"] > 0
+    assert abs(r["misfit"] - L) <= 1e-3 * L
+    assert rel_l2(r["grad_c0"], gc) < 2e-3, rel_l2(r["grad_c0"], gc)

@@ -209,3 +209,25 @@ def test_kspace_first_order_api_progress_and_monitor():
     assert out.pFinal.shape == (n, n)
     assert steps == [(t, 12) for t in range(12)]
     assert [m[0] for m in mons] == [0, 5, 10] and all(m[1] == (n, n) for m in mons)
+
+
+def test_time_reversal_matches_oracle():
+    # the shape of ParityTests.swift:271-329: a disc p0 radiates to a circular sensor; the recorded
+    # pressure is re-injected time-reversed as a Dirichlet source; the compensated, clipped final
+    # pressure is the reconstruction
+    from kwave import timeReversal
+    n = 64
+    g = KWaveGrid(n, 1e-4, n, 1e-4)
+    g.makeTime(1500.0, cfl=0.3)
+    med = KWaveMedium(1500.0, 1000.0)
+    mask = makeCircle(n, n, radius=24)
+    fwd = DescBuilder(g, med, KWaveSource(p0=makeDisc(n, n, radius=4) * 1.0),
+                      KWaveSensor(mask=mask, record=RecordField.p), SimulationOptions(pmlSize=10))
+    rec = run_gpu(fwd)["p"]
+    mine = timeReversal(g, med, KWaveSensor(mask=mask), rec, compensationFactor=2.0,
+                        options=SimulationOptions(pmlSize=10))
+    tr = DescBuilder(g, med, KWaveSource(pMask=mask, p=np.ascontiguousarray(rec[:, ::-1]), pMode=SourceMode.dirichlet),
+                     KWaveSensor(), SimulationOptions(pmlSize=10))
+    ref = np.maximum(oracle.run(tr)[0]["pFinal"] * 2.0, 0.0)
+    assert rel_l2(mine, ref) < 1e-4, rel_l2(mine, ref)
+    assert rel_max(mine, ref) < 1e-4, rel_max(mine, ref)
