@@ -5,11 +5,12 @@
 //    KW_CHECKPOINT_STORE_ALL, the reverse sweep's inputs of every step.
 // 2. Residuals r_t = p_sensor(t) - data(t) and the misfit on the host (FP64).
 // 3. Reverse sweep, segment by segment from the last: restore the segment's checkpoint, rerun its
-//    steps storing p, S, div (Stokes) and u_a (B/A) of each step, then walk the segment backwards
-//    through the reverse step. The spectral pieces of a reverse step are ordinary jobs of the pass
-//    kernels on FS_ADJ fields (the transposed absorption filters with A2(S(t)), D-_a u_a for the
-//    B/A term, the source filter), and D+_a, D-_a whose C2R epilogues carry the velocity adjoint
-//    and the sum into lambda_p (register row kernels; separate kernels otherwise).
+//    steps storing p, S, div (Stokes) and d_a = D-_a u_a (B/A; the density epilogue stores it) of
+//    each step, then walk the segment backwards through the reverse step. The spectral pieces of
+//    a reverse step are ordinary jobs of the pass kernels on FS_ADJ fields (the transposed
+//    absorption filters with A2(S(t)), the source filter), and D+_a, D-_a whose C2R epilogues carry
+//    the velocity adjoint and the sum into lambda_p (register row kernels; separate kernels
+//    otherwise).
 // 4. The t = 0 override of an initial pressure gives dL/dp0 and its share of dL/dc0.
 #include <cmath>
 #include <cstdlib>
@@ -110,8 +111,8 @@ void Engine::adjoint(const kw_sim_desc& din, kw_adjoint_desc& a) {
     };
     std::vector<float*> tape = alloc_fields((size_t)K * tp_fields);
     std::vector<float*> ck = alloc_fields((size_t)nck * ck_fields);
-    auto tslot = [&](int slot, int f) { return tape[(size_t)slot * tp_fields + f]; };   // f: 0 p, 1 S, 2 div, then u_a
-    const int TF_DIV = 2, TF_U = stokes ? 3 : 2;
+    auto tslot = [&](int slot, int f) { return tape[(size_t)slot * tp_fields + f]; };   // f: 0 p, 1 S, 2 div, then d_a
+    const int TF_DIV = 2, TF_DD = stokes ? 3 : 2;
     auto ckf = [&](int c, int f) { return ck[(size_t)c * ck_fields + f]; };   // u_a, rho_a, S, p, S(t-1), div
     auto cpy = [&](float* dst, const float* src) {
         check(cudaMemcpyAsync(dst, src, fb, cudaMemcpyDeviceToDevice, st()), "adjoint copy");
@@ -127,11 +128,13 @@ void Engine::adjoint(const kw_sim_desc& din, kw_adjoint_desc& a) {
         e.p = tslot(slot, 0);
         e.s = tslot(slot, 1);
         e.div = stokes ? tslot(slot, TF_DIV) : nullptr;
-        for (int b = 0; b < kMaxComp; ++b) e.u[b] = nonlin && b < D ? tslot(slot, TF_U + b) : nullptr;
+        for (int b = 0; b < kMaxComp; ++b) e.dd[b] = nonlin && b < D ? tslot(slot, TF_DD + b) : nullptr;
         e.sprev = t == 0 ? zero_field : (slot > 0 ? tslot(slot - 1, 1) : ckf(t / K, 2 * D + 2));
     }
     const AdjTapeEntry* d_table = upload(table);
-    auto tape_now = [&]() { launch_adj_tape(st(), d_sims_, d_t_, d_table, stokes, nonlin, N); };
+    // copy p, S, div of the step just taken into the tape (the density epilogue stores d_a itself)
+    // and aim the density epilogue's d_a store at the next step's slot
+    auto tape_now = [&](int copy) { launch_adj_tape(st(), d_sims_, d_t_, d_table, nt, copy, stokes, nonlin, N); };
 
     cudaEvent_t e0, e1, e2;
     check(cudaEventCreate(&e0), "event");
@@ -141,6 +144,7 @@ void Engine::adjoint(const kw_sim_desc& din, kw_adjoint_desc& a) {
     // ---- 1. forward ----
     reset();
     check(cudaEventRecord(e0, st()), "event");
+    if (store_all) tape_now(0);
     for (int t = 0; t < nt; ++t) {
         const bool ck_step = !store_all && t % K == 0;
         if (ck_step) {
@@ -149,7 +153,7 @@ void Engine::adjoint(const kw_sim_desc& din, kw_adjoint_desc& a) {
             else cpy(ckf(c, 2 * D + 2), v.rho_sum);
         }
         step(1);
-        if (store_all) tape_now();
+        if (store_all) tape_now(1);
         if (ck_step) {
             const int c = t / K;
             for (int b = 0; b < D; ++b) { cpy(ckf(c, b), v.u[b]); cpy(ckf(c, D + b), v.rho[b]); }
@@ -191,7 +195,6 @@ void Engine::adjoint(const kw_sim_desc& din, kw_adjoint_desc& a) {
     A.lam_p = v.adj[ADJ_LP];
     for (int b = 0; b < kMaxComp; ++b) {
         const int bb = b < D ? b : 0;
-        A.dd[b] = v.adj[ADJ_DD + bb];
         A.lam_u[b] = v.adj[ADJ_LU + bb];
         A.lam_r[b] = v.adj[ADJ_LR + bb];
         A.w[b] = v.adj[ADJ_W + bb];
@@ -200,9 +203,9 @@ void Engine::adjoint(const kw_sim_desc& din, kw_adjoint_desc& a) {
     A.gc = gc;
     A.y = y;
 
-    auto job = [&](int in, int out, int nin, auto opf, int epi, int coupled, const char* name) {
+    auto job_in = [&](int in_field, int out, int nin, auto opf, int epi, int coupled, const char* name) {
         SpecJob j;
-        j.in_field = FS_ADJ + in;
+        j.in_field = in_field;
         j.nin = nin;
         j.nout = nin;
         for (int c = 0; c < nin; ++c) j.op[c] = opf(c);
@@ -214,6 +217,9 @@ void Engine::adjoint(const kw_sim_desc& din, kw_adjoint_desc& a) {
         j.name = name;
         issue_job(j, -1);
     };
+    auto job = [&](int in, int out, int nin, auto opf, int epi, int coupled, const char* name) {
+        job_in(FS_ADJ + in, out, nin, opf, epi, coupled, name);
+    };
     // absorption filters: x1 with |k|^(y-2); x2 and S(t) with |k|^(y-1)
     auto absorption_op = [](int c) { return OpSpec{AO_NONE, 0, (int8_t)(c == 0 ? RT_NU1 : RT_NU2), (int8_t)c}; };
     auto radial = [](int r) { return [r](int c) { return OpSpec{AO_NONE, 0, (int8_t)r, (int8_t)c}; }; };
@@ -223,7 +229,6 @@ void Engine::adjoint(const kw_sim_desc& din, kw_adjoint_desc& a) {
     // for every step and run as a CUDA graph (one per variant: additive source active or not)
     auto reverse_body = [&](bool src_on) {
         launch_adj_begin(st(), d_sims_, d_t_, d_rev, d_table, d_resid, npts);   // also sets the step counter the pass kernels gate on
-        if (nonlin) job(ADJ_UTP, ADJ_DD, D, deriv(AO_DNEG), EPI_STORE, 0, "adj_du");
         A.sig = src_on ? v.adj[ADJ_SIG] : nullptr;
         if (powerlaw && fused && eos_fused) {   // the absorption filters with the reverse EoS as epilogue
             job(ADJ_X1, ADJ_A1, disp ? 3 : 1, absorption_op, EPI_ADJ_EOS, 1, "adj_eos");
@@ -284,12 +289,17 @@ void Engine::adjoint(const kw_sim_desc& din, kw_adjoint_desc& a) {
             cpy(v.rho_sum, ckf(c, 2 * D));
             cpy(v.p, ckf(c, 2 * D + 1));
             if (stokes) cpy(v.div_term, ckf(c, 2 * D + 3));
+            if (nonlin) {   // d_a(t0) = D-_a u_a(t0) of the restored state into its tape slot
+                launch_set_step(st(), d_t_, t0);
+                launch_adj_views(st(), d_sims_, d_table, t0);
+                job_in(FS_U, ADJ_DDP, D, deriv(AO_DNEG), EPI_STORE, 0, "adj_du");
+            }
             launch_set_step(st(), d_t_, t0 + 1);
             t_ = t0 + 1;
-            tape_now();
+            tape_now(1);
             for (int t = t0 + 1; t < t1; ++t) {
                 step(1);
-                tape_now();
+                tape_now(1);
             }
             for (int t = t1 - 1; t >= std::max(t0, t_stop); --t) reverse_step(t);
         }

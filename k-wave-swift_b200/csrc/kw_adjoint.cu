@@ -35,17 +35,30 @@ __device__ __forceinline__ int layout_coord(const SimDev& S, long long i, int a)
 
 __global__ void k_set_step(int* d_t, int t) { *d_t = t; }
 
-__global__ void k_adj_tape(const SimDev* __restrict__ sims, const int* __restrict__ d_t,
-                           const AdjTapeEntry* __restrict__ table, int stokes, int nonlinear) {
-    const SimDev& S = sims[0];
-    const AdjTapeEntry e = table[*d_t - 1];
+__device__ __forceinline__ void set_views(SimDev& S, const AdjTapeEntry& e) {
+    S.adj[ADJ_PTP] = e.p;
+    S.adj[ADJ_STP] = e.s;
+    S.adj[ADJ_SPRP] = e.sprev;
+    S.adj[ADJ_DIVP] = e.div;
+    for (int b = 0; b < kMaxComp; ++b) S.adj[ADJ_DDP + b] = e.dd[b];
+}
+
+__global__ void k_adj_tape(SimDev* __restrict__ sims, const int* __restrict__ d_t, const AdjTapeEntry* __restrict__ table,
+                           int nt, int copy, int stokes, int nonlinear) {
+    SimDev& S = sims[0];
+    const int tn = *d_t;
     const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= S.N) return;
+    if (i == 0 && nonlinear)
+        for (int b = 0; b < kMaxComp; ++b) S.tape_dd[b] = tn < nt ? table[tn].dd[b] : nullptr;
+    if (!copy || i >= S.N) return;
+    const AdjTapeEntry e = table[tn - 1];
     e.p[i] = S.p[i];
     e.s[i] = S.rho_sum[i];
     if (stokes) e.div[i] = S.div_term[i];
-    if (nonlinear)
-        for (int b = 0; b < S.dim; ++b) e.u[b][i] = S.u[b][i];
+}
+
+__global__ void k_adj_views(SimDev* __restrict__ sims, const AdjTapeEntry* __restrict__ table, int t) {
+    set_views(sims[0], table[t]);
 }
 
 // Start of a reverse step: t = *d_rev (counted down by k_adj_eos); thread 0 sets the step counter
@@ -58,12 +71,7 @@ __global__ void k_adj_begin(SimDev* __restrict__ sims, int* __restrict__ d_t, co
     const int t = *d_rev;
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         *d_t = t;
-        const AdjTapeEntry e = table[t];
-        S.adj[ADJ_PTP] = e.p;
-        S.adj[ADJ_STP] = e.s;
-        S.adj[ADJ_SPRP] = e.sprev;
-        S.adj[ADJ_DIVP] = e.div;
-        for (int b = 0; b < kMaxComp; ++b) S.adj[ADJ_UTP + b] = e.u[b];
+        set_views(S, table[t]);
     }
     const SensorDev& sn = S.sensor;
     const int q = blockIdx.x * blockDim.x + threadIdx.x;
@@ -122,7 +130,7 @@ __global__ void k_adj_eos(const SimDev* __restrict__ sims, AdjStepArgs A, int* _
         pm[a] = __ldg(S.ax[a].pml + layout_coord(S, i, a));
         lam[a] = A.lam_r[a][i] + lS;
         A.w[a][i] = r0 * ldiv - pm[a] * dtr * nl * lam[a];
-        if (S.nonlinear) lsprev += -2.f * S.dt * pm[a] * A.dd[a][i] * lam[a];
+        if (S.nonlinear) lsprev += -2.f * S.dt * pm[a] * S.adj[ADJ_DDP + a][i] * lam[a];
         sig += lam[a] * S.ax[a].inv_d;
     }
 #pragma unroll
@@ -212,9 +220,12 @@ void launch_adj_begin(cudaStream_t st, SimDev* d_sims, int* d_t, const int* d_re
                       const float* resid, int npts) {
     k_adj_begin<<<blocks(npts > 0 ? npts : 1), 256, 0, st>>>(d_sims, d_t, d_rev, table, resid);
 }
-void launch_adj_tape(cudaStream_t st, const SimDev* d_sims, const int* d_t, const AdjTapeEntry* table, int stokes,
-                     int nonlinear, long long N) {
-    k_adj_tape<<<blocks(N), 256, 0, st>>>(d_sims, d_t, table, stokes, nonlinear);
+void launch_adj_tape(cudaStream_t st, SimDev* d_sims, const int* d_t, const AdjTapeEntry* table, int nt, int copy,
+                     int stokes, int nonlinear, long long N) {
+    k_adj_tape<<<blocks(N), 256, 0, st>>>(d_sims, d_t, table, nt, copy, stokes, nonlinear);
+}
+void launch_adj_views(cudaStream_t st, SimDev* d_sims, const AdjTapeEntry* table, int t) {
+    k_adj_views<<<1, 1, 0, st>>>(d_sims, table, t);
 }
 void launch_adj_eos(cudaStream_t st, const SimDev* d_sims, long long N, const AdjStepArgs& a, int* d_rev) {
     k_adj_eos<<<blocks(N), 256, 0, st>>>(d_sims, a, d_rev);

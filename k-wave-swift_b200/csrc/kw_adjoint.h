@@ -22,8 +22,8 @@ enum AdjField {
     ADJ_Q2 = 18,      // A2(S(t))              }
     ADJ_SIG = 19,     // sum_a L_a / dx_a
     ADJ_GSIG = 20,    // G(sigma)
-    ADJ_UTP = 21,     // u_a(t) (points into the tape), 3
-    ADJ_DD = 24,      // D-_a u_a(t), 3
+    ADJ_DDP = 21,     // d_a(t) = D-_a u_a(t) (points into the tape), 3
+    ADJ_SPARE = 24,   // 3 unused
     ADJ_PTP = 27,     // p(t)   (points into the tape)
     ADJ_SPRP = 28,    // S(t-1) (points into the tape, a checkpoint or a zero field)
     ADJ_DIVP = 29,    // div(t) (points into the tape; Stokes)
@@ -31,7 +31,8 @@ enum AdjField {
 };
 // entries that point into the tape instead of owning a field
 __host__ __device__ constexpr bool adj_is_view(int k) {
-    return k == ADJ_STP || (k >= ADJ_UTP && k < ADJ_UTP + 3) || k == ADJ_PTP || k == ADJ_SPRP || k == ADJ_DIVP;
+    return k == ADJ_STP || (k >= ADJ_DDP && k < ADJ_DDP + 3) || (k >= ADJ_SPARE && k < ADJ_SPARE + 3) || k == ADJ_PTP ||
+           k == ADJ_SPRP || k == ADJ_DIVP;
 }
 
 // where the reverse sweep finds the forward quantities of step t (one entry per step, device memory)
@@ -40,7 +41,7 @@ struct AdjTapeEntry {
     float* s;
     float* sprev;
     float* div;
-    float* u[kMaxComp];
+    float* dd[kMaxComp];   // d_a(t) = D-_a u_a(t) (B/A)
 };
 static_assert(ADJ_COUNT <= kAdjFields, "adjoint fields");
 
@@ -49,7 +50,6 @@ struct AdjStepArgs {
     const float* a1;
     const float* a2;
     const float* q2;
-    const float* dd[kMaxComp];
     float* lam_p;
     float* lam_u[kMaxComp];
     float* lam_r[kMaxComp];
@@ -67,9 +67,12 @@ void launch_set_step(cudaStream_t st, int* d_t, int t);
 // lambda_p += Sample^T r_t, and x1 = tau c^2 lambda_p, x2 = eta c^2 lambda_p at the same points.
 void launch_adj_begin(cudaStream_t st, SimDev* d_sims, int* d_t, const int* d_rev, const AdjTapeEntry* table,
                       const float* resid, int npts);
-// after forward step t (*d_t = t + 1): copy p, S, div, u_a into table[t]
-void launch_adj_tape(cudaStream_t st, const SimDev* d_sims, const int* d_t, const AdjTapeEntry* table, int stokes,
-                     int nonlinear, long long N);
+// around forward steps: with `copy`, copy p, S, div of step t = *d_t - 1 into table[t]; then
+// point the density epilogue's d_a store at table[*d_t].dd (null past the end)
+void launch_adj_tape(cudaStream_t st, SimDev* d_sims, const int* d_t, const AdjTapeEntry* table, int nt, int copy,
+                     int stokes, int nonlinear, long long N);
+// point the tape views of the work fields at table[t] (no step counter change)
+void launch_adj_views(cudaStream_t st, SimDev* d_sims, const AdjTapeEntry* table, int t);
 void launch_adj_eos(cudaStream_t st, const SimDev* d_sims, long long N, const AdjStepArgs& a, int* d_rev);
 void launch_adj_src(cudaStream_t st, const SimDev* d_sims, int nsrc, const float* gsig, const int* d_t, double* gc);
 void launch_adj_vel(cudaStream_t st, const SimDev* d_sims, long long N, const AdjStepArgs& a);

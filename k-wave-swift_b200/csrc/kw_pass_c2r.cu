@@ -134,6 +134,7 @@ __device__ __forceinline__ void epi_point(const SimDev& S, const RowC2RJob& job,
                 const float mass = S.nonlinear ? dtr * d[a] * nl : dtr * d[a];
                 const float r = pm * (pm * av(AX_F0 + a) - mass);
                 S.rho[a][i] = r;
+                if (S.tape_dd[a]) S.tape_dd[a][i] = d[a];   // the adjoint's recompute keeps d_a
                 rs = a == 0 ? r : rs + r;
                 dv = a == 0 ? d[a] : dv + d[a];
             }

@@ -245,6 +245,11 @@ __global__ void __launch_bounds__(256) k_rowr_c2r(const SimDev* __restrict__ sim
 #pragma unroll
                 for (int a = 0; a < kMaxComp; ++a)
                     if (a < D) st_state(S.rho[a], e, rn[a]);
+                if (EPI == EPI_DEN && S.tape_dd[0]) {   // the adjoint's recompute keeps d_a = D-_a u_a
+#pragma unroll
+                    for (int a = 0; a < kMaxComp; ++a)
+                        if (a < D) st_state(S.tape_dd[a], e, dpair(a, m));
+                }
                 st_state(S.rho_sum, e, rs2);
                 if (EPI == EPI_DEN && S.absorb >= 1) st_state(S.div_term, e, dv2);
                 if (S.eos_pointwise) st_state(S.p, e, p2);
@@ -326,7 +331,7 @@ __global__ void __launch_bounds__(256) k_rowr_c2r(const SimDev* __restrict__ sim
                 for (int a = 0; a < kMaxComp; ++a)
                     if (a < D) {
                         lr[a] = ld_state(S.adj[ADJ_LR + a], e);
-                        if (S.nonlinear) dd[a] = ld_state(S.adj[ADJ_DD + a], e);
+                        if (S.nonlinear) dd[a] = ld_state(S.adj[ADJ_DDP + a], e);
                     }
                 const float2 pmr = row_pair(S.ax[D - 1].pml, n);
                 const float2 a1 = dpair(0, m);
