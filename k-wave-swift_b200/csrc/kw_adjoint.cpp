@@ -67,6 +67,10 @@ void Engine::adjoint(const kw_sim_desc& din, kw_adjoint_desc& a) {
     // on large grids; on small (L2-resident, launch-bound) grids the separate elementwise kernel
     // runs on more threads and is faster (2D 512^2: 3.13x against 3.24x forward time).
     // KW_ADJOINT_FUSED_EOS=1 / 0 forces the choice.
+    // the summing step's operator pass adds up the components' spectra (register column kernel)
+    const int last_n = D == 3 ? h.A : h.B;
+    bool fanin = fused && D >= 2 && has_fixed_kernel(last_n) && has_colop(last_n);
+    if (const char* f = std::getenv("KW_ADJOINT_FANIN")) fanin = fanin && f[0] == '1';
     bool eos_fused = N >= (1LL << 22);
     if (const char* f = std::getenv("KW_ADJOINT_FUSED_EOS")) eos_fused = f[0] == '1';
     double* gc = (double*)dalloc((size_t)N * sizeof(double));
@@ -79,7 +83,7 @@ void Engine::adjoint(const kw_sim_desc& din, kw_adjoint_desc& a) {
     // ---- checkpoint policy ----
     const bool stokes = v.absorb == 1;   // the Stokes term reads div(t); the power law only p(t), S(t)
     const int ck_fields = 2 * D + 3 + (stokes ? 1 : 0);   // u_a, rho_a, S, p, S(t-1), div
-    const int tp_fields = 2 + (stokes ? 1 : 0) + (nonlin ? D : 0);   // p, S, div, u_a
+    const int tp_fields = 2 + (stokes ? 1 : 0) + (nonlin ? D : 0) + (disp ? 1 : 0);   // p, S, div, d_a, A2(S)
     bool store_all = a.policy == KW_CHECKPOINT_STORE_ALL;
     int K = 1;
     if (a.policy == KW_CHECKPOINT_SQRT) K = (int)std::ceil(std::sqrt((double)nt));
@@ -111,8 +115,8 @@ void Engine::adjoint(const kw_sim_desc& din, kw_adjoint_desc& a) {
     };
     std::vector<float*> tape = alloc_fields((size_t)K * tp_fields);
     std::vector<float*> ck = alloc_fields((size_t)nck * ck_fields);
-    auto tslot = [&](int slot, int f) { return tape[(size_t)slot * tp_fields + f]; };   // f: 0 p, 1 S, 2 div, then d_a
-    const int TF_DIV = 2, TF_DD = stokes ? 3 : 2;
+    auto tslot = [&](int slot, int f) { return tape[(size_t)slot * tp_fields + f]; };   // f: 0 p, 1 S, 2 div, then d_a, A2(S)
+    const int TF_DIV = 2, TF_DD = stokes ? 3 : 2, TF_Q2 = TF_DD + (nonlin ? D : 0);
     auto ckf = [&](int c, int f) { return ck[(size_t)c * ck_fields + f]; };   // u_a, rho_a, S, p, S(t-1), div
     auto cpy = [&](float* dst, const float* src) {
         check(cudaMemcpyAsync(dst, src, fb, cudaMemcpyDeviceToDevice, st()), "adjoint copy");
@@ -129,12 +133,13 @@ void Engine::adjoint(const kw_sim_desc& din, kw_adjoint_desc& a) {
         e.s = tslot(slot, 1);
         e.div = stokes ? tslot(slot, TF_DIV) : nullptr;
         for (int b = 0; b < kMaxComp; ++b) e.dd[b] = nonlin && b < D ? tslot(slot, TF_DD + b) : nullptr;
+        e.q2 = disp ? tslot(slot, TF_Q2) : nullptr;
         e.sprev = t == 0 ? zero_field : (slot > 0 ? tslot(slot - 1, 1) : ckf(t / K, 2 * D + 2));
     }
     const AdjTapeEntry* d_table = upload(table);
-    // copy p, S, div of the step just taken into the tape (the density epilogue stores d_a itself)
-    // and aim the density epilogue's d_a store at the next step's slot
-    auto tape_now = [&](int copy) { launch_adj_tape(st(), d_sims_, d_t_, d_table, nt, copy, stokes, nonlin, N); };
+    // copy p, S, div of the step just taken into the tape (the density and dispersion epilogues
+    // store d_a and A2(S) themselves) and aim those stores at the next step's slot
+    auto tape_now = [&](int copy) { launch_adj_tape(st(), d_sims_, d_t_, d_table, nt, copy, stokes, N); };
 
     cudaEvent_t e0, e1, e2;
     check(cudaEventCreate(&e0), "event");
@@ -191,7 +196,6 @@ void Engine::adjoint(const kw_sim_desc& din, kw_adjoint_desc& a) {
     AdjStepArgs A{};
     A.a1 = v.adj[ADJ_A1];
     A.a2 = v.adj[ADJ_A2];
-    A.q2 = v.adj[ADJ_Q2];
     A.lam_p = v.adj[ADJ_LP];
     for (int b = 0; b < kMaxComp; ++b) {
         const int bb = b < D ? b : 0;
@@ -203,11 +207,12 @@ void Engine::adjoint(const kw_sim_desc& din, kw_adjoint_desc& a) {
     A.gc = gc;
     A.y = y;
 
-    auto job_in = [&](int in_field, int out, int nin, auto opf, int epi, int coupled, const char* name) {
+    auto job_in = [&](int in_field, int out, int nin, auto opf, int epi, int coupled, const char* name, int fanin = 0) {
         SpecJob j;
         j.in_field = in_field;
         j.nin = nin;
-        j.nout = nin;
+        j.nout = fanin ? 1 : nin;
+        j.fanin = fanin ? nin : 0;
         for (int c = 0; c < nin; ++c) j.op[c] = opf(c);
         j.spec_in = 0;
         j.spec_out = 0;
@@ -217,10 +222,10 @@ void Engine::adjoint(const kw_sim_desc& din, kw_adjoint_desc& a) {
         j.name = name;
         issue_job(j, -1);
     };
-    auto job = [&](int in, int out, int nin, auto opf, int epi, int coupled, const char* name) {
-        job_in(FS_ADJ + in, out, nin, opf, epi, coupled, name);
+    auto job = [&](int in, int out, int nin, auto opf, int epi, int coupled, const char* name, int fanin = 0) {
+        job_in(FS_ADJ + in, out, nin, opf, epi, coupled, name, fanin);
     };
-    // absorption filters: x1 with |k|^(y-2); x2 and S(t) with |k|^(y-1)
+    // absorption filters: x1 with |k|^(y-2); x2 with |k|^(y-1) (A2(S(t)) comes from the tape)
     auto absorption_op = [](int c) { return OpSpec{AO_NONE, 0, (int8_t)(c == 0 ? RT_NU1 : RT_NU2), (int8_t)c}; };
     auto radial = [](int r) { return [r](int c) { return OpSpec{AO_NONE, 0, (int8_t)r, (int8_t)c}; }; };
     auto deriv = [](int ao) { return [ao](int c) { return OpSpec{(int8_t)ao, (int8_t)c, RT_KAPPA, (int8_t)c}; }; };
@@ -231,9 +236,9 @@ void Engine::adjoint(const kw_sim_desc& din, kw_adjoint_desc& a) {
         launch_adj_begin(st(), d_sims_, d_t_, d_rev, d_table, d_resid, npts);   // also sets the step counter the pass kernels gate on
         A.sig = src_on ? v.adj[ADJ_SIG] : nullptr;
         if (powerlaw && fused && eos_fused) {   // the absorption filters with the reverse EoS as epilogue
-            job(ADJ_X1, ADJ_A1, disp ? 3 : 1, absorption_op, EPI_ADJ_EOS, 1, "adj_eos");
+            job(ADJ_X1, ADJ_A1, disp ? 2 : 1, absorption_op, EPI_ADJ_EOS, 1, "adj_eos");
         } else {
-            if (powerlaw) job(ADJ_X1, ADJ_A1, disp ? 3 : 1, absorption_op, EPI_STORE, 0, "adj_abs");
+            if (powerlaw) job(ADJ_X1, ADJ_A1, disp ? 2 : 1, absorption_op, EPI_STORE, 0, "adj_abs");
             launch_adj_eos(st(), d_sims_, N, A, d_rev);
         }
         if (src_on) {
@@ -242,7 +247,9 @@ void Engine::adjoint(const kw_sim_desc& din, kw_adjoint_desc& a) {
         }
         if (fused) {
             job(ADJ_W, ADJ_E, D, deriv(AO_DPOS), EPI_ADJ_VEL, 0, "adj_vel");
-            job(ADJ_W, ADJ_E, D, deriv(AO_DNEG), EPI_ADJ_SUM, 1, "adj_sum");
+            // lambda_p = sum_a D-_a w_a: the operator pass sums the components' spectra, so one
+            // inverse transform serves all of them
+            job(ADJ_W, ADJ_E, D, deriv(AO_DNEG), EPI_ADJ_SUM, 1, "adj_sum", fanin ? 1 : 0);
         } else {
             job(ADJ_W, ADJ_E, D, deriv(AO_DPOS), EPI_STORE, 0, "adj_dpos");
             launch_adj_vel(st(), d_sims_, N, A);
@@ -289,10 +296,11 @@ void Engine::adjoint(const kw_sim_desc& din, kw_adjoint_desc& a) {
             cpy(v.rho_sum, ckf(c, 2 * D));
             cpy(v.p, ckf(c, 2 * D + 1));
             if (stokes) cpy(v.div_term, ckf(c, 2 * D + 3));
-            if (nonlin) {   // d_a(t0) = D-_a u_a(t0) of the restored state into its tape slot
+            if (nonlin || disp) {   // d_a(t0) = D-_a u_a(t0), A2(S(t0)) of the restored state into its tape slot
                 launch_set_step(st(), d_t_, t0);
                 launch_adj_views(st(), d_sims_, d_table, t0);
-                job_in(FS_U, ADJ_DDP, D, deriv(AO_DNEG), EPI_STORE, 0, "adj_du");
+                if (nonlin) job_in(FS_U, ADJ_DDP, D, deriv(AO_DNEG), EPI_STORE, 0, "adj_du");
+                if (disp) job_in(FS_RHO_SUM, ADJ_Q2, 1, radial(RT_NU2), EPI_STORE, 0, "adj_q2");
             }
             launch_set_step(st(), d_t_, t0 + 1);
             t_ = t0 + 1;

@@ -12,7 +12,8 @@
 // Reverse (lambda_x = dL/dx of the state after step t):
 //   lambda_p += Sample^T r_t
 //   dL/dc  += lambda_p (2 p / c + c ((y-1) tau A1(div) - y eta A2(S)))      (Stokes: + c tau div)
-//             with tau A1(div) - eta A2(S) = p / c^2 - S - B/A S^2 / (2 rho0), so only A2(S) is transformed
+//             with tau A1(div) - eta A2(S) = p / c^2 - S - B/A S^2 / (2 rho0), so only A2(S) is needed:
+//             the forward (recompute) step's dispersion epilogue keeps it on the tape
 //   lE = c^2 lambda_p;  lS = lE + lE B/A S / rho0 - A2(eta lE);  ldiv = A1(tau lE) (Stokes: tau lE)
 //   L_a = lambda_rho_a + lS;  source: dL/dc_i += G(sum_a L_a / dx_a)_i sig (-scale_i / c_i)
 //   w_a = rho0 ldiv - pm_a dt rho0 nl L_a
@@ -41,15 +42,18 @@ __device__ __forceinline__ void set_views(SimDev& S, const AdjTapeEntry& e) {
     S.adj[ADJ_SPRP] = e.sprev;
     S.adj[ADJ_DIVP] = e.div;
     for (int b = 0; b < kMaxComp; ++b) S.adj[ADJ_DDP + b] = e.dd[b];
+    S.adj[ADJ_Q2] = e.q2;
 }
 
 __global__ void k_adj_tape(SimDev* __restrict__ sims, const int* __restrict__ d_t, const AdjTapeEntry* __restrict__ table,
-                           int nt, int copy, int stokes, int nonlinear) {
+                           int nt, int copy, int stokes) {
     SimDev& S = sims[0];
     const int tn = *d_t;
     const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i == 0 && nonlinear)
+    if (i == 0) {
         for (int b = 0; b < kMaxComp; ++b) S.tape_dd[b] = tn < nt ? table[tn].dd[b] : nullptr;
+        S.tape_q2 = tn < nt ? table[tn].q2 : nullptr;
+    }
     if (!copy || i >= S.N) return;
     const AdjTapeEntry e = table[tn - 1];
     e.p[i] = S.p[i];
@@ -109,7 +113,7 @@ __global__ void k_adj_eos(const SimDev* __restrict__ sims, AdjStepArgs A, int* _
         double E = (double)pv / c2 - sv;
         if (S.nonlinear) E -= (double)S.bona.at(i) * sv * sv / (2.0 * r0);
         double term = (double)(A.y - 1.f) * E;
-        if (S.absorb == 3) term -= (double)S.eta.at(i) * A.q2[i];
+        if (S.absorb == 3) term -= (double)S.eta.at(i) * S.adj[ADJ_Q2][i];
         dpdc += (double)c * term;
     }
     A.gc[i] += (double)lp * dpdc;
@@ -221,8 +225,8 @@ void launch_adj_begin(cudaStream_t st, SimDev* d_sims, int* d_t, const int* d_re
     k_adj_begin<<<blocks(npts > 0 ? npts : 1), 256, 0, st>>>(d_sims, d_t, d_rev, table, resid);
 }
 void launch_adj_tape(cudaStream_t st, SimDev* d_sims, const int* d_t, const AdjTapeEntry* table, int nt, int copy,
-                     int stokes, int nonlinear, long long N) {
-    k_adj_tape<<<blocks(N), 256, 0, st>>>(d_sims, d_t, table, nt, copy, stokes, nonlinear);
+                     int stokes, long long N) {
+    k_adj_tape<<<blocks(N), 256, 0, st>>>(d_sims, d_t, table, nt, copy, stokes);
 }
 void launch_adj_views(cudaStream_t st, SimDev* d_sims, const AdjTapeEntry* table, int t) {
     k_adj_views<<<1, 1, 0, st>>>(d_sims, table, t);

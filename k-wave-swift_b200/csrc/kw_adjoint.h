@@ -14,12 +14,12 @@ enum AdjField {
     ADJ_LP = 6,       // lambda_p
     ADJ_W = 7,        // w[a] (job inputs), 3
     ADJ_E = 10,       // e[a] (job outputs), 3
-    ADJ_X1 = 13,      // tau c^2 lambda_p      } absorption job inputs: NU1, NU2, NU2
+    ADJ_X1 = 13,      // tau c^2 lambda_p      } absorption job inputs: NU1, NU2
     ADJ_X2 = 14,      // eta c^2 lambda_p      }
-    ADJ_STP = 15,     // S(t) (points into the tape) }
+    ADJ_STP = 15,     // S(t) (points into the tape)
     ADJ_A1 = 16,      // A1(tau c^2 lambda_p)  } outputs
     ADJ_A2 = 17,      // A2(eta c^2 lambda_p)  }
-    ADJ_Q2 = 18,      // A2(S(t))              }
+    ADJ_Q2 = 18,      // A2(S(t)) (points into the tape)
     ADJ_SIG = 19,     // sum_a L_a / dx_a
     ADJ_GSIG = 20,    // G(sigma)
     ADJ_DDP = 21,     // d_a(t) = D-_a u_a(t) (points into the tape), 3
@@ -31,7 +31,7 @@ enum AdjField {
 };
 // entries that point into the tape instead of owning a field
 __host__ __device__ constexpr bool adj_is_view(int k) {
-    return k == ADJ_STP || (k >= ADJ_DDP && k < ADJ_DDP + 3) || (k >= ADJ_SPARE && k < ADJ_SPARE + 3) || k == ADJ_PTP ||
+    return k == ADJ_STP || k == ADJ_Q2 || (k >= ADJ_DDP && k < ADJ_DDP + 3) || (k >= ADJ_SPARE && k < ADJ_SPARE + 3) || k == ADJ_PTP ||
            k == ADJ_SPRP || k == ADJ_DIVP;
 }
 
@@ -42,6 +42,7 @@ struct AdjTapeEntry {
     float* sprev;
     float* div;
     float* dd[kMaxComp];   // d_a(t) = D-_a u_a(t) (B/A)
+    float* q2;             // A2(S(t)) (power law with dispersion)
 };
 static_assert(ADJ_COUNT <= kAdjFields, "adjoint fields");
 
@@ -49,7 +50,6 @@ static_assert(ADJ_COUNT <= kAdjFields, "adjoint fields");
 struct AdjStepArgs {
     const float* a1;
     const float* a2;
-    const float* q2;
     float* lam_p;
     float* lam_u[kMaxComp];
     float* lam_r[kMaxComp];
@@ -68,9 +68,10 @@ void launch_set_step(cudaStream_t st, int* d_t, int t);
 void launch_adj_begin(cudaStream_t st, SimDev* d_sims, int* d_t, const int* d_rev, const AdjTapeEntry* table,
                       const float* resid, int npts);
 // around forward steps: with `copy`, copy p, S, div of step t = *d_t - 1 into table[t]; then
-// point the density epilogue's d_a store at table[*d_t].dd (null past the end)
+// point the density epilogue's d_a store and the dispersion epilogue's A2(S) store at
+// table[*d_t].dd, table[*d_t].q2 (null past the end)
 void launch_adj_tape(cudaStream_t st, SimDev* d_sims, const int* d_t, const AdjTapeEntry* table, int nt, int copy,
-                     int stokes, int nonlinear, long long N);
+                     int stokes, long long N);
 // point the tape views of the work fields at table[t] (no step counter change)
 void launch_adj_views(cudaStream_t st, SimDev* d_sims, const AdjTapeEntry* table, int t);
 void launch_adj_eos(cudaStream_t st, const SimDev* d_sims, long long N, const AdjStepArgs& a, int* d_rev);

@@ -191,6 +191,7 @@ struct SimDev {
     float2* spec[4];
     float* adj[kAdjFields];     // adjoint work fields (kw_adjoint.cpp), unused by a forward run
     float* tape_dd[kMaxComp];   // adjoint recompute: the density epilogue also stores d_a here (else null)
+    float* tape_q2;             // adjoint recompute: the dispersion epilogue also stores A2(S) here (else null)
     double* adj_gc;             // adjoint: dL/dc accumulated in FP64
     int* adj_rev;               // adjoint: the reverse step counter
     float adj_y;                // adjoint: absorption power y

@@ -104,6 +104,7 @@ private:
         int coupled = 0;
         int gate = GATE_NONE;
         int comp_mask = 7;        // which components take part (per-comp jobs)
+        int fanin = 0;            // the operator pass sums the nin inputs into output 0 (register column kernel)
         const char* name = "job";
     };
     struct ProfRec {

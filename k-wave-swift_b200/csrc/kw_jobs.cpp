@@ -166,6 +166,7 @@ void Engine::issue_job(const SpecJob& job, int sim_only) {
             cj.spec_out = job.spec_out;
             cj.nout = job.nout;
             cj.fanout = job.fanout;
+            cj.fanin = mode == COL_FWD_OP_INV ? job.fanin : 0;
             for (int c = 0; c < kMaxComp; ++c) cj.op[c] = job.op[c];
             cj.gate = job.gate;
             cj.tile_elems = te;
@@ -174,6 +175,8 @@ void Engine::issue_job(const SpecJob& job, int sim_only) {
             const double bytes = sum_sims(in_class, bytes_of);
             const long long tiles = sc ? (op ? 4 : 2) : (op ? 5 : 3);
             const size_t smem = (size_t)(tiles * te * sizeof(float2));
+            if (op && job.fanin && !(sc && has_colop(sc)))
+                throw KwError{KW_ERR_UNSUPPORTED, "fan-in spectral job needs the register column kernel"};
             if (sc && op && has_colop(sc))
                 timed(std::string(label) + job.name, bytes, [&] { launch_colop(st(), d_sims_, d_t_, m.d, m.n, cj, sc); });
             else if (sc && !op && has_colp(sc))
@@ -194,6 +197,7 @@ void Engine::issue_job(const SpecJob& job, int sim_only) {
                        const int no = open_comps(h, job.fanout ? 1 : job.nout);
                        if (no == 0) return 0.0;
                        const double tables = job.op[0].radial != RT_NONE ? (double)h.A * h.B * h.Ch * 4 : 0.0;
+                       if (job.fanin) return spec_bytes(h) * (job.fanin + 1) + tables * job.fanin;
                        return job.fanout ? spec_bytes(h) * (1 + job.nout) + tables : no * (2 * spec_bytes(h) + tables);
                    });
         spec_final = job.spec_out;

@@ -33,6 +33,7 @@ struct ColJob {
     int spec_out;
     int nout;              // outputs written by one CTA (fan-out) or 1
     int fanout;
+    int fanin;             // > 0: the operator pass sums op[c] X_c over this many inputs into one output
     OpSpec op[kMaxComp];
     int gate;
     long long tile_elems;

@@ -162,6 +162,7 @@ __device__ __forceinline__ void epi_point(const SimDev& S, const RowC2RJob& job,
             const float rs = av(AX_F0);
             float term = (S.tau.ptr ? av(AX_TAU) : S.tau.s) * d[0];
             if (S.absorb == 3) term = term - (S.eta.ptr ? av(AX_ETA) : S.eta.s) * d[1];
+            if (S.absorb == 3 && S.tape_q2) S.tape_q2[i] = d[1];   // the adjoint's recompute keeps A2(S)
             float e = rs + term;
             if (S.nonlinear) e = e + (S.bona.ptr ? av(AX_BONA) : S.bona.s) * (rs * rs) / (2.f * rho0_at());
             S.p[i] = c2_at() * e;

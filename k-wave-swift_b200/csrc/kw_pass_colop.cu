@@ -36,6 +36,51 @@ __global__ void __launch_bounds__(256) k_colop(const SimDev* __restrict__ sims, 
     const bool col_ok = c < inner;
     const long long base = col_ok ? c : 0;
     const float2* __restrict__ twn = axisA ? S.plan_a.twn : S.plan_b.twn;
+    auto op_of = [&](int oc) { return oc == 0 ? job.op[0] : (oc == 1 ? job.op[1] : job.op[2]); };
+    auto factor_vec = [&](const OpSpec& op) -> const float2* {
+        if (op.axis_op == AO_NONE) return nullptr;
+        const AxisDev& ax = S.ax[op.axis];
+        return op.axis_op == AO_DPOS ? ax.dpos : (op.axis_op == AO_DNEG ? ax.dneg : ax.colloc);
+    };
+    const int pass_ref_axis = (axisA ? 0 : 1) - (3 - S.dim);
+
+    if (job.fanin > 0) {
+        // fan-in: sum_c H_c X_c with one inverse transform (the adjoint's lambda_p = sum_a D-_a w_a)
+        int kb = 0, kc = c;
+        if (axisA) { kb = c / S.Cp; kc = c - kb * S.Cp; }
+        const bool bin_ok = col_ok && kc < S.Ch;
+        float2 acc[R1];
+#pragma unroll
+        for (int m = 0; m < R1; ++m) acc[m] = make_float2(0.f, 0.f);
+        for (int ci = 0; ci < job.fanin; ++ci) {
+            const float2* inc = S.spec[job.spec_in + ci] + base;
+            float2 v[R1];
+#pragma unroll
+            for (int r = 0; r < R1; ++r) v[r] = col_ok ? inc[(long long)(t + T * r) * inner] : make_float2(0.f, 0.f);
+            FftReg<N, P, false, Lay>::run(v, sh, t, l, twn);
+            const OpSpec op = op_of(ci);
+            const float2* fv = factor_vec(op);
+            const bool alg = fv && op.axis == pass_ref_axis;
+            float2 fc = make_float2(S.inv_n, 0.f);
+            if (fv && !alg && bin_ok) fc = cscale(__ldg(fv + axis_index(S, op.axis, 0, kb, kc)), S.inv_n);
+            const float* tab = op.radial != RT_NONE ? S.radial[op.radial] + base : nullptr;
+#pragma unroll
+            for (int m = 0; m < R1; ++m) {
+                if (!bin_ok) continue;
+                float2 f = alg ? cscale(__ldg(fv + t + T * m), S.inv_n) : fc;
+                if (tab) f = cscale(f, __ldg(tab + (long long)(t + T * m) * inner));
+                acc[m] = cadd(acc[m], cmul(v[m], f));
+            }
+        }
+        FftReg<N, P, true, Lay>::run(acc, sh, t, l, twn);
+        float2* out = S.spec[job.spec_out] + base;
+        if (bin_ok) {
+#pragma unroll
+            for (int m = 0; m < R1; ++m) out[(long long)(t + T * m) * inner] = acc[m];
+        }
+        return;
+    }
+
     const int comp_in = job.fanout ? 0 : bw.comp;
     const float2* in = S.spec[job.spec_in + comp_in] + base;
 
@@ -47,15 +92,8 @@ __global__ void __launch_bounds__(256) k_colop(const SimDev* __restrict__ sims, 
     int kb = 0, kc = c;
     if (axisA) { kb = c / S.Cp; kc = c - kb * S.Cp; }
     const bool bin_ok = col_ok && kc < S.Ch;
-    const int pass_ref_axis = (axisA ? 0 : 1) - (3 - S.dim);
     const int nouts = job.fanout ? job.nout : 1;
-    auto op_of = [&](int oc) { return oc == 0 ? job.op[0] : (oc == 1 ? job.op[1] : job.op[2]); };
     auto out_comp = [&](int oo) { return job.fanout ? oo : bw.comp; };
-    auto factor_vec = [&](const OpSpec& op) -> const float2* {
-        if (op.axis_op == AO_NONE) return nullptr;
-        const AxisDev& ax = S.ax[op.axis];
-        return op.axis_op == AO_DPOS ? ax.dpos : (op.axis_op == AO_DNEG ? ax.dneg : ax.colloc);
-    };
     auto along = [&](const OpSpec& op) { return op.axis_op != AO_NONE && op.axis == pass_ref_axis; };
     const int rad = op_of(job.fanout ? 0 : bw.comp).radial;
     // X * radial / N: the factor common to every output (padding bins are never stored: they stay zero)

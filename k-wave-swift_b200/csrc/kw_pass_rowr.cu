@@ -336,7 +336,7 @@ __global__ void __launch_bounds__(256) k_rowr_c2r(const SimDev* __restrict__ sim
                 const float2 pmr = row_pair(S.ax[D - 1].pml, n);
                 const float2 a1 = dpair(0, m);
                 float2 a2 = make_float2(0.f, 0.f), q2 = a2;
-                if (S.absorb == 3) { a2 = dpair(1, m); q2 = dpair(2, m); }
+                if (S.absorb == 3) { a2 = dpair(1, m); q2 = ld_state(S.adj[ADJ_Q2], e); }
                 double2 gcv = *reinterpret_cast<const double2*>(S.adj_gc + e);
                 float2 lro[kMaxComp], wo[kMaxComp], sg2;
 #pragma unroll
@@ -411,6 +411,7 @@ __global__ void __launch_bounds__(256) k_rowr_c2r(const SimDev* __restrict__ sim
                     half(p2, h) = half(c2[b], h) * ee;
                 }
                 st_state(S.p, rbase + 2 * (t + T * m), p2);
+                if (S.absorb == 3 && S.tape_q2) st_state(S.tape_q2, rbase + 2 * (t + T * m), d1);   // the adjoint's recompute keeps A2(S)
             }
         }
     }

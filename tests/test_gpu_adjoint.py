@@ -61,6 +61,20 @@ def test_fused_reverse_eos_matches_fp64_adjoint(shape, kw, monkeypatch):
         assert rel_l2(r["grad_p0"], gp) < 2e-3, rel_l2(r["grad_p0"], gp)
 
 
+@pytest.mark.parametrize("shape,kw", [((48, 64), dict(absorb="powerlaw", nonlinear=True, nt=40)),
+                                      ((16, 20, 32), dict(absorb="stokes", nonlinear=True, nt=30))])
+def test_fan_in_sum_matches_per_component_sum(shape, kw, monkeypatch):
+    # lambda_p = sum_a D-_a w_a: one inverse of the summed spectra against one inverse per component
+    c, p0, data, kw = problem(shape, **kw)
+    monkeypatch.setenv("KW_ADJOINT_FANIN", "1")
+    r1 = gpu_adjoint(shape, c, p0, data, kw)
+    monkeypatch.setenv("KW_ADJOINT_FANIN", "0")
+    r0 = gpu_adjoint(shape, c, p0, data, kw)
+    assert rel_l2(r1["grad_c0"], r0["grad_c0"]) < 1e-4, rel_l2(r1["grad_c0"], r0["grad_c0"])
+    if p0 is not None:
+        assert rel_l2(r1["grad_p0"], r0["grad_p0"]) < 1e-4
+
+
 def test_checkpoint_policies_agree():
     shape = (40, 36)
     c, p0, data, kw = problem(shape, absorb="powerlaw", nonlinear=True, nt=45)
