@@ -5,6 +5,7 @@
 #include "kw_engine.h"
 
 #include <algorithm>
+#include <cstdlib>
 #include <set>
 
 namespace kw {
@@ -16,6 +17,14 @@ static int row_class(const SimHost& h) {
 // register-resident row kernels (kw_pass_rowr.cu) serve the even rows of two-stage half length;
 // the 1D forward row pass, which also applies the operator, keeps the staged kernel
 static bool rowr_class(int sclass) { return sclass != 0 && has_reg_row(sclass); }
+// which register column kernels run: bit 0 the operator pass on the double-buffered kernel (else
+// one tile per CTA), bit 1 the in-place passes up to 256 points on it too (else TMA-fed), bit 2
+// the in-place passes above 256 points on the staged kernels (else double-buffered); KW_COLA
+// overrides
+static int cola_policy() {
+    if (const char* e = std::getenv("KW_COLA")) return std::atoi(e);
+    return 0;
+}
 static int col_class(const SimHost& h, int axis) {
     const int n = axis == 0 ? h.A : h.B;
     return has_fixed_kernel(n) ? n : 0;
@@ -62,7 +71,8 @@ const Engine::Map& Engine::map_cols(int axis, int ncomp, int sim_only, bool op, 
         const int inner = axis == 0 ? h.B * h.Cp : h.Cp;
         const int outer = axis == 0 ? 1 : h.A;
         int tiles;
-        if (sclass && (op ? has_colop(sclass) : has_colp(sclass))) {   // register-plan kernels: columns of one plane
+        const bool reg = op ? has_colop(sclass) : (has_colp(sclass) || (has_colop(sclass) && !(cola_policy() & 4)));
+        if (sclass && reg) {   // register-plan kernels: columns of one plane
             const int tw = op ? colop_lines(n) : colr_lines(n);
             tiles = outer * ((inner + tw - 1) / tw);
         } else {
@@ -177,11 +187,18 @@ void Engine::issue_job(const SpecJob& job, int sim_only) {
             const size_t smem = (size_t)(tiles * te * sizeof(float2));
             if (op && job.fanin && !(sc && has_colop(sc)))
                 throw KwError{KW_ERR_UNSUPPORTED, "fan-in spectral job needs the register column kernel"};
-            if (sc && op && has_colop(sc))
+            // register column kernels: the operator pass double-buffered (cola) or one tile per CTA
+            // (colop); the in-place passes TMA-fed up to 256 points (colp), double-buffered above
+            const int cola = cola_policy();
+            if (sc && op && has_colop(sc) && (cola & 1))
+                timed(std::string(label) + job.name, bytes, [&] { launch_cola(st(), d_sims_, d_t_, m.d, m.n, cj, sc); });
+            else if (sc && op && has_colop(sc))
                 timed(std::string(label) + job.name, bytes, [&] { launch_colop(st(), d_sims_, d_t_, m.d, m.n, cj, sc); });
-            else if (sc && !op && has_colp(sc))
+            else if (sc && !op && has_colp(sc) && !(cola & 2))
                 timed(std::string(label) + job.name, bytes,
                       [&] { launch_colp(st(), d_sims_, d_t_, m.d, m.n, cj, sc, d_flag_ + 1); });
+            else if (sc && !op && has_colop(sc) && !(cola & 4))
+                timed(std::string(label) + job.name, bytes, [&] { launch_cola(st(), d_sims_, d_t_, m.d, m.n, cj, sc); });
             else
                 timed(std::string(label) + job.name, bytes, [&] { launch_col(st(), d_sims_, d_t_, m.d, m.n, cj, smem, sc); });
         }

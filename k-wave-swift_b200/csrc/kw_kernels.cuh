@@ -68,6 +68,13 @@ void launch_row_c2r(cudaStream_t st, const SimDev* d_sims, const int* d_t, const
 void init_colop_attributes(int optin);
 void launch_colop(cudaStream_t st, const SimDev* d_sims, const int* d_t, const BlockWork* map, int nmap,
                   const ColJob& job, int n);
+// persistent, cp.async double-buffered register column passes for has_colop(n) lengths: in-place
+// forward / inverse, operator (with fan-out) and fan-in operator modes; same tiles as launch_colop
+// (colop_lines(n) consecutive columns of one plane)
+enum ColaMode { CA_FWD = 0, CA_INV, CA_OP, CA_FANIN };
+void init_cola_attributes(int optin);
+void launch_cola(cudaStream_t st, const SimDev* d_sims, const int* d_t, const BlockWork* map, int nmap,
+                 const ColJob& job, int n);
 // TMA-fed warp-specialised in-place column pass for has_colp(n) lengths (persistent grid);
 // tiles are colr_lines(n) columns of one plane; `err` receives a KernelError code if a wait times out
 void init_colp_attributes();

@@ -8,7 +8,8 @@
 // one inverse and take the factor on the way out; an output whose factor varies along the line
 // gets its own inverse. With several outputs the product is parked in shared memory (each thread
 // its own slots) so that only one line's worth of registers is live. Many small CTAs per SM keep
-// enough loads in flight.
+// enough loads in flight. The fan-in variant sums H_c X_c over several inputs into one output
+// with one inverse.
 #include "kw_fft_reg.cuh"
 #include "kw_pass_common.cuh"
 
@@ -36,53 +37,18 @@ __global__ void __launch_bounds__(256) k_colop(const SimDev* __restrict__ sims, 
     const bool col_ok = c < inner;
     const long long base = col_ok ? c : 0;
     const float2* __restrict__ twn = axisA ? S.plan_a.twn : S.plan_b.twn;
-    auto op_of = [&](int oc) { return oc == 0 ? job.op[0] : (oc == 1 ? job.op[1] : job.op[2]); };
-    auto factor_vec = [&](const OpSpec& op) -> const float2* {
-        if (op.axis_op == AO_NONE) return nullptr;
-        const AxisDev& ax = S.ax[op.axis];
-        return op.axis_op == AO_DPOS ? ax.dpos : (op.axis_op == AO_DNEG ? ax.dneg : ax.colloc);
-    };
-    const int pass_ref_axis = (axisA ? 0 : 1) - (3 - S.dim);
-
-    if (job.fanin > 0) {
-        // fan-in: sum_c H_c X_c with one inverse transform (the adjoint's lambda_p = sum_a D-_a w_a)
-        int kb = 0, kc = c;
-        if (axisA) { kb = c / S.Cp; kc = c - kb * S.Cp; }
-        const bool bin_ok = col_ok && kc < S.Ch;
-        float2 acc[R1];
-#pragma unroll
-        for (int m = 0; m < R1; ++m) acc[m] = make_float2(0.f, 0.f);
-        for (int ci = 0; ci < job.fanin; ++ci) {
-            const float2* inc = S.spec[job.spec_in + ci] + base;
-            float2 v[R1];
-#pragma unroll
-            for (int r = 0; r < R1; ++r) v[r] = col_ok ? inc[(long long)(t + T * r) * inner] : make_float2(0.f, 0.f);
-            FftReg<N, P, false, Lay>::run(v, sh, t, l, twn);
-            const OpSpec op = op_of(ci);
-            const float2* fv = factor_vec(op);
-            const bool alg = fv && op.axis == pass_ref_axis;
-            float2 fc = make_float2(S.inv_n, 0.f);
-            if (fv && !alg && bin_ok) fc = cscale(__ldg(fv + axis_index(S, op.axis, 0, kb, kc)), S.inv_n);
-            const float* tab = op.radial != RT_NONE ? S.radial[op.radial] + base : nullptr;
-#pragma unroll
-            for (int m = 0; m < R1; ++m) {
-                if (!bin_ok) continue;
-                float2 f = alg ? cscale(__ldg(fv + t + T * m), S.inv_n) : fc;
-                if (tab) f = cscale(f, __ldg(tab + (long long)(t + T * m) * inner));
-                acc[m] = cadd(acc[m], cmul(v[m], f));
-            }
-        }
-        FftReg<N, P, true, Lay>::run(acc, sh, t, l, twn);
-        float2* out = S.spec[job.spec_out] + base;
-        if (bin_ok) {
-#pragma unroll
-            for (int m = 0; m < R1; ++m) out[(long long)(t + T * m) * inner] = acc[m];
-        }
-        return;
-    }
-
     const int comp_in = job.fanout ? 0 : bw.comp;
     const float2* in = S.spec[job.spec_in + comp_in] + base;
+    // the radial table of this thread's bins is copied into its own shared-memory slots while the
+    // spectrum loads and the forward transform run (behind the parked product, if any)
+    const int rad = (comp_in == 0 ? job.op[0] : (comp_in == 1 ? job.op[1] : job.op[2])).radial;
+    float* tsl = reinterpret_cast<float*>(parked + (job.fanout && job.nout > 1 ? R1 * 256 : 0)) + threadIdx.x;
+    if (rad != RT_NONE && col_ok) {
+        const float* tab = S.radial[rad] + base;
+#pragma unroll
+        for (int r = 0; r < R1; ++r) cp_async4(tsl + r * 256, tab + (long long)(t + T * r) * inner);
+    }
+    cp_commit();
 
     float2 v[R1];
 #pragma unroll
@@ -92,17 +58,23 @@ __global__ void __launch_bounds__(256) k_colop(const SimDev* __restrict__ sims, 
     int kb = 0, kc = c;
     if (axisA) { kb = c / S.Cp; kc = c - kb * S.Cp; }
     const bool bin_ok = col_ok && kc < S.Ch;
+    const int pass_ref_axis = (axisA ? 0 : 1) - (3 - S.dim);
     const int nouts = job.fanout ? job.nout : 1;
+    auto op_of = [&](int oc) { return oc == 0 ? job.op[0] : (oc == 1 ? job.op[1] : job.op[2]); };
     auto out_comp = [&](int oo) { return job.fanout ? oo : bw.comp; };
+    auto factor_vec = [&](const OpSpec& op) -> const float2* {
+        if (op.axis_op == AO_NONE) return nullptr;
+        const AxisDev& ax = S.ax[op.axis];
+        return op.axis_op == AO_DPOS ? ax.dpos : (op.axis_op == AO_DNEG ? ax.dneg : ax.colloc);
+    };
     auto along = [&](const OpSpec& op) { return op.axis_op != AO_NONE && op.axis == pass_ref_axis; };
-    const int rad = op_of(job.fanout ? 0 : bw.comp).radial;
     // X * radial / N: the factor common to every output (padding bins are never stored: they stay zero)
-    const float* tab = rad != RT_NONE ? S.radial[rad] + base : nullptr;
     const float inv_n = S.inv_n;
+    cp_wait<0>();
 #pragma unroll
     for (int m = 0; m < R1; ++m) {
         float f = inv_n;
-        if (tab && bin_ok) f *= __ldg(tab + (long long)(t + T * m) * inner);
+        if (rad != RT_NONE && bin_ok) f *= tsl[m * 256];
         v[m] = bin_ok ? cscale(v[m], f) : make_float2(0.f, 0.f);
     }
     // H_o = F_o(k_a) kappa / N. A factor F_o along another axis is constant along the line, so
@@ -152,13 +124,84 @@ __global__ void __launch_bounds__(256) k_colop(const SimDev* __restrict__ sims, 
     }
 }
 
+
+// fan-in operator pass: sum_c H_c X_c over job.fanin inputs with one inverse transform (the
+// adjoint's lambda_p = sum_a D-_a w_a); the running sum is kept in this thread's shared-memory slots
+template <int N>
+__global__ void __launch_bounds__(256, 2) k_colop_fanin(const SimDev* __restrict__ sims, const int* __restrict__ d_t,
+                                                        const BlockWork* __restrict__ map, int nmap, ColJob job) {
+    using P = RegPlan<N, reg_r1(N)>;
+    using Lay = ColLayout<P, N>;
+    constexpr int R1 = P::R1, T = P::T, TW = P::LINES;
+    __shared__ float2 sh[Lay::SLOTS];
+    extern __shared__ __align__(16) float2 parked[];   // [R1][256]
+    if (blockIdx.x >= nmap) return;
+    const BlockWork bw = map[blockIdx.x];
+    const SimDev& S = sims[bw.sim];
+    if (!gate_open(S, job.gate, bw.comp, *d_t)) return;
+    const bool axisA = job.layout_axis == 0;
+    const int inner = axisA ? S.B * S.Cp : S.Cp;
+    const int l = threadIdx.x % TW;
+    const int t = threadIdx.x / TW;
+    const int c = bw.tile * TW + l;
+    const bool col_ok = c < inner;
+    const long long base = col_ok ? c : 0;
+    const float2* __restrict__ twn = axisA ? S.plan_a.twn : S.plan_b.twn;
+    auto op_of = [&](int oc) { return oc == 0 ? job.op[0] : (oc == 1 ? job.op[1] : job.op[2]); };
+    auto factor_vec = [&](const OpSpec& op) -> const float2* {
+        if (op.axis_op == AO_NONE) return nullptr;
+        const AxisDev& ax = S.ax[op.axis];
+        return op.axis_op == AO_DPOS ? ax.dpos : (op.axis_op == AO_DNEG ? ax.dneg : ax.colloc);
+    };
+    const int pass_ref_axis = (axisA ? 0 : 1) - (3 - S.dim);
+    // fan-in: sum_c H_c X_c with one inverse transform (the adjoint's lambda_p = sum_a D-_a w_a);
+    // the running sum is kept in this thread's shared-memory slots
+    int kb = 0, kc = c;
+    if (axisA) { kb = c / S.Cp; kc = c - kb * S.Cp; }
+    const bool bin_ok = col_ok && kc < S.Ch;
+    float2 v[R1];
+#pragma unroll 1
+    for (int ci = 0; ci < job.fanin; ++ci) {
+        const float2* inc = S.spec[job.spec_in + ci] + base;
+#pragma unroll
+        for (int r = 0; r < R1; ++r) v[r] = col_ok ? inc[(long long)(t + T * r) * inner] : make_float2(0.f, 0.f);
+        FftReg<N, P, false, Lay>::run(v, sh, t, l, twn);
+        const OpSpec op = op_of(ci);
+        const float2* fv = factor_vec(op);
+        const bool alg = fv && op.axis == pass_ref_axis;
+        float2 fc = make_float2(S.inv_n, 0.f);
+        if (fv && !alg && bin_ok) fc = cscale(__ldg(fv + axis_index(S, op.axis, 0, kb, kc)), S.inv_n);
+        const float* tab = op.radial != RT_NONE ? S.radial[op.radial] + base : nullptr;
+#pragma unroll
+        for (int m = 0; m < R1; ++m) {
+            float2 f = alg ? cscale(__ldg(fv + t + T * m), S.inv_n) : fc;
+            if (tab && bin_ok) f = cscale(f, __ldg(tab + (long long)(t + T * m) * inner));
+            const float2 y = bin_ok ? cmul(v[m], f) : make_float2(0.f, 0.f);
+            parked[m * 256 + threadIdx.x] = ci == 0 ? y : cadd(parked[m * 256 + threadIdx.x], y);
+        }
+    }
+#pragma unroll
+    for (int m = 0; m < R1; ++m) v[m] = parked[m * 256 + threadIdx.x];
+    FftReg<N, P, true, Lay>::run(v, sh, t, l, twn);
+    float2* out = S.spec[job.spec_out] + base;
+    if (bin_ok) {
+#pragma unroll
+        for (int m = 0; m < R1; ++m) out[(long long)(t + T * m) * inner] = v[m];
+    }
+    return;
+}
+
+// dynamic shared memory: the parked product (several outputs, or the fan-in sum) and the radial
+// table slots
 template <int N>
 static size_t colop_park_bytes(const ColJob& job) {
-    return job.fanout && job.nout > 1 ? (size_t)reg_r1(N) * 256 * sizeof(float2) : 0;
+    const bool park = job.fanin || (job.fanout && job.nout > 1);
+    const bool table = !job.fanin && (job.op[0].radial != RT_NONE || job.op[1].radial != RT_NONE || job.op[2].radial != RT_NONE);
+    return (size_t)reg_r1(N) * 256 * ((park ? sizeof(float2) : 0) + (table ? sizeof(float) : 0));
 }
 
 void init_colop_attributes(int optin) {
-#define KW_SET(n) set_max_smem((const void*)k_colop<n>, optin);
+#define KW_SET(n) set_max_smem((const void*)k_colop<n>, optin); set_max_smem((const void*)k_colop_fanin<n>, optin);
     KW_COLOP_SIZES(KW_SET)
 #undef KW_SET
 }
@@ -167,8 +210,11 @@ void launch_colop(cudaStream_t st, const SimDev* d_sims, const int* d_t, const B
                   const ColJob& job, int n) {
     if (nmap <= 0) return;
     switch (n) {
-#define KW_CASE(n) \
-    case n: k_colop<n><<<nmap, 256, colop_park_bytes<n>(job), st>>>(d_sims, d_t, map, nmap, job); break;
+#define KW_CASE(n)                                                                                     \
+    case n:                                                                                            \
+        if (job.fanin) k_colop_fanin<n><<<nmap, 256, colop_park_bytes<n>(job), st>>>(d_sims, d_t, map, nmap, job); \
+        else k_colop<n><<<nmap, 256, colop_park_bytes<n>(job), st>>>(d_sims, d_t, map, nmap, job);                 \
+        break;
         KW_COLOP_SIZES(KW_CASE)
 #undef KW_CASE
         default: break;

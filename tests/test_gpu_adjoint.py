@@ -61,10 +61,13 @@ def test_fused_reverse_eos_matches_fp64_adjoint(shape, kw, monkeypatch):
         assert rel_l2(r["grad_p0"], gp) < 2e-3, rel_l2(r["grad_p0"], gp)
 
 
+@pytest.mark.parametrize("cola", ["0", "1"])
 @pytest.mark.parametrize("shape,kw", [((48, 64), dict(absorb="powerlaw", nonlinear=True, nt=40)),
                                       ((16, 20, 32), dict(absorb="stokes", nonlinear=True, nt=30))])
-def test_fan_in_sum_matches_per_component_sum(shape, kw, monkeypatch):
+def test_fan_in_sum_matches_per_component_sum(shape, kw, cola, monkeypatch):
     # lambda_p = sum_a D-_a w_a: one inverse of the summed spectra against one inverse per component
+    # (operator pass on the one-tile-per-CTA or the double-buffered column kernel)
+    monkeypatch.setenv("KW_COLA", cola)
     c, p0, data, kw = problem(shape, **kw)
     monkeypatch.setenv("KW_ADJOINT_FANIN", "1")
     r1 = gpu_adjoint(shape, c, p0, data, kw)

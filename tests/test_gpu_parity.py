@@ -172,6 +172,18 @@ def test_register_plan_lengths(shape):
     compare(run_gpu(b), ref)
 
 
+@pytest.mark.parametrize("cola", ["1", "3"])
+@pytest.mark.parametrize("shape", [(96, 192), (1024, 64), (48, 24, 96), (24, 192, 40), (16, 32, 32), (20, 384, 16),
+                                   (16, 512, 24)])
+def test_double_buffered_column_passes(shape, cola, monkeypatch):
+    # the double-buffered register column kernel for the operator pass (KW_COLA=1) and also for the
+    # in-place passes up to 256 points (KW_COLA=3); in 3D along B lengths above 256 take it anyway
+    monkeypatch.setenv("KW_COLA", cola)
+    b = _reg_case(shape, sum(shape) // 2, 6)
+    ref, _ = oracle.run(b)
+    compare(run_gpu(b), ref)
+
+
 def test_batch_equals_individual_runs():
     rng = np.random.default_rng(3)
     builders = []
