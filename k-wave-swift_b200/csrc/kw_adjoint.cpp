@@ -137,9 +137,17 @@ void Engine::adjoint(const kw_sim_desc& din, kw_adjoint_desc& a) {
         e.sprev = t == 0 ? zero_field : (slot > 0 ? tslot(slot - 1, 1) : ckf(t / K, 2 * D + 2));
     }
     const AdjTapeEntry* d_table = upload(table);
-    // copy p, S, div of the step just taken into the tape (the density and dispersion epilogues
-    // store d_a and A2(S) themselves) and aim those stores at the next step's slot
-    auto tape_now = [&](int copy) { launch_adj_tape(st(), d_sims_, d_t_, d_table, nt, copy, stokes, N); };
+    v.tape = d_table;
+    check(cudaMemcpyAsync(d_sims_, &v, sizeof(SimDev), cudaMemcpyHostToDevice, st()), "upload sim");
+    // Steps captured in tape mode store p, S, div, d_a and A2(S) of step t into table[t] from their
+    // epilogues; a restored checkpoint (and step 0, whose t = 0 override follows its epilogues) is
+    // copied into its slot instead.
+    auto tape_copy = [&]() { launch_adj_tape(st(), d_sims_, d_t_, d_table, stokes, N); };
+    auto set_tape_mode = [&](bool on) {
+        tape_mode_ = on;
+        if (graph_exec_) { cudaGraphExecDestroy(graph_exec_); graph_exec_ = nullptr; }
+        if (graph_) { cudaGraphDestroy(graph_); graph_ = nullptr; }
+    };
 
     cudaEvent_t e0, e1, e2;
     check(cudaEventCreate(&e0), "event");
@@ -147,9 +155,9 @@ void Engine::adjoint(const kw_sim_desc& din, kw_adjoint_desc& a) {
     check(cudaEventCreate(&e2), "event");
 
     // ---- 1. forward ----
+    set_tape_mode(store_all);
     reset();
     check(cudaEventRecord(e0, st()), "event");
-    if (store_all) tape_now(0);
     for (int t = 0; t < nt; ++t) {
         const bool ck_step = !store_all && t % K == 0;
         if (ck_step) {
@@ -158,7 +166,7 @@ void Engine::adjoint(const kw_sim_desc& din, kw_adjoint_desc& a) {
             else cpy(ckf(c, 2 * D + 2), v.rho_sum);
         }
         step(1);
-        if (store_all) tape_now(1);
+        if (store_all && t == 0) tape_copy();
         if (ck_step) {
             const int c = t / K;
             for (int b = 0; b < D; ++b) { cpy(ckf(c, b), v.u[b]); cpy(ckf(c, D + b), v.rho[b]); }
@@ -186,10 +194,10 @@ void Engine::adjoint(const kw_sim_desc& din, kw_adjoint_desc& a) {
     float* d_resid = upload(resid);
 
     // ---- 3. reverse sweep ----
-    // the recomputed segments do not sample the sensor: capture the forward step again without it
+    // the recomputed segments do not sample the sensor and fill the tape: capture the forward step
+    // again that way
     any_recp_ = false;
-    if (graph_exec_) { cudaGraphExecDestroy(graph_exec_); graph_exec_ = nullptr; }
-    if (graph_) { cudaGraphDestroy(graph_); graph_ = nullptr; }
+    set_tape_mode(true);
     for (int k = 0; k < ADJ_COUNT; ++k)
         if (!adj_is_view(k)) zero(v.adj[k]);
     check(cudaMemsetAsync(gc, 0, (size_t)N * sizeof(double), st()), "zero");
@@ -304,11 +312,8 @@ void Engine::adjoint(const kw_sim_desc& din, kw_adjoint_desc& a) {
             }
             launch_set_step(st(), d_t_, t0 + 1);
             t_ = t0 + 1;
-            tape_now(1);
-            for (int t = t0 + 1; t < t1; ++t) {
-                step(1);
-                tape_now(1);
-            }
+            tape_copy();
+            for (int t = t0 + 1; t < t1; ++t) step(1);
             for (int t = t1 - 1; t >= std::max(t0, t_stop); --t) reverse_step(t);
         }
     }
@@ -343,6 +348,9 @@ void Engine::adjoint(const kw_sim_desc& din, kw_adjoint_desc& a) {
     cudaEventDestroy(e2);
     for (auto& g : rgraph)
         if (g) cudaGraphExecDestroy(g);
+    set_tape_mode(false);
+    v.tape = nullptr;
+    check(cudaMemcpyAsync(d_sims_, &v, sizeof(SimDev), cudaMemcpyHostToDevice, st()), "upload sim");
 }
 
 }  // namespace kw

@@ -45,16 +45,12 @@ __device__ __forceinline__ void set_views(SimDev& S, const AdjTapeEntry& e) {
     S.adj[ADJ_Q2] = e.q2;
 }
 
-__global__ void k_adj_tape(SimDev* __restrict__ sims, const int* __restrict__ d_t, const AdjTapeEntry* __restrict__ table,
-                           int nt, int copy, int stokes) {
-    SimDev& S = sims[0];
+__global__ void k_adj_tape(const SimDev* __restrict__ sims, const int* __restrict__ d_t,
+                           const AdjTapeEntry* __restrict__ table, int stokes) {
+    const SimDev& S = sims[0];
     const int tn = *d_t;
     const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i == 0) {
-        for (int b = 0; b < kMaxComp; ++b) S.tape_dd[b] = tn < nt ? table[tn].dd[b] : nullptr;
-        S.tape_q2 = tn < nt ? table[tn].q2 : nullptr;
-    }
-    if (!copy || i >= S.N) return;
+    if (i >= S.N) return;
     const AdjTapeEntry e = table[tn - 1];
     e.p[i] = S.p[i];
     e.s[i] = S.rho_sum[i];
@@ -224,9 +220,8 @@ void launch_adj_begin(cudaStream_t st, SimDev* d_sims, int* d_t, const int* d_re
                       const float* resid, int npts) {
     k_adj_begin<<<blocks(npts > 0 ? npts : 1), 256, 0, st>>>(d_sims, d_t, d_rev, table, resid);
 }
-void launch_adj_tape(cudaStream_t st, SimDev* d_sims, const int* d_t, const AdjTapeEntry* table, int nt, int copy,
-                     int stokes, long long N) {
-    k_adj_tape<<<blocks(N), 256, 0, st>>>(d_sims, d_t, table, nt, copy, stokes);
+void launch_adj_tape(cudaStream_t st, SimDev* d_sims, const int* d_t, const AdjTapeEntry* table, int stokes, long long N) {
+    k_adj_tape<<<blocks(N), 256, 0, st>>>(d_sims, d_t, table, stokes);
 }
 void launch_adj_views(cudaStream_t st, SimDev* d_sims, const AdjTapeEntry* table, int t) {
     k_adj_views<<<1, 1, 0, st>>>(d_sims, table, t);

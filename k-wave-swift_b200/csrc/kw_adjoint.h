@@ -35,15 +35,6 @@ __host__ __device__ constexpr bool adj_is_view(int k) {
            k == ADJ_SPRP || k == ADJ_DIVP;
 }
 
-// where the reverse sweep finds the forward quantities of step t (one entry per step, device memory)
-struct AdjTapeEntry {
-    float* p;
-    float* s;
-    float* sprev;
-    float* div;
-    float* dd[kMaxComp];   // d_a(t) = D-_a u_a(t) (B/A)
-    float* q2;             // A2(S(t)) (power law with dispersion)
-};
 static_assert(ADJ_COUNT <= kAdjFields, "adjoint fields");
 
 // device pointers of one reverse step
@@ -67,11 +58,9 @@ void launch_set_step(cudaStream_t st, int* d_t, int t);
 // lambda_p += Sample^T r_t, and x1 = tau c^2 lambda_p, x2 = eta c^2 lambda_p at the same points.
 void launch_adj_begin(cudaStream_t st, SimDev* d_sims, int* d_t, const int* d_rev, const AdjTapeEntry* table,
                       const float* resid, int npts);
-// around forward steps: with `copy`, copy p, S, div of step t = *d_t - 1 into table[t]; then
-// point the density epilogue's d_a store and the dispersion epilogue's A2(S) store at
-// table[*d_t].dd, table[*d_t].q2 (null past the end)
-void launch_adj_tape(cudaStream_t st, SimDev* d_sims, const int* d_t, const AdjTapeEntry* table, int nt, int copy,
-                     int stokes, long long N);
+// copy p, S, div of the current state (step t = *d_t - 1) into table[t] (a restored checkpoint, or
+// step 0 whose t = 0 override follows its epilogues)
+void launch_adj_tape(cudaStream_t st, SimDev* d_sims, const int* d_t, const AdjTapeEntry* table, int stokes, long long N);
 // point the tape views of the work fields at table[t] (no step counter change)
 void launch_adj_views(cudaStream_t st, SimDev* d_sims, const AdjTapeEntry* table, int t);
 void launch_adj_eos(cudaStream_t st, const SimDev* d_sims, long long N, const AdjStepArgs& a, int* d_rev);

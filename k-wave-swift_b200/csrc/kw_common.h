@@ -164,6 +164,17 @@ struct SensorDev {
 __host__ __device__ constexpr int tmap_spec(int s, int layout_axis) { return 2 * s + layout_axis; }
 constexpr int kNumTmaps = 8;
 
+// Where the adjoint's reverse sweep finds the forward quantities of step t (one entry per step,
+// device memory; kw_adjoint.cpp). Recomputed steps write it from their epilogues.
+struct AdjTapeEntry {
+    float* p;
+    float* s;              // S(t) = sum_a rho_a
+    float* sprev;          // S(t-1)
+    float* div;            // Stokes div term
+    float* dd[kMaxComp];   // d_a(t) = D-_a u_a(t) (B/A)
+    float* q2;             // A2(S(t)) (power law with dispersion)
+};
+
 struct SimDev {
     int dim;
     int A, B, C, Ch, Cp;
@@ -190,8 +201,7 @@ struct SimDev {
     float* tmp[kMaxComp];       // real scratch fields (collocated velocity etc.)
     float2* spec[4];
     float* adj[kAdjFields];     // adjoint work fields (kw_adjoint.cpp), unused by a forward run
-    float* tape_dd[kMaxComp];   // adjoint recompute: the density epilogue also stores d_a here (else null)
-    float* tape_q2;             // adjoint recompute: the dispersion epilogue also stores A2(S) here (else null)
+    const AdjTapeEntry* tape;   // adjoint recompute: the tape epilogues store into tape[t] (else null)
     double* adj_gc;             // adjoint: dL/dc accumulated in FP64
     int* adj_rev;               // adjoint: the reverse step counter
     float adj_y;                // adjoint: absorption power y

@@ -190,6 +190,7 @@ void Engine::issue_step(bool first) {
     den.spec_in = sp1;
     den.spec_out = sp1;
     den.epi = EPI_DEN;
+    den.tape = tape_mode_ ? 1 : 0;
     den.coupled = 1;
     den.name = "den";
     issue_job(den, -1);
@@ -206,6 +207,7 @@ void Engine::issue_step(bool first) {
         ps.spec_in = 0;
         ps.spec_out = 0;
         ps.epi = EPI_ADD_RHO;
+        ps.tape = tape_mode_ ? 1 : 0;
         ps.gate = GATE_PSRC;
         ps.name = "psrc";
         issue_job(ps, -1);
@@ -222,6 +224,7 @@ void Engine::issue_step(bool first) {
         ab.spec_in = 0;
         ab.spec_out = 0;
         ab.epi = EPI_EOS_ABS;
+        ab.tape = tape_mode_ ? 1 : 0;
         ab.coupled = 1;
         ab.gate = GATE_ABS;
         ab.name = "abs";

@@ -105,6 +105,7 @@ private:
         int gate = GATE_NONE;
         int comp_mask = 7;        // which components take part (per-comp jobs)
         int fanin = 0;            // the operator pass sums the nin inputs into output 0 (register column kernel)
+        int tape = 0;             // the epilogue also stores the adjoint tape of the step
         const char* name = "job";
     };
     struct ProfRec {
@@ -174,6 +175,7 @@ private:
     char* arena_ = nullptr;
     size_t arena_size_ = 0, arena_used_ = 0;
     bool finalized_ = false;
+    bool tape_mode_ = false;   // adjoint: steps are captured with the tape epilogues
     int finalized_t_ = -1;
     // finalised aggregate outputs per sim (device)
     struct Outs {

@@ -245,6 +245,7 @@ void Engine::issue_job(const SpecJob& job, int sim_only) {
         cj.out_field = job.out_field;
         cj.gate = job.gate;
         cj.generic = has_fixed_kernel(sc) ? 0 : 1;
+        cj.tape = job.tape;
         cj.tile_elems = te;
         const bool reg = rowr_class(sc);
         const Map& m = map_rows(reg ? -2 : ncta, job.coupled ? 1 : job.nout, sim_only, sc);

@@ -47,6 +47,7 @@ struct RowC2RJob {
     int gate;
     int generic;           // some simulation needs the runtime-plan (ping-pong) path
     long long tile_elems;
+    int tape;              // the density / source / absorption epilogues also fill the adjoint tape
 };
 
 // Host entry points (kw_passes.cu, kw_small.cu). The pass launchers take the tile map and its

@@ -89,7 +89,7 @@ __device__ __forceinline__ void c2r_stage_aux(const SimDev& S, const AuxPlan& a,
 // epilogue at one grid point; staged inputs come from `av(field)` (the value of that field here)
 template <class AV>
 __device__ __forceinline__ void epi_point(const SimDev& S, const RowC2RJob& job, int comp0, int ncomp, long long i,
-                                          int ca, int cb, int cc, const float* d, AV av) {
+                                          int ca, int cb, int cc, const float* d, AV av, const AdjTapeEntry* te) {
     auto coord = [&](int ax) { const int L = ax + 3 - S.dim; return L == 0 ? ca : (L == 1 ? cb : cc); };
     auto c2_at = [&]() { return S.c2.ptr ? av(AX_C2) : S.c2.s; };
     auto rho0_at = [&]() { return S.rho0.ptr ? av(AX_RHO0) : S.rho0.s; };
@@ -134,7 +134,7 @@ __device__ __forceinline__ void epi_point(const SimDev& S, const RowC2RJob& job,
                 const float mass = S.nonlinear ? dtr * d[a] * nl : dtr * d[a];
                 const float r = pm * (pm * av(AX_F0 + a) - mass);
                 S.rho[a][i] = r;
-                if (S.tape_dd[a]) S.tape_dd[a][i] = d[a];   // the adjoint's recompute keeps d_a
+                if (te && S.nonlinear) te->dd[a][i] = d[a];   // the adjoint's recompute keeps d_a
                 rs = a == 0 ? r : rs + r;
                 dv = a == 0 ? d[a] : dv + d[a];
             }
@@ -143,8 +143,13 @@ __device__ __forceinline__ void epi_point(const SimDev& S, const RowC2RJob& job,
             if (S.absorb >= 1) {
                 divterm = r0v * dv;
                 S.div_term[i] = divterm;
+                if (te && S.absorb == 1) te->div[i] = divterm;
             }
-            if (S.eos_pointwise) S.p[i] = eos(rs, divterm);
+            if (S.eos_pointwise) {
+                const float pv = eos(rs, divterm);
+                S.p[i] = pv;
+                if (te) { te->s[i] = rs; te->p[i] = pv; }
+            }
             break;
         }
         case EPI_ADD_RHO: {  // additive p source, k-space corrected (KSpaceFirstOrder.swift:167-172)
@@ -155,17 +160,25 @@ __device__ __forceinline__ void epi_point(const SimDev& S, const RowC2RJob& job,
                 rs = a == 0 ? r : rs + r;
             }
             S.rho_sum[i] = rs;
-            if (S.eos_pointwise) S.p[i] = eos(rs, S.absorb == 1 ? av(AX_ETA) : 0.f);
+            if (S.eos_pointwise) {
+                const float pv = eos(rs, S.absorb == 1 ? av(AX_ETA) : 0.f);
+                S.p[i] = pv;
+                if (te) { te->s[i] = rs; te->p[i] = pv; }
+            }
             break;
         }
         case EPI_EOS_ABS: {  // power-law absorption / dispersion (KSpaceFirstOrder.swift:836-845)
             const float rs = av(AX_F0);
             float term = (S.tau.ptr ? av(AX_TAU) : S.tau.s) * d[0];
             if (S.absorb == 3) term = term - (S.eta.ptr ? av(AX_ETA) : S.eta.s) * d[1];
-            if (S.absorb == 3 && S.tape_q2) S.tape_q2[i] = d[1];   // the adjoint's recompute keeps A2(S)
             float e = rs + term;
             if (S.nonlinear) e = e + (S.bona.ptr ? av(AX_BONA) : S.bona.s) * (rs * rs) / (2.f * rho0_at());
             S.p[i] = c2_at() * e;
+            if (te) {   // the adjoint's recompute keeps p, S and A2(S)
+                te->p[i] = c2_at() * e;
+                te->s[i] = rs;
+                if (S.absorb == 3) te->q2[i] = d[1];
+            }
             break;
         }
         default: break;
@@ -173,7 +186,7 @@ __device__ __forceinline__ void epi_point(const SimDev& S, const RowC2RJob& job,
 }
 
 template <int MT>
-__device__ __forceinline__ void c2r_compute(const SimDev& S, const BlockWork bw, const RowC2RJob& job, float2* buf,
+__device__ __forceinline__ void c2r_compute(const SimDev& S, const BlockWork bw, const RowC2RJob& job, const AdjTapeEntry* te, float2* buf,
                                             float2* tmp, const float* aux, const AuxPlan& a) {
     constexpr bool FIX = MT > 0;
     constexpr int LT = FIX ? c2r_lines(MT) : 1;
@@ -247,13 +260,13 @@ __device__ __forceinline__ void c2r_compute(const SimDev& S, const BlockWork bw,
             const long long i0 = (long long)row * C + 2 * m;
             const int e0 = l * C + 2 * m;
             epi_point(S, job, r.comp0, ncomp, i0, ca, cb, 2 * m, d0,
-                      [&](int f) { return aux[a.slot[f] * rowsz + e0]; });
+                      [&](int f) { return aux[a.slot[f] * rowsz + e0]; }, te);
             epi_point(S, job, r.comp0, ncomp, i0 + 1, ca, cb, 2 * m + 1, d1,
-                      [&](int f) { return aux[a.slot[f] * rowsz + e0 + 1]; });
+                      [&](int f) { return aux[a.slot[f] * rowsz + e0 + 1]; }, te);
         } else {
             const int e0 = l * C + m;
             epi_point(S, job, r.comp0, ncomp, (long long)row * C + m, ca, cb, m, d0,
-                      [&](int f) { return aux[a.slot[f] * rowsz + e0]; });
+                      [&](int f) { return aux[a.slot[f] * rowsz + e0]; }, te);
         }
     }
 }
@@ -285,7 +298,7 @@ __global__ void __launch_bounds__(256) k_row_c2r(const SimDev* __restrict__ sims
         cp_commit();
         cp_wait<2>();                                                // spectrum of tile k
         __syncthreads();
-        if (open) c2r_compute<MT>(S, bw, job, sm + (k & 1) * te, tmp, aux, a);
+        if (open) c2r_compute<MT>(S, bw, job, job.tape ? S.tape + t : nullptr, sm + (k & 1) * te, tmp, aux, a);
         __syncthreads();
     }
     cp_wait<0>();

@@ -72,7 +72,7 @@ __device__ __forceinline__ float2 ld_medium(const FieldOrScalar& f, long long e)
 }
 __device__ __forceinline__ float& half(float2& v, int h) { return h ? v.y : v.x; }
 
-template <int M, int EPI>
+template <int M, int EPI, bool TAPE = false>
 __global__ void __launch_bounds__(256) k_rowr_c2r(const SimDev* __restrict__ sims, const int* __restrict__ d_t,
                                                   const BlockWork* __restrict__ map, int nmap, RowC2RJob job) {
     using P = RegPlan<M, c2r_r1(M)>;
@@ -245,14 +245,22 @@ __global__ void __launch_bounds__(256) k_rowr_c2r(const SimDev* __restrict__ sim
 #pragma unroll
                 for (int a = 0; a < kMaxComp; ++a)
                     if (a < D) st_state(S.rho[a], e, rn[a]);
-                if (EPI == EPI_DEN && S.tape_dd[0]) {   // the adjoint's recompute keeps d_a = D-_a u_a
-#pragma unroll
-                    for (int a = 0; a < kMaxComp; ++a)
-                        if (a < D) st_state(S.tape_dd[a], e, dpair(a, m));
-                }
                 st_state(S.rho_sum, e, rs2);
                 if (EPI == EPI_DEN && S.absorb >= 1) st_state(S.div_term, e, dv2);
                 if (S.eos_pointwise) st_state(S.p, e, p2);
+                if constexpr (TAPE) {   // the adjoint's recompute: d_a = D-_a u_a, and S, p, div when they are final here
+                    const AdjTapeEntry& te = S.tape[*d_t];
+                    if (EPI == EPI_DEN && S.nonlinear) {
+#pragma unroll
+                        for (int a = 0; a < kMaxComp; ++a)
+                            if (a < D) st_state(te.dd[a], e, dpair(a, m));
+                    }
+                    if (S.eos_pointwise) {
+                        st_state(te.s, e, rs2);
+                        st_state(te.p, e, p2);
+                    }
+                    if (EPI == EPI_DEN && S.absorb == 1) st_state(te.div, e, dv2);
+                }
             }
         } else if constexpr (EPI == EPI_ADJ_VEL) {
             // adjoint of the velocity update (kw_adjoint.cu)
@@ -411,7 +419,13 @@ __global__ void __launch_bounds__(256) k_rowr_c2r(const SimDev* __restrict__ sim
                     half(p2, h) = half(c2[b], h) * ee;
                 }
                 st_state(S.p, rbase + 2 * (t + T * m), p2);
-                if (S.absorb == 3 && S.tape_q2) st_state(S.tape_q2, rbase + 2 * (t + T * m), d1);   // the adjoint's recompute keeps A2(S)
+                if constexpr (TAPE) {   // the adjoint's recompute keeps p, S and A2(S)
+                    const AdjTapeEntry& te = S.tape[*d_t];
+                    const long long e = rbase + 2 * (t + T * m);
+                    st_state(te.p, e, p2);
+                    st_state(te.s, e, rs[b]);
+                    if (S.absorb == 3) st_state(te.q2, e, d1);
+                }
             }
         }
     }
@@ -423,9 +437,9 @@ __global__ void __launch_bounds__(256) k_rowr_c2r(const SimDev* __restrict__ sim
 template <int M>
 static size_t rowr_park_bytes(int ncomp) { return (size_t)(ncomp > 1 ? ncomp - 1 : 0) * c2r_r1(M) * 256 * sizeof(float2); }
 
-template <int EPI>
+template <int EPI, bool TAPE = false>
 static void set_rowr_attrs(int optin) {
-#define KW_SET(m) set_max_smem((const void*)k_rowr_c2r<m, EPI>, optin);
+#define KW_SET(m) set_max_smem((const void*)k_rowr_c2r<m, EPI, TAPE>, optin);
     KW_REG_ROW_SIZES(KW_SET)
 #undef KW_SET
 }
@@ -433,6 +447,8 @@ static void set_rowr_attrs(int optin) {
 void init_rowr_attributes(int optin) {
     set_rowr_attrs<EPI_DEN>(optin);
     set_rowr_attrs<EPI_EOS_ABS>(optin);
+    set_rowr_attrs<EPI_DEN, true>(optin);
+    set_rowr_attrs<EPI_EOS_ABS, true>(optin);
     set_rowr_attrs<EPI_ADJ_SUM>(optin);
     set_rowr_attrs<EPI_ADJ_EOS>(optin);
 }
@@ -458,9 +474,18 @@ static void launch_c2r_m(cudaStream_t st, const SimDev* d_sims, const int* d_t, 
         case EPI_VEL: k_rowr_c2r<M, EPI_VEL><<<nmap, 256, smem, st>>>(d_sims, d_t, map, nmap, job); break;
         case EPI_VEL_INIT: k_rowr_c2r<M, EPI_VEL_INIT><<<nmap, 256, smem, st>>>(d_sims, d_t, map, nmap, job); break;
         case EPI_ADD_U: k_rowr_c2r<M, EPI_ADD_U><<<nmap, 256, smem, st>>>(d_sims, d_t, map, nmap, job); break;
-        case EPI_DEN: k_rowr_c2r<M, EPI_DEN><<<nmap, 256, smem, st>>>(d_sims, d_t, map, nmap, job); break;
-        case EPI_ADD_RHO: k_rowr_c2r<M, EPI_ADD_RHO><<<nmap, 256, smem, st>>>(d_sims, d_t, map, nmap, job); break;
-        case EPI_EOS_ABS: k_rowr_c2r<M, EPI_EOS_ABS><<<nmap, 256, smem, st>>>(d_sims, d_t, map, nmap, job); break;
+        case EPI_DEN:
+            if (job.tape) k_rowr_c2r<M, EPI_DEN, true><<<nmap, 256, smem, st>>>(d_sims, d_t, map, nmap, job);
+            else k_rowr_c2r<M, EPI_DEN><<<nmap, 256, smem, st>>>(d_sims, d_t, map, nmap, job);
+            break;
+        case EPI_ADD_RHO:
+            if (job.tape) k_rowr_c2r<M, EPI_ADD_RHO, true><<<nmap, 256, smem, st>>>(d_sims, d_t, map, nmap, job);
+            else k_rowr_c2r<M, EPI_ADD_RHO><<<nmap, 256, smem, st>>>(d_sims, d_t, map, nmap, job);
+            break;
+        case EPI_EOS_ABS:
+            if (job.tape) k_rowr_c2r<M, EPI_EOS_ABS, true><<<nmap, 256, smem, st>>>(d_sims, d_t, map, nmap, job);
+            else k_rowr_c2r<M, EPI_EOS_ABS><<<nmap, 256, smem, st>>>(d_sims, d_t, map, nmap, job);
+            break;
         case EPI_ADJ_VEL: k_rowr_c2r<M, EPI_ADJ_VEL><<<nmap, 256, smem, st>>>(d_sims, d_t, map, nmap, job); break;
         case EPI_ADJ_SUM: k_rowr_c2r<M, EPI_ADJ_SUM><<<nmap, 256, smem, st>>>(d_sims, d_t, map, nmap, job); break;
         case EPI_ADJ_EOS: k_rowr_c2r<M, EPI_ADJ_EOS><<<nmap, 256, smem, st>>>(d_sims, d_t, map, nmap, job); break;
