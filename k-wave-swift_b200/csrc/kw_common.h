@@ -19,6 +19,7 @@ namespace kw {
 constexpr int kMaxStages = 16;
 constexpr int kMaxComp = 3;
 constexpr int kAdjFields = 32;
+constexpr int kMaxDirAngles = 16;   // distinct 2D sensor directivity angles of one simulation
 
 // FFT plan of one complex transform length n (a Stockham sequence of radix stages).
 struct FFTPlanDev {
@@ -104,7 +105,8 @@ struct FieldOrScalar {
 };
 
 // Radial (|k|-only) operator tables over the half-spectrum [A][B][Cp], precomputed in FP64.
-enum RadialTable { RT_NONE = 0, RT_KAPPA, RT_SKAPPA, RT_NU1, RT_NU2, RT_WINDOW, RT_COUNT };
+// RT_DIR0 + j: the k-space weight of directivity angle j (Hermitian part; [A][B][Cp])
+enum RadialTable { RT_NONE = 0, RT_KAPPA, RT_SKAPPA, RT_NU1, RT_NU2, RT_WINDOW, RT_DIR0, RT_COUNT = RT_DIR0 + kMaxDirAngles };
 // Per-axis factor selector.
 enum AxisOp { AO_NONE = 0, AO_DPOS, AO_DNEG, AO_COLLOC };
 
@@ -156,6 +158,11 @@ struct SensorDev {
     float* u_series[kMaxComp];
     float* p_max; float* p_min; float* p_ss; float* p_ssc;   // running aggregates (Kahan)
     float* u_max[kMaxComp]; float* u_ss[kMaxComp]; float* u_ssc[kMaxComp];
+    // 2D directivity (binary sensors): p of row q is sampled from dir_field[dir_slot[q]], the
+    // pressure filtered by the k-space weight of the row's angle ([ndir][N])
+    int ndir;
+    float* dir_field;
+    const int* dir_slot;
 };
 
 // Tensor maps of one simulation (TMA descriptors, kw_tmaps.cpp): spectrum s viewed as tiles of

@@ -27,7 +27,9 @@ __device__ __forceinline__ float* field_ptr(const SimDev& S, int sel, int comp) 
         case FS_SRCBUF: return S.src_buf[comp];
         case FS_WORK: return comp == 0 ? S.div_term : S.rho_sum;   // power-law inputs
         case FS_TMP: return S.tmp[comp];
-        default: return S.adj[sel - FS_ADJ + comp];
+        default:
+            if (sel >= FS_DIR) return S.sensor.dir_field + (long long)(sel - FS_DIR + comp) * S.N;
+            return S.adj[sel - FS_ADJ + comp];
     }
 }
 
@@ -38,6 +40,7 @@ __device__ __forceinline__ bool gate_open(const SimDev& S, int gate, int comp, i
     if (gate == GATE_P0) return S.has_p0 != 0;
     if (gate == GATE_ABS) return comp == 0 ? S.absorb >= 2 : S.absorb == 3;
     if (gate == GATE_RECU) return S.sensor.kind != 0 && (S.sensor.record_u_series || S.sensor.record_u_agg);
+    if (gate >= GATE_DIR) return gate - GATE_DIR < S.sensor.ndir;
     return true;
 }
 

@@ -242,7 +242,23 @@ void Engine::issue_step(bool first) {
         issue_job(vi, -1);
     }
 
-    // sensor sampling (KSFO:523-540)
+    // sensor sampling (KSFO:523-540); 2D directivity first filters p once per angle
+    // (Directivity.swift:41-79)
+    if (any_recp_)
+        for (int j = 0; j < max_dir_; ++j) {
+            SpecJob dj;
+            dj.in_field = FS_P;
+            dj.nin = 1;
+            dj.nout = 1;
+            dj.op[0] = OpSpec{AO_NONE, 0, (int8_t)(RT_DIR0 + j), 0};
+            dj.spec_in = 0;
+            dj.spec_out = 0;
+            dj.epi = EPI_STORE;
+            dj.out_field = FS_DIR + j;
+            dj.gate = GATE_DIR + j;
+            dj.name = "dir";
+            issue_job(dj, -1);
+        }
     if (any_recp_) timed("sample_p", 0, [&] { launch_sample(st(), d_sims_, d_t_, count(), max_pts_, 0, 0); });
     if (any_recu_) {
         SpecJob co;
@@ -271,7 +287,7 @@ bool Engine::host_gate(const SimHost& h, int gate, int comp) const {
         case GATE_P0: return S.has_p0 != 0;
         case GATE_ABS: return comp == 0 ? S.absorb >= 2 : S.absorb == 3;
         case GATE_RECU: return S.sensor.kind != 0 && (S.sensor.record_u_series || S.sensor.record_u_agg);
-        default: return true;
+        default: return gate >= GATE_DIR ? gate - GATE_DIR < S.sensor.ndir : true;
     }
 }
 
@@ -436,8 +452,6 @@ void Engine::setup_sim(int s, const kw_sim_desc& d) {
         if (d.pml_size > h.n_ref[a]) throw err(KW_ERR_INVALID, "pmlSize larger than the grid");
     if (d.alpha_coeff.data && !grid_sized(d.alpha_coeff)) throw err(KW_ERR_INVALID, "alphaCoeff must be scalar or grid-shaped");
     if (d.b_on_a.data && !grid_sized(d.b_on_a)) throw err(KW_ERR_INVALID, "bOnA must be scalar or grid-shaped");
-    if (d.directivity_angle && h.dim == 2 && d.sensor_kind == KW_SENSOR_BINARY)
-        throw err(KW_ERR_UNSUPPORTED, "2D sensor directivity is not available in this build");
 
     SimDev& v = h.dev;
     std::memset(&v, 0, sizeof(v));
@@ -841,6 +855,49 @@ void Engine::setup_sim(int s, const kw_sim_desc& d) {
         }
         if (h.record_p) any_recp_ = true;
         max_pts_ = std::max(max_pts_, sn.npts);
+
+        // 2D directivity of binary sensors (Directivity.swift:41-79): per distinct angle th a
+        // k-space weight W (pressure pattern: sinc of k along the element, size 10 max(dx, dy) by
+        // default; gradient pattern: the normal component of k over |k|). The sampled value is
+        // Re F^-1(W F(p)), i.e. the C2R of (W(k) + W(-k)) / 2 times the half spectrum.
+        if (h.dim == 2 && d.sensor_kind == KW_SENSOR_BINARY && d.directivity_angle && sn.npts > 0 && h.record_p) {
+            std::vector<int> gidx = flat_nonzero(d.sensor_mask, N);
+            std::vector<double> rowAngle(gidx.size());
+            for (size_t r = 0; r < gidx.size(); ++r) rowAngle[r] = (double)d.directivity_angle[gidx[r]];
+            std::vector<double> uniq(rowAngle);
+            std::sort(uniq.begin(), uniq.end());
+            uniq.erase(std::unique(uniq.begin(), uniq.end()), uniq.end());
+            if ((int)uniq.size() > kMaxDirAngles)
+                throw err(KW_ERR_UNSUPPORTED, "more than " + std::to_string(kMaxDirAngles) + " distinct directivity angles");
+            const double elem = std::isnan(d.directivity_size) ? 10.0 * std::max(h.d_ref[0], h.d_ref[1]) : d.directivity_size;
+            const std::vector<double>& kx = kv[0];   // reference axis 0: layout axis B
+            const std::vector<double>& ky = kv[1];   // reference axis 1: layout axis C (rows)
+            auto weight = [&](double th, double x, double y) {
+                if (d.directivity_pattern == KW_DIRECTIVITY_PRESSURE) {
+                    const double u = (std::cos(th) * y - std::sin(th) * x) * (elem / 2.0);
+                    return u == 0.0 ? 1.0 : std::sin(M_PI * u) / (M_PI * u);
+                }
+                const double k = std::sqrt(x * x + y * y);
+                return k == 0.0 ? 0.0 : (std::sin(th) * y + std::cos(th) * x) / k;
+            };
+            for (size_t j = 0; j < uniq.size(); ++j) {
+                std::vector<float> tab((size_t)h.Ns, 0.f);
+                for (int ib = 0; ib < h.B; ++ib)
+                    for (int kc = 0; kc < h.Ch; ++kc) {
+                        const int mb = (h.B - ib) % h.B, mc = (h.C - kc) % h.C;
+                        const double w = 0.5 * (weight(uniq[j], kx[ib], ky[kc]) + weight(uniq[j], kx[mb], ky[mc]));
+                        tab[(size_t)ib * h.Cp + kc] = (float)w;
+                    }
+                v.radial[RT_DIR0 + j] = upload(tab);
+            }
+            std::vector<int> slot(gidx.size());
+            for (size_t r = 0; r < gidx.size(); ++r)
+                slot[r] = (int)(std::lower_bound(uniq.begin(), uniq.end(), rowAngle[r]) - uniq.begin());
+            sn.ndir = (int)uniq.size();
+            sn.dir_slot = upload(slot);
+            sn.dir_field = (float*)dalloc((size_t)sn.ndir * N * sizeof(float));
+            max_dir_ = std::max(max_dir_, sn.ndir);
+        }
     }
     if (v.absorb >= 2) any_abs_ = true;
     if (v.has_p0) any_p0_ = true;

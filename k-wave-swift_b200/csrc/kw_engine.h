@@ -162,7 +162,7 @@ private:
     unsigned int* d_red_ = nullptr;
     int t_ = 0;
     int dim_ = 0;
-    int max_psrc_ = 0, max_usrc_ = 0, max_pts_ = 0;
+    int max_psrc_ = 0, max_usrc_ = 0, max_pts_ = 0, max_dir_ = 0;
     bool any_p_direct_ = false, any_p_add_ = false, any_u_direct_ = false, any_u_add_ = false;
     bool any_abs_ = false, any_p0_ = false, any_recu_ = false, any_recp_ = false;
     int max_A_ = 1, max_B_ = 1, max_M_ = 1;

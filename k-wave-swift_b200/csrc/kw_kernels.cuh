@@ -11,9 +11,12 @@ enum FieldSel {
     FS_WORK,  // power-law absorption inputs: component 0 = rho0 div u, component 1 = rho_sum
     FS_ADJ    // adjoint work fields: FS_ADJ + k selects adj[k + component]
 };
+// FS_DIR + j: the directivity-filtered pressure of angle j + component (kw_common.h SensorDev)
+constexpr int FS_DIR = FS_ADJ + kAdjFields;
 
 // A launch may be gated on a source being active at the current step.
-enum Gate { GATE_NONE = 0, GATE_PSRC, GATE_USRC, GATE_P0, GATE_ABS, GATE_RECU };
+// GATE_DIR + j: open while the simulation has a directivity angle j.
+enum Gate { GATE_NONE = 0, GATE_PSRC, GATE_USRC, GATE_P0, GATE_ABS, GATE_RECU, GATE_DIR = 16 };
 
 enum ColMode { COL_FWD = 0, COL_INV, COL_FWD_OP_INV };
 

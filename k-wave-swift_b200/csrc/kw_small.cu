@@ -97,7 +97,7 @@ __global__ void k_sample(const SimDev* __restrict__ sims, const int* __restrict_
     if (which == 0 ? !(sn.record_p_series || sn.record_p_agg) : !(sn.record_u_series || sn.record_u_agg)) return;
     const int q = blockIdx.x * blockDim.x + threadIdx.x;
     if (q >= sn.npts) return;
-    const float* f = which == 0 ? S.p : S.tmp[comp];
+    const float* f = which == 0 ? (sn.ndir > 0 ? sn.dir_field + (long long)__ldg(sn.dir_slot + q) * S.N : S.p) : S.tmp[comp];
     float v;
     if (sn.kind == 1) {
         v = f[__ldg(sn.idx + q)];

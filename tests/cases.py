@@ -5,11 +5,12 @@ import os
 
 import numpy as np
 
-from kwave import (AbsorptionMode, DescBuilder, KWaveGrid, KWaveMedium, KWaveSensor, KWaveSource,
-                   RecordField, SimulationOptions, SourceMode)
+from kwave import (AbsorptionMode, DescBuilder, DirectivityPattern, KWaveGrid, KWaveMedium, KWaveSensor,
+                   KWaveSource, RecordField, SimulationOptions, SourceMode)
 
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
-GOLDEN_CASES = ["1d_source_hetero", "2d_ivp", "2d_hetero_abs_nl", "2d_stokes_nc", "3d_hetero_src"]
+GOLDEN_CASES = ["1d_source_hetero", "2d_ivp", "2d_hetero_abs_nl", "2d_stokes_nc", "3d_hetero_src",
+                "2d_directivity_pressure", "2d_directivity_gradient"]
 
 
 def load_golden(name: str):
@@ -49,6 +50,10 @@ def builder_from_case(case) -> DescBuilder:
                          ux=s.get("ux"), uy=s.get("uy"), uz=s.get("uz"),
                          uMode=SourceMode(int(s.get("u_mode", 1))))
     sensor = KWaveSensor(mask=case.get("sensor_mask"), record=RecordField(int(case["record"])))
+    if "directivity_angle" in case:
+        sensor.directivityAngle = case["directivity_angle"]
+        sensor.directivitySize = float(case["directivity_size"])
+        sensor.directivityPattern = DirectivityPattern(int(case["directivity_pattern"]))
     options = SimulationOptions(pmlSize=int(case["pml_size"]), pmlAlpha=float(case.get("pml_alpha", 2.0)),
                                 smoothP0=bool(case.get("smooth_p0", True)),
                                 smoothC0=bool(case.get("smooth_c0", False)),

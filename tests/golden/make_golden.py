@@ -239,6 +239,32 @@ def simulate(case):
         else:
             idx = np.flatnonzero(sens.reshape(-1) != 0)
             sampler = lambda f: f.reshape(-1)[idx]  # noqa: E731
+    # 2D directivity of a binary sensor (Directivity.swift:41-79): per distinct angle th, the
+    # pressure filtered by W(k) in k-space (real part of the inverse), sampled at the rows of th
+    psampler = sampler
+    ang = case.get("directivity_angle")
+    if ang is not None and dim == 2 and sampler is not None and not (sens.ndim == 2 and sens.shape[0] == dim):
+        row_ang = np.asarray(ang, dtype=np.float32).astype(float).reshape(-1)[idx]
+        size = case.get("directivity_size")
+        size = 10 * max(spacing[0], spacing[1]) if size is None or np.isnan(size) else float(size)
+        kx, ky = kgrids[0], kgrids[1]
+        filters = []
+        for th in sorted(set(row_ang.tolist())):
+            if int(case.get("directivity_pattern", 0)) == 0:
+                x = (math.cos(th) * ky - math.sin(th) * kx) * (size / 2)
+                with np.errstate(invalid="ignore", divide="ignore"):
+                    w = np.where(x == 0, 1.0, np.sin(math.pi * x) / (math.pi * x))
+            else:
+                with np.errstate(invalid="ignore", divide="ignore"):
+                    w = np.where(kmag == 0, 0.0, (math.sin(th) * ky + math.cos(th) * kx) / kmag)
+            filters.append((w, np.flatnonzero(row_ang == th)))
+
+        def psampler(f):
+            out = np.zeros(len(idx))
+            Pk = F(f)
+            for w, rows in filters:
+                out[rows] = np.real(IF(Pk * w)).reshape(-1)[idx[rows]]
+            return out
     p = np.zeros(shape)
     u = [np.zeros(shape) for _ in range(dim)]
     rho = [np.zeros(shape) for _ in range(dim)]
@@ -278,7 +304,7 @@ def simulate(case):
             u = [(dtor[a] / 2) * np.real(IF(ddp[a] * kappa * P0)) for a in range(dim)]
         if sampler is not None:
             if rp:
-                prec.append(sampler(p))
+                prec.append(psampler(p))
             if ru:
                 for a in range(dim):
                     urec[a].append(sampler(np.real(IF(col[a] * F(u[a])))))
@@ -387,11 +413,34 @@ def cases():
         source=dict(p0=makeBall(nx, ny, nz, radius=2), p_mask=pmk,
                     p=(toneBurst(1 / dt, 2e6, 2) * 1e3).astype(np.float32), p_mode=ADDITIVE),
         sensor_mask=sm, record=R["p"] | R["pMax"] | R["uz"] | R["uFinal"])
+    # 2D sensor directivity (ParityDirectivityTests.swift:20-81 shape): point source, a line of
+    # binary sensor points whose angles take three values, both patterns
+    n = 48
+    dx = 1e-4
+    dt = 0.3 * dx / 1500.0
+    pm = np.zeros((n, n), np.float32)
+    pm[14, 24] = 1
+    line = np.zeros((n, n), np.float32)
+    line[32, 8:40] = 1
+    angles = np.zeros((n, n), np.float32)
+    angles[32, 8:40] = np.float32(math.pi / 2)
+    angles[32, 8:19] = np.float32(math.pi / 4)
+    angles[32, 29:40] = np.float32(3 * math.pi / 4)
+    for name, pat in (("2d_directivity_pressure", 0), ("2d_directivity_gradient", 1)):
+        cs[name] = dict(
+            dim=2, shape=[n, n], spacing=[dx, dx], dt=dt, nt=70, pml_size=8, c0=np.float32(1500),
+            rho0=np.float32(1000),
+            source=dict(p_mask=pm, p=(toneBurst(1 / dt, 2e6, 2) * 1.0).astype(np.float32), p_mode=ADDITIVE),
+            sensor_mask=line, directivity_angle=angles, directivity_size=6e-4, directivity_pattern=pat,
+            record=R["p"] | R["pMax"])
     return cs
 
 
 def main():
+    only = set(sys.argv[1:])   # optional: regenerate only the named cases
     for name, case in cases().items():
+        if only and name not in only:
+            continue
         out = simulate(case)
         flat = {}
         for k, v in case.items():
