@@ -147,6 +147,7 @@ private:
     const Map& map_rows(int lines_per_row, int ncomp, int sim_only, int sclass);
     const Map& map_cols(int axis, int ncomp, int sim_only, bool op, int sclass);
     const Map& map_elems(int sim_only);
+    const Map& map_planes(int ncomp, int sim_only);
     void issue_job(const SpecJob& job, int sim_only);
     void issue_step(bool first);
     void capture_graph();

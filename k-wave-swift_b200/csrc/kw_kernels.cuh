@@ -87,6 +87,13 @@ void launch_colp(cudaStream_t st, const SimDev* d_sims, const int* d_t, const Bl
 // register-resident row passes for even rows with has_reg_row(M) half lengths; one CTA per map
 // entry, whose tile indexes r2c_rows(M) / c2r_rows(M) consecutive rows
 void init_rowr_attributes(int optin);
+// 3D plane pass on a thread-block cluster (kw_pass_plane.cu): R2C along C and the forward FFT along
+// B of whole A-planes, map entries (sim, comp, plane a); plane_cluster(M, B) is the cluster size of
+// the instantiated (half row length, column length) pairs, 0 when there is none
+int plane_cluster(int M, int NB);
+void init_plane_attributes(int optin);
+void launch_plane_r2c(cudaStream_t st, const SimDev* d_sims, const int* d_t, const BlockWork* map, int nmap,
+                      const RowR2CJob& job, int M, int NB);
 void launch_rowr_r2c(cudaStream_t st, const SimDev* d_sims, const int* d_t, const BlockWork* map, int nmap,
                      const RowR2CJob& job, int M);
 void launch_rowr_c2r(cudaStream_t st, const SimDev* d_sims, const int* d_t, const BlockWork* map, int nmap,

@@ -221,6 +221,7 @@ void init_col_attributes(int optin) {
     set_col_attrs<COL_FWD_OP_INV>(optin);
     init_colop_attributes(optin);
     init_cola_attributes(optin);
+    init_plane_attributes(optin);
 }
 
 template <int MODE>

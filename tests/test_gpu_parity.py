@@ -187,6 +187,41 @@ def test_double_buffered_column_passes(shape, cola, monkeypatch):
     compare(run_gpu(b), ref)
 
 
+def _plane_case(shape, seed):
+    """3D heterogeneous nonlinear power-law IVP (a p0 ball off centre) with a sensor plane, thin
+    along A so that long B and C lines stay cheap for the oracle."""
+    rng = np.random.default_rng(seed)
+    c = (1500 + 60 * rng.standard_normal(shape)).astype(np.float32)
+    rho = (1000 + 40 * rng.standard_normal(shape)).astype(np.float32)
+    args = []
+    for n in shape:
+        args += [n, 1e-4]
+    g = KWaveGrid(*args)
+    g.makeTime(float(c.max()), cfl=0.3)
+    g.setTime(24, g.dt)
+    a, b, cc = shape
+    p0 = makeBall(a, b, cc, a // 2, b // 3, cc // 2 + 3, 3) * 1e4
+    sm = np.zeros(shape, np.float32)
+    sm[:, :, cc // 2] = 1
+    med = KWaveMedium(c, rho, alphaCoeff=0.5, alphaPower=1.5, alphaMode=1, bOnA=5.0)
+    return DescBuilder(g, med, KWaveSource(p0=p0), KWaveSensor(mask=sm, record=RecordField.p | RecordField.pFinal),
+                       SimulationOptions(pmlSize=4, smoothP0=False))
+
+
+@pytest.mark.parametrize("plane", ["1", "0"])
+@pytest.mark.parametrize("shape", [(16, 32, 32), (12, 48, 48), (12, 64, 128), (10, 128, 256), (10, 256, 256),
+                                   (10, 384, 384)])
+def test_plane_pass_shapes(shape, plane, monkeypatch):
+    # 3D: the R2C and the forward pass along B as one cluster kernel per plane (cluster sizes 1, 2,
+    # 4 and 8, the packed DC / Nyquist column) against the separate passes and the oracle
+    monkeypatch.setenv("KW_PLANE", plane)
+    b = _plane_case(shape, sum(shape) // 3)
+    ref, _ = oracle.run(b)
+    out = run_gpu(b)
+    assert np.abs(ref["p"]).max() > 0
+    compare(out, ref)
+
+
 def test_batch_equals_individual_runs():
     rng = np.random.default_rng(3)
     builders = []
