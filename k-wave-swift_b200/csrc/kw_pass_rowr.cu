@@ -22,8 +22,16 @@ namespace kw {
 // ---------------------------------------------------------------------------------------------
 // R2C: X[k] = (Z[k] + conj Z[M-k]) / 2 - i W_C^k (Z[k] - conj Z[M-k]) / 2, k = 0 .. M
 // ---------------------------------------------------------------------------------------------
+// Resident CTAs per SM the register budget is cut to (3 = at most 85 registers a thread): the
+// R2C and the C2R epilogues that fit without spilling take three CTAs per SM for more loads in
+// flight; the others keep the compiler's choice.
+template <int M, int EPI, bool TAPE>
+constexpr int rowr_minb() {
+    return (M <= 128 && !TAPE && EPI != EPI_ADD_RHO && EPI != EPI_ADJ_EOS) ? 3 : 1;
+}
+
 template <int M>
-__global__ void __launch_bounds__(256) k_rowr_r2c(const SimDev* __restrict__ sims, const int* __restrict__ d_t,
+__global__ void __launch_bounds__(256, 3) k_rowr_r2c(const SimDev* __restrict__ sims, const int* __restrict__ d_t,
                                                   const BlockWork* __restrict__ map, int nmap, RowR2CJob job) {
     using P = RegPlan<M, reg_r1(M)>;
     using Lay = RowLayout<P, M>;
@@ -73,7 +81,7 @@ __device__ __forceinline__ float2 ld_medium(const FieldOrScalar& f, long long e)
 __device__ __forceinline__ float& half(float2& v, int h) { return h ? v.y : v.x; }
 
 template <int M, int EPI, bool TAPE = false>
-__global__ void __launch_bounds__(256) k_rowr_c2r(const SimDev* __restrict__ sims, const int* __restrict__ d_t,
+__global__ void __launch_bounds__(256, rowr_minb<M, EPI, TAPE>()) k_rowr_c2r(const SimDev* __restrict__ sims, const int* __restrict__ d_t,
                                                   const BlockWork* __restrict__ map, int nmap, RowC2RJob job) {
     using P = RegPlan<M, c2r_r1(M)>;
     using Lay = RowLayout<P, M>;
