@@ -137,7 +137,7 @@ private:
         return p;
     }
     void check(cudaError_t e, const char* what);
-    cudaStream_t st() const { return ctx_->stream; }
+    cudaStream_t st() const { return st_override_ ? st_override_ : ctx_->stream; }
 
     void setup_sim(int s, const kw_sim_desc& d);
     void build_tensor_maps(SimHost& h, SimDev& v);   // kw_tmaps.cpp
@@ -177,6 +177,7 @@ private:
     size_t arena_size_ = 0, arena_used_ = 0;
     bool finalized_ = false;
     bool tape_mode_ = false;   // adjoint: steps are captured with the tape epilogues
+    cudaStream_t st_override_ = nullptr;   // adjoint: the reverse sweep's own stream while it issues work
     int finalized_t_ = -1;
     // finalised aggregate outputs per sim (device)
     struct Outs {

@@ -31,7 +31,7 @@ constexpr int rowr_minb() {
 }
 
 template <int M>
-__global__ void __launch_bounds__(256, 3) k_rowr_r2c(const SimDev* __restrict__ sims, const int* __restrict__ d_t,
+__global__ void __launch_bounds__(256, rowr_minb<M, EPI_STORE, false>()) k_rowr_r2c(const SimDev* __restrict__ sims, const int* __restrict__ d_t,
                                                   const BlockWork* __restrict__ map, int nmap, RowR2CJob job) {
     using P = RegPlan<M, reg_r1(M)>;
     using Lay = RowLayout<P, M>;

@@ -78,6 +78,22 @@ def test_fan_in_sum_matches_per_component_sum(shape, kw, cola, monkeypatch):
         assert rel_l2(r1["grad_p0"], r0["grad_p0"]) < 1e-4
 
 
+@pytest.mark.parametrize("shape,kw", [((40, 36), dict(absorb="powerlaw", nonlinear=True, nt=45)),
+                                      ((16, 20, 32), dict(absorb="stokes", nonlinear=True, nt=30))])
+def test_overlapped_reverse_sweep_matches_sequential(shape, kw, monkeypatch):
+    # segment c + 1 reversed on a second stream while segment c is recomputed (two tape banks)
+    # gives the same gradient as running them one after the other
+    c, p0, data, kw = problem(shape, **kw)
+    monkeypatch.setenv("KW_ADJOINT_OVERLAP", "1")
+    r1 = gpu_adjoint(shape, c, p0, data, kw, policy=abi.KW_CHECKPOINT_INTERVAL, interval=6)
+    monkeypatch.setenv("KW_ADJOINT_OVERLAP", "0")
+    r0 = gpu_adjoint(shape, c, p0, data, kw, policy=abi.KW_CHECKPOINT_INTERVAL, interval=6)
+    assert r1["checkpoints"] == r0["checkpoints"] > 2
+    assert rel_l2(r1["grad_c0"], r0["grad_c0"]) < 1e-6
+    assert rel_l2(r1["grad_p0"], r0["grad_p0"]) < 1e-6
+    assert r1["misfit"] == r0["misfit"]
+
+
 def test_checkpoint_policies_agree():
     shape = (40, 36)
     c, p0, data, kw = problem(shape, absorb="powerlaw", nonlinear=True, nt=45)
