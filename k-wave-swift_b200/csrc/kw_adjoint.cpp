@@ -88,11 +88,12 @@ void Engine::adjoint(const kw_sim_desc& din, kw_adjoint_desc& a) {
     const int tp_fields = 2 + (stokes ? 1 : 0) + (nonlin ? D : 0) + (disp ? 1 : 0);   // p, S, div, d_a, A2(S)
     bool store_all = a.policy == KW_CHECKPOINT_STORE_ALL;
     // With checkpoints, segment c's recompute runs on the library's stream while segment c + 1 is
-    // reversed on a second stream: the tape has two banks of K slots (even and odd segments) and the
-    // reverse sweep its own spectra. KW_ADJOINT_OVERLAP=0 runs them one after the other.
+    // reversed on a second stream (the reverse sweep has its own spectra). The K tape slots are
+    // walked forwards by even segments and backwards by odd ones, so the recompute of segment c
+    // fills the slots in the order the reverse of segment c + 1 releases them; each recomputed step
+    // waits for its slot's release. KW_ADJOINT_OVERLAP=0 runs them one after the other.
     bool overlap = true;
     if (const char* f = std::getenv("KW_ADJOINT_OVERLAP")) overlap = f[0] != '0';
-    const int banks_cost = overlap ? 2 : 1;   // tape banks the memory-budget schedule tries first
     int K = 1;
     if (a.policy == KW_CHECKPOINT_SQRT) K = (int)std::ceil(std::sqrt((double)nt));
     else if (a.policy == KW_CHECKPOINT_INTERVAL) K = a.checkpoint_interval;
@@ -100,16 +101,11 @@ void Engine::adjoint(const kw_sim_desc& din, kw_adjoint_desc& a) {
         const double all = (double)nt * tp_fields * fb;
         if (all <= a.memory_budget) store_all = true;
         else {
-            // memory(K) = ceil(nt / K) checkpoints + K tape slots per bank; one bank (no overlap)
-            // when two do not fit
+            // memory(K) = ceil(nt / K) checkpoints + K tape slots
             double best = 1e300;
-            for (int banks_try = banks_cost; banks_try >= 1 && best > a.memory_budget; --banks_try) {
-                best = 1e300;
-                for (int k = 1; k <= nt; ++k) {
-                    const double m = (double)((nt + k - 1) / k) * ck_fields * fb + (double)banks_try * k * tp_fields * fb;
-                    if (m < best) { best = m; K = k; }
-                }
-                if (banks_try == 1) overlap = false;
+            for (int k = 1; k <= nt; ++k) {
+                const double m = (double)((nt + k - 1) / k) * ck_fields * fb + (double)k * tp_fields * fb;
+                if (m < best) { best = m; K = k; }
             }
             if (best > a.memory_budget) throw err(KW_ERR_OOM, "adjoint: the smallest checkpoint schedule needs more than memory_budget");
         }
@@ -118,17 +114,16 @@ void Engine::adjoint(const kw_sim_desc& din, kw_adjoint_desc& a) {
     if (K < 1 || K > nt) throw err(KW_ERR_INVALID, "adjoint: checkpoint_interval must be in [1, nt]");
     const int nck = store_all ? 0 : (nt + K - 1) / K;
     if (nck < 2) overlap = false;
-    const int banks = overlap ? 2 : 1;
     a.interval = K;
     a.checkpoints = nck;
 
-    // tape: banks x K slots of tp_fields fields; checkpoints: nck of ck_fields fields
+    // tape: K slots of tp_fields fields; checkpoints: nck of ck_fields fields
     auto alloc_fields = [&](size_t count) {
         std::vector<float*> f(count);
         for (auto& x : f) x = (float*)dalloc(fb);
         return f;
     };
-    std::vector<float*> tape = alloc_fields((size_t)banks * K * tp_fields);
+    std::vector<float*> tape = alloc_fields((size_t)K * tp_fields);
     std::vector<float*> ck = alloc_fields((size_t)nck * ck_fields);
     auto tslot = [&](int slot, int f) { return tape[(size_t)slot * tp_fields + f]; };   // f: 0 p, 1 S, 2 div, then d_a, A2(S)
     const int TF_DIV = 2, TF_DD = stokes ? 3 : 2, TF_Q2 = TF_DD + (nonlin ? D : 0);
@@ -139,17 +134,19 @@ void Engine::adjoint(const kw_sim_desc& din, kw_adjoint_desc& a) {
     auto zero = [&](float* x) { check(cudaMemsetAsync(x, 0, fb, st()), "adjoint zero"); };
     float* zero_field = (float*)dalloc(fb);   // S(-1): the state before step 0 is zero
 
+    // tape slot of step t: even segments walk the slots forwards, odd ones backwards
+    auto slot_of = [&](int t) { return store_all ? t : ((t / K) % 2 == 0 ? t % K : K - 1 - t % K); };
     // where step t's forward quantities live while the reverse sweep reads them
     std::vector<AdjTapeEntry> table(nt);
     for (int t = 0; t < nt; ++t) {
-        const int slot = store_all ? t : (t / K % banks) * K + t % K;
+        const int slot = slot_of(t);
         AdjTapeEntry& e = table[t];
         e.p = tslot(slot, 0);
         e.s = tslot(slot, 1);
         e.div = stokes ? tslot(slot, TF_DIV) : nullptr;
         for (int b = 0; b < kMaxComp; ++b) e.dd[b] = nonlin && b < D ? tslot(slot, TF_DD + b) : nullptr;
         e.q2 = disp ? tslot(slot, TF_Q2) : nullptr;
-        e.sprev = t == 0 ? zero_field : (store_all || t % K > 0 ? tslot(slot - 1, 1) : ckf(t / K, 2 * D + 2));
+        e.sprev = t == 0 ? zero_field : (store_all || t % K > 0 ? tslot(slot_of(t - 1), 1) : ckf(t / K, 2 * D + 2));
     }
     const AdjTapeEntry* d_table = upload(table);
     v.tape = d_table;
@@ -223,7 +220,8 @@ void Engine::adjoint(const kw_sim_desc& din, kw_adjoint_desc& a) {
     cudaStream_t rs = nullptr;
     SimDev* d_sims_rev = nullptr;
     int* d_t_rev = nullptr;
-    cudaEvent_t ev_rec = nullptr, ev_done = nullptr, ev_bank[2] = {nullptr, nullptr};
+    cudaEvent_t ev_rec = nullptr, ev_done = nullptr;
+    std::vector<cudaEvent_t> ev_free;   // per tape slot: its last reader in the reverse sweep is done
     if (overlap) {
         SimDev vr = v;
         for (int k = 0; k < 4; ++k) {
@@ -239,12 +237,16 @@ void Engine::adjoint(const kw_sim_desc& din, kw_adjoint_desc& a) {
         check(cudaMemcpyAsync(d_sims_rev, &vr, sizeof(SimDev), cudaMemcpyHostToDevice, fs), "upload sim");
         d_t_rev = (int*)dalloc(sizeof(int));
         check(cudaStreamCreateWithFlags(&rs, cudaStreamNonBlocking), "stream");
-        for (cudaEvent_t* e : {&ev_rec, &ev_done, &ev_bank[0], &ev_bank[1]})
+        for (cudaEvent_t* e : {&ev_rec, &ev_done})
             check(cudaEventCreateWithFlags(e, cudaEventDisableTiming), "event");
-        // both banks are free, and the reverse stream starts after the zeroing above
-        check(cudaEventRecord(ev_bank[0], fs), "event");
-        check(cudaEventRecord(ev_bank[1], fs), "event");
-        check(cudaStreamWaitEvent(rs, ev_bank[0], 0), "wait");
+        ev_free.assign(K, nullptr);
+        for (auto& e : ev_free) {
+            check(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "event");
+            check(cudaEventRecord(e, fs), "event");   // every slot is free
+        }
+        // the reverse stream starts after the zeroing above
+        check(cudaEventRecord(ev_rec, fs), "event");
+        check(cudaStreamWaitEvent(rs, ev_rec, 0), "wait");
     }
     // issue `fn` as reverse-sweep work (on the reverse stream when overlapped)
     auto on_reverse = [&](auto&& fn) {
@@ -363,8 +365,11 @@ void Engine::adjoint(const kw_sim_desc& din, kw_adjoint_desc& a) {
         for (int c = nck - 1; c >= 0; --c) {
             const int t0 = c * K, t1 = std::min(t0 + K, nt);
             if (t1 - 1 < t_stop) continue;
-            // this segment's tape bank was last read by the reverse of segment c + 2
-            if (overlap) check(cudaStreamWaitEvent(fs, ev_bank[c % 2], 0), "wait");
+            // slot writes wait until the reverse of segment c + 1 has released the slot
+            auto slot_free = [&](int t) {
+                if (overlap) check(cudaStreamWaitEvent(fs, ev_free[slot_of(t)], 0), "wait");
+            };
+            slot_free(t0);
             // restore the state after step t0 and rerun the segment, storing each step
             for (int b = 0; b < D; ++b) { cpy(v.u[b], ckf(c, b)); cpy(v.rho[b], ckf(c, D + b)); }
             cpy(v.rho_sum, ckf(c, 2 * D));
@@ -379,16 +384,21 @@ void Engine::adjoint(const kw_sim_desc& din, kw_adjoint_desc& a) {
             launch_set_step(st(), d_t_, t0 + 1);
             t_ = t0 + 1;
             tape_copy();
-            for (int t = t0 + 1; t < t1; ++t) step(1);
+            for (int t = t0 + 1; t < t1; ++t) {
+                slot_free(t);
+                step(1);
+            }
             if (overlap) {
                 check(cudaEventRecord(ev_rec, fs), "event");
                 check(cudaStreamWaitEvent(rs, ev_rec, 0), "wait");
             }
             // the reverse of this segment overlaps the recompute of the next one
             on_reverse([&] {
-                for (int t = t1 - 1; t >= std::max(t0, t_stop); --t) reverse_step(t);
+                for (int t = t1 - 1; t >= std::max(t0, t_stop); --t) {
+                    reverse_step(t);
+                    if (overlap) check(cudaEventRecord(ev_free[slot_of(t)], rs), "event");
+                }
             });
-            if (overlap) check(cudaEventRecord(ev_bank[c % 2], rs), "event");
         }
         if (overlap) {
             check(cudaEventRecord(ev_done, rs), "event");
@@ -429,7 +439,9 @@ void Engine::adjoint(const kw_sim_desc& din, kw_adjoint_desc& a) {
     if (rs) {
         cudaStreamSynchronize(rs);
         cudaStreamDestroy(rs);
-        for (cudaEvent_t e : {ev_rec, ev_done, ev_bank[0], ev_bank[1]})
+        for (cudaEvent_t e : {ev_rec, ev_done})
+            if (e) cudaEventDestroy(e);
+        for (cudaEvent_t e : ev_free)
             if (e) cudaEventDestroy(e);
     }
     set_tape_mode(false);

@@ -24,10 +24,11 @@ namespace kw {
 // ---------------------------------------------------------------------------------------------
 // Resident CTAs per SM the register budget is cut to (3 = at most 85 registers a thread): the
 // R2C and the C2R epilogues that fit without spilling take three CTAs per SM for more loads in
-// flight; the others keep the compiler's choice.
+// flight; the others keep the compiler's choice (0: no minimum; a minimum of 1 lets the compiler
+// take more registers and the 384-point rows ran 1.4x slower with it).
 template <int M, int EPI, bool TAPE>
 constexpr int rowr_minb() {
-    return (M <= 128 && !TAPE && EPI != EPI_ADD_RHO && EPI != EPI_ADJ_EOS) ? 3 : 1;
+    return (M <= 128 && !TAPE && EPI != EPI_ADD_RHO && EPI != EPI_ADJ_EOS) ? 3 : 0;
 }
 
 template <int M>
