@@ -15,8 +15,12 @@
 
 namespace kw {
 
+// three CTAs per SM (85 registers) up to 256 points; longer lines keep the compiler's choice
 template <int N>
-__global__ void __launch_bounds__(256) k_colop(const SimDev* __restrict__ sims, const int* __restrict__ d_t,
+constexpr int colop_minb() { return N <= 256 ? 3 : 0; }
+
+template <int N>
+__global__ void __launch_bounds__(256, colop_minb<N>()) k_colop(const SimDev* __restrict__ sims, const int* __restrict__ d_t,
                                                const BlockWork* __restrict__ map, int nmap, ColJob job) {
     using P = RegPlan<N, reg_r1(N)>;
     using Lay = ColLayout<P, N>;

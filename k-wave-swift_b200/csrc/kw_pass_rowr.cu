@@ -22,9 +22,9 @@ namespace kw {
 // ---------------------------------------------------------------------------------------------
 // R2C: X[k] = (Z[k] + conj Z[M-k]) / 2 - i W_C^k (Z[k] - conj Z[M-k]) / 2, k = 0 .. M
 // ---------------------------------------------------------------------------------------------
-// Resident CTAs per SM the register budget is cut to (3 = at most 85 registers a thread): the
-// R2C and the C2R epilogues that fit without spilling take three CTAs per SM for more loads in
-// flight; the others keep the compiler's choice (0: no minimum; a minimum of 1 lets the compiler
+// Resident CTAs per SM the register budget of a C2R kernel is cut to (3 = at most 85 registers a
+// thread): the epilogues that fit without spilling take three CTAs per SM for more loads in flight;
+// the others, and the R2C, keep the compiler's choice (0: no minimum; a minimum of 1 lets the compiler
 // take more registers and the 384-point rows ran 1.4x slower with it).
 template <int M, int EPI, bool TAPE>
 constexpr int rowr_minb() {
@@ -32,7 +32,7 @@ constexpr int rowr_minb() {
 }
 
 template <int M>
-__global__ void __launch_bounds__(256, rowr_minb<M, EPI_STORE, false>()) k_rowr_r2c(const SimDev* __restrict__ sims, const int* __restrict__ d_t,
+__global__ void __launch_bounds__(256) k_rowr_r2c(const SimDev* __restrict__ sims, const int* __restrict__ d_t,
                                                   const BlockWork* __restrict__ map, int nmap, RowR2CJob job) {
     using P = RegPlan<M, reg_r1(M)>;
     using Lay = RowLayout<P, M>;
