@@ -197,16 +197,10 @@ def run_batch(args) -> None:
     from kwave import workloads
     from kwave.runtime import Context
 
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    torch.cuda.set_device(local)
-    dist = None
-    if world > 1:
-        import datetime
-
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    from kwave import replicas
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    rep = replicas.init("nccl")   # one replica per GPU; no collective on the data path
+    world, rank, local = rep.world, rep.rank, rep.local
     builders = workloads.batch2d()
     W = args.warmup
     work = float(sum(b.grid.totalGridPoints * b.grid.nt for b in builders))
@@ -223,8 +217,7 @@ def run_batch(args) -> None:
     batch.step(W)
     batch.reset()
     torch.cuda.synchronize()
-    if dist:
-        dist.barrier()
+    rep.barrier()
     gpu_id = "GPU-" + str(torch.cuda.get_device_properties(local).uuid)
     steps = max(b.grid.nt for b in builders)
     e0, e1 = ev(), ev()
@@ -262,10 +255,8 @@ def run_batch(args) -> None:
     h2d = sum(sum(a.nbytes for a in b.keep) for b in builders)
     d2h = sum(o.nbytes for o in outs if o is not None)
 
-    if dist:
-        t = torch.tensor([ms_batch, ms_plain], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms_batch, ms_plain = float(t[0]), float(t[1])
+    ms_batch = rep.max_over_ranks(ms_batch, device="cuda")
+    ms_plain = rep.max_over_ranks(ms_plain, device="cuda")
     if rank == 0:
         peak, peak_kind = measured_peak_gbs()
         sizes = sorted({b.grid.shape[0] for b in builders})
@@ -289,9 +280,7 @@ def run_batch(args) -> None:
         }
         print(json.dumps(line), flush=True)
     ctx.close()
-    if dist:
-        dist.barrier()
-        dist.destroy_process_group()
+    rep.close()
 
 
 ADJ = "adjoint2d_512"
@@ -336,16 +325,10 @@ def run_adjoint(args) -> None:
     from kwave import abi, workloads
     from kwave.runtime import Context
 
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    torch.cuda.set_device(local)
-    dist = None
-    if world > 1:
-        import datetime
-
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    from kwave import replicas
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    rep = replicas.init("nccl")   # one replica per GPU; no collective on the data path
+    world, rank, local = rep.world, rep.rank, rep.local
     three_d = args.workload == ADJ3
     bp, bt = workloads.adjoint3d() if three_d else workloads.adjoint2d()
     nt, npts = bp.grid.nt, bp.grid.totalGridPoints
@@ -388,10 +371,8 @@ def run_adjoint(args) -> None:
         r_all = None if three_d else ctx.adjoint(bp, data, policy=abi.KW_CHECKPOINT_STORE_ALL)
     grad_ms = r["forward_ms"] + r["reverse_ms"]
     all_ms = r_all["forward_ms"] + r_all["reverse_ms"] if r_all else None
-    if dist:
-        t = torch.tensor([grad_ms, fwd_ms], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        grad_ms, fwd_ms = float(t[0]), float(t[1])
+    grad_ms = rep.max_over_ranks(grad_ms, device="cuda")
+    fwd_ms = rep.max_over_ranks(fwd_ms, device="cuda")
     if rank == 0:
         g = r["grad_c0"]
         line = {
@@ -419,9 +400,7 @@ def run_adjoint(args) -> None:
         }
         print(json.dumps(line), flush=True)
     ctx.close()
-    if dist:
-        dist.barrier()
-        dist.destroy_process_group()
+    rep.close()
 
 
 def run_ours(args) -> None:
@@ -430,16 +409,10 @@ def run_ours(args) -> None:
 
     from kwave.runtime import Context
 
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    torch.cuda.set_device(local)
-    dist = None
-    if world > 1:
-        import datetime
-
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    from kwave import replicas
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    rep = replicas.init("nccl")   # one replica per GPU; no collective on the data path
+    world, rank, local = rep.world, rep.rank, rep.local
     W = args.warmup
     b = workload(args.workload, (args.steps or 1) + W)
     # default: the whole simulation (every time step after the warm-up ones)
@@ -458,8 +431,7 @@ def run_ours(args) -> None:
         gpu_id = "GPU-" + str(torch.cuda.get_device_properties(local).uuid)
     except Exception:
         gpu_id = str(local)
-    if dist:
-        dist.barrier()
+    rep.barrier()
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     with ClockSampler(gpu_id) as clk:
@@ -467,14 +439,10 @@ def run_ours(args) -> None:
         sim.step(K)
         e1.record(stream)
         torch.cuda.synchronize()
-    if dist:
-        dist.barrier()
+    rep.barrier()
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1)
-    if dist:
-        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = rep.max_over_ranks(ms, device="cuda")
     value = npts * K * world / (ms / 1e3)
 
     # per-launch device profile of a step, taken on a restarted run right after its warm-up steps
@@ -558,9 +526,7 @@ def run_ours(args) -> None:
         }
         print(json.dumps(line), flush=True)
     ctx.close()
-    if dist:
-        dist.barrier()
-        dist.destroy_process_group()
+    rep.close()
 
 
 def main() -> None:
