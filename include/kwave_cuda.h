@@ -32,7 +32,7 @@
 extern "C" {
 #endif
 
-#define KW_ABI_VERSION 1
+#define KW_ABI_VERSION 2
 
 #if defined(__GNUC__)
 #define KW_API __attribute__((visibility("default")))
@@ -190,6 +190,11 @@ typedef struct kw_sim_desc {
     const float* directivity_angle;  /* 2D binary sensors only: grid-shaped angles (rad) or NULL */
     double directivity_size;         /* NaN: 10*max(dx, dy) */
     int directivity_pattern;         /* kw_directivity_pattern */
+
+    /* 1: run kspaceFirstOrderAS (Solver/KSpaceFirstOrderAS.swift:19-309) instead of
+     * kspaceFirstOrder: 2D, x axial, y radial (r >= 0, PML at the outer edge only); p0 and
+     * pressure / velocity sources, Stokes absorption, B/A; records p and pFinal. */
+    int axisymmetric;
 } kw_sim_desc;
 
 /* Fill a descriptor with the reference's defaults (SimulationOptions(), KWaveSource(),

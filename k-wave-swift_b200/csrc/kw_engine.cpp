@@ -907,6 +907,8 @@ void Engine::setup_sim(int s, const kw_sim_desc& d) {
 
 void Engine::create(const kw_sim_desc* descs, int n) {
     if (n <= 0) throw err(KW_ERR_INVALID, "no simulations");
+    for (int i = 0; i < n; ++i)
+        if (descs[i].axisymmetric) throw err(KW_ERR_UNSUPPORTED, "the axisymmetric solver is not available in this build");
     check(cudaSetDevice(ctx_->device), "cudaSetDevice");
     sims_.resize(n);
     outs_.resize(n);

@@ -7,12 +7,13 @@ from .abi import FIELDS
 from .api import (AbsorptionMode, AdjointOutput, DescBuilder, DeviceKind, DirectivityPattern, KWaveError,
                   KWaveGrid, KWaveMedium, KWaveSensor, KWaveSource, RecordField,
                   SimulationOptions, SimulationOutput, SourceMode, kspaceFirstOrder,
-                  kspaceFirstOrderAdjoint, timeReversal, wavenumberVector)
+                  kspaceFirstOrderAdjoint, kspaceFirstOrderAS, timeReversal, wavenumberVector)
 from .shapes import gaussian, makeBall, makeCartCircle, makeCircle, makeDisc, toneBurst
 
 __all__ = [
     "AbsorptionMode", "AdjointOutput", "DescBuilder", "DeviceKind", "DirectivityPattern", "FIELDS", "KWaveError",
     "KWaveGrid", "KWaveMedium", "KWaveSensor", "KWaveSource", "RecordField", "SimulationOptions",
-    "SimulationOutput", "SourceMode", "gaussian", "kspaceFirstOrder", "kspaceFirstOrderAdjoint", "makeBall",
+    "SimulationOutput", "SourceMode", "gaussian", "kspaceFirstOrder", "kspaceFirstOrderAS", "kspaceFirstOrderAdjoint",
+    "makeBall",
     "makeCartCircle", "makeCircle", "makeDisc", "timeReversal", "toneBurst", "wavenumberVector",
 ]

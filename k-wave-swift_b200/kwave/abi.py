@@ -7,7 +7,7 @@ from __future__ import annotations
 
 import ctypes as C
 
-KW_ABI_VERSION = 1
+KW_ABI_VERSION = 2
 
 # kw_status
 KW_OK = 0
@@ -83,6 +83,7 @@ class kw_sim_desc(C.Structure):
         ("directivity_angle", C.POINTER(C.c_float)),
         ("directivity_size", C.c_double),
         ("directivity_pattern", C.c_int),
+        ("axisymmetric", C.c_int),
     ]
 
 

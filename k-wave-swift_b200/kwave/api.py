@@ -237,7 +237,7 @@ class DescBuilder:
     """Flattens the mirror structs into one kw_sim_desc, keeping the host arrays alive."""
 
     def __init__(self, grid: KWaveGrid, medium: KWaveMedium, source: KWaveSource,
-                 sensor: KWaveSensor, options: Optional[SimulationOptions] = None):
+                 sensor: KWaveSensor, options: Optional[SimulationOptions] = None, axisymmetric: bool = False):
         options = options or SimulationOptions()
         self.keep: list[np.ndarray] = []
         self.grid = grid
@@ -250,6 +250,7 @@ class DescBuilder:
         d.nx, d.ny, d.nz = grid.nx, grid.ny, grid.nz
         d.dx, d.dy, d.dz = grid.dx, grid.dy, grid.dz
         d.dt, d.nt = grid.dt, grid.nt
+        d.axisymmetric = int(bool(axisymmetric))
         d.pml_size = int(options.pmlSize)
         d.pml_alpha = float(options.pmlAlpha)
         d.smooth_p0 = int(bool(options.smoothP0))
@@ -351,6 +352,28 @@ def kspaceFirstOrder(grid: KWaveGrid, medium: KWaveMedium, source: KWaveSource,
         raise KWaveError(abi.KW_ERR_INVALID, f"kspaceFirstOrder: dim {grid.dim} not yet implemented")
     with Context.default() as ctx:
         sim = ctx.create_sim(DescBuilder(grid, medium, source, sensor, options))
+        try:
+            sim.run(progress=options.progress, monitor=options.fieldMonitor,
+                    monitor_interval=options.fieldMonitorInterval)
+            return sim.outputs()
+        finally:
+            sim.close()
+
+
+def kspaceFirstOrderAS(grid: KWaveGrid, medium: KWaveMedium, source: KWaveSource,
+                       sensor: KWaveSensor, options: Optional[SimulationOptions] = None) -> SimulationOutput:
+    """Axisymmetric k-space solver on the GPU (KSpaceFirstOrderAS.swift:19-309): a 2D grid with x
+    axial and y radial (r >= 0); p0 and pressure / velocity sources, Stokes absorption, B/A;
+    returns p and pFinal."""
+    from .runtime import Context
+
+    options = options or SimulationOptions()
+    if options.device == DeviceKind.cpu:
+        raise KWaveError(abi.KW_ERR_UNSUPPORTED, "this build runs on CUDA devices only")
+    if grid.dim != 2:
+        raise KWaveError(abi.KW_ERR_INVALID, "axisymmetric solver requires a 2D grid (x axial, y radial)")
+    with Context.default() as ctx:
+        sim = ctx.create_sim(DescBuilder(grid, medium, source, sensor, options, axisymmetric=True))
         try:
             sim.run(progress=options.progress, monitor=options.fieldMonitor,
                     monitor_interval=options.fieldMonitorInterval)

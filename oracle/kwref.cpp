@@ -742,6 +742,227 @@ static void sample_field(const Model& m, const vecd& f, vecd& dst) {
     }
 }
 
+/* ======================================================================================
+ * Axisymmetric solver (Solver/KSpaceFirstOrderAS.swift:19-309): x axial (FFT, periodic), y radial
+ * (r >= 0). Fields are mirrored into a 4x-expanded radial grid with their symmetry (p, ux: WSWA;
+ * uy: HAHS; uy / r: HSHA) and transformed with ordinary 2D FFTs there; the radial PML is
+ * one-sided; the divergence gains uy / r on the staggered radial grid r = (j + 1/2) dy.
+ * Scope as the reference: p0, pressure and velocity sources (all three modes), Stokes
+ * absorption, B/A, p / pFinal recording.
+ * ====================================================================================== */
+static int run_as(const kw_sim_desc* d, int max_steps, kwref_result** out) {
+    if (d->dim != 2) { g_err = "axisymmetric solver requires a 2D grid (x axial, y radial)"; return KW_ERR_INVALID; }
+    Model m;   // parsing of the medium, sources (signals, scales), p0, sensor (KSFO rules)
+    const int st0 = build_model(d, m);
+    if (st0 != KW_OK) return st0;
+    if (m.absorb && !m.stokes) { g_err = "axisymmetric absorption requires the Stokes model (alphaPower = 2)"; return KW_ERR_INVALID; }
+    const int nx = m.s.n[0], ny = m.s.n[1], nyE = 4 * ny;
+    const size_t N = m.N, NE = (size_t)nx * nyE;
+    const double dx = m.s.d[0], dy = m.s.d[1], dt = m.dt;
+    Shape se; se.dim = 2; se.n[0] = nx; se.n[1] = nyE; se.d[0] = dx; se.d[1] = dy; se.finish();
+    // k-space operators on the expanded grid (KSpaceFirstOrderAS.swift:51-67)
+    const vecd kx = wavenumber_vector(nx, dx), kyE = wavenumber_vector(nyE, dy);
+    vecd kappa(NE), skappa(NE);
+    for (int i = 0; i < nx; ++i)
+        for (int j = 0; j < nyE; ++j) {
+            const double arg = std::sqrt(kx[i] * kx[i] + kyE[j] * kyE[j]) * (m.cRef * dt / 2.0);
+            kappa[(size_t)i * nyE + j] = arg == 0.0 ? 1.0 : std::sin(arg) / arg;
+            skappa[(size_t)i * nyE + j] = std::cos(arg);
+        }
+    const cd I(0, 1);
+    vecc ddxPos(nx), ddxNeg(nx), ddyPos(nyE), ddyNeg(nyE), yShNeg(nyE);
+    for (int i = 0; i < nx; ++i) {
+        const double th = kx[i] * dx / 2.0;
+        ddxPos[i] = I * kx[i] * cd(std::cos(th), std::sin(th));
+        ddxNeg[i] = I * kx[i] * cd(std::cos(th), -std::sin(th));
+    }
+    for (int j = 0; j < nyE; ++j) {
+        const double th = kyE[j] * dy / 2.0;
+        ddyPos[j] = I * kyE[j] * cd(std::cos(th), std::sin(th));
+        ddyNeg[j] = I * kyE[j] * cd(std::cos(th), -std::sin(th));
+        yShNeg[j] = cd(std::cos(th), -std::sin(th));
+    }
+    // PMLs: axial two-sided, radial outer edge only (PML.swift:17-43 axisymmetric)
+    auto one_sided = [&](bool stag) {   // the right ramp of PML.swift:27-41 only
+        vecd v(ny, 1.0);
+        const double a = d->pml_alpha * (m.cRef / dy), md = (double)d->pml_size;
+        for (int k = 0; k < std::min(d->pml_size, ny); ++k) {
+            const double x = (double)(k + 1), pos = stag ? (x + 0.5) / md : x / md;
+            v[ny - d->pml_size + k] = std::exp(-a * dt / 2.0 * std::pow(pos, 4.0));
+        }
+        return v;
+    };
+    const vecd& pmlX = m.pml[0];
+    const vecd& pmlXsg = m.pmlSg[0];
+    const vecd pmlY = one_sided(false), pmlYsg = one_sided(true);
+    vecd invYsg(ny);
+    for (int j = 0; j < ny; ++j) invYsg[j] = 1.0 / ((j + 0.5) * dy);
+    // pressure source into both density splits with the axial spacing (KSpaceFirstOrderAS.swift:160-163)
+    const SourceOp& pOp = m.pOp[0];
+    const bool hasP = m.hasP[0];
+    const int umode = d->u_mode;
+
+    auto mirror = [&](const vecd& w, int kind, vecc& e) {   // 0 WSWA, 1 HAHS, 2 HSHA
+        e.assign(NE, cd(0, 0));
+        for (int i = 0; i < nx; ++i) {
+            const double* r = &w[(size_t)i * ny];
+            cd* o = &e[(size_t)i * nyE];
+            if (kind == 0) {
+                for (int j = 0; j < ny; ++j) { o[j] = r[j]; o[2 * ny + j] = -r[j]; }
+                for (int j = 1; j < ny; ++j) { o[ny + j] = -r[ny - j]; o[3 * ny + j] = r[ny - j]; }
+                o[ny] = 0.0; o[3 * ny] = 0.0;
+            } else {
+                const double sg = kind == 1 ? 1.0 : -1.0;
+                for (int j = 0; j < ny; ++j) {
+                    o[j] = r[j]; o[ny + j] = sg * r[ny - 1 - j];
+                    o[2 * ny + j] = -r[j]; o[3 * ny + j] = -sg * r[ny - 1 - j];
+                }
+            }
+        }
+    };
+    auto trim = [&](const vecc& e, vecd& w) {
+        w.resize(N);
+        for (int i = 0; i < nx; ++i)
+            for (int j = 0; j < ny; ++j) w[(size_t)i * ny + j] = e[(size_t)i * nyE + j].real();
+    };
+    vecc E, F2;
+    // Re F^-1(H F(mirror(w))) trimmed, H(i, j) on the expanded grid
+    auto filtered = [&](const vecd& w, int kind, auto H, vecd& outv) {
+        mirror(w, kind, E);
+        fftn(se, E, false);
+        for (int i = 0; i < nx; ++i)
+            for (int j = 0; j < nyE; ++j) E[(size_t)i * nyE + j] *= H(i, j);
+        fftn(se, E, true);
+        trim(E, outv);
+    };
+    auto source_matrix = [&](const SourceOp& op, int t, vecd& mat) {
+        mat.assign(N, 0.0);
+        for (size_t q = 0; q < op.idx.size(); ++q)
+            mat[op.idx[q]] = (op.signal.size() == 1 ? op.signal[0][t] : op.signal[q][t]) * op.scale[q];
+    };
+    auto apply_u_source = [&](int a, vecd& u, int t, int kind) {
+        const SourceOp& op = m.uOp[a];
+        if (!m.hasU[a] || t >= op.len()) return;
+        vecd mat;
+        source_matrix(op, t, mat);
+        if (umode == KW_SOURCE_DIRICHLET) {
+            for (size_t q = 0; q < op.idx.size(); ++q) u[op.idx[q]] = mat[op.idx[q]];
+        } else if (umode == KW_SOURCE_ADDITIVE_NO_CORRECTION) {
+            for (size_t i = 0; i < N; ++i) u[i] += mat[i];
+        } else {
+            vecd c;
+            filtered(mat, kind, [&](int i, int j) { return cd(skappa[(size_t)i * nyE + j], 0); }, c);
+            for (size_t i = 0; i < N; ++i) u[i] += c[i];
+        }
+    };
+    auto grads = [&](const vecd& p, vecd& gx, vecd& gy) {
+        mirror(p, 0, E);
+        fftn(se, E, false);
+        F2 = E;
+        for (int i = 0; i < nx; ++i)
+            for (int j = 0; j < nyE; ++j) {
+                const size_t k = (size_t)i * nyE + j;
+                E[k] *= ddxPos[i] * kappa[k];
+                F2[k] *= ddyPos[j] * kappa[k];
+            }
+        fftn(se, E, true);
+        fftn(se, F2, true);
+        trim(E, gx);
+        trim(F2, gy);
+    };
+    auto sg_rho = [&](int a) {   // dt / rho_sg along axis a (staggerDensity KSFO:799-806)
+        const bool map = d->density.len > 1;
+        vecd sg = map ? stagger_density(m.s, m.rho0, a) : m.rho0;
+        vecd r(N);
+        for (size_t i = 0; i < N; ++i) r[i] = dt / sg[i];
+        return r;
+    };
+    const vecd dtorX = sg_rho(0), dtorY = sg_rho(1);
+
+    vecd p(N, 0.0), ux(N, 0.0), uy(N, 0.0), rx(N, 0.0), ry(N, 0.0), gx, gy, duxdx, duydy, t1, t2, mat;
+    std::vector<vecd> pRec;
+    const int steps = max_steps >= 0 ? std::min(max_steps, m.nt) : m.nt;
+    auto tstart = std::chrono::steady_clock::now();
+    for (int t = 0; t < steps; ++t) {
+        grads(p, gx, gy);
+        for (size_t i = 0; i < N; ++i) {
+            const int xi = (int)(i / ny), yj = (int)(i % ny);
+            ux[i] = pmlXsg[xi] * (pmlXsg[xi] * ux[i] - dtorX[i] * gx[i]);
+            uy[i] = pmlYsg[yj] * (pmlYsg[yj] * uy[i] - dtorY[i] * gy[i]);
+        }
+        apply_u_source(0, ux, t, 0);
+        apply_u_source(1, uy, t, 1);
+        filtered(ux, 0, [&](int i, int j) { return ddxNeg[i] * kappa[(size_t)i * nyE + j]; }, duxdx);
+        {   // duydy = Re F^-1(kappa yShiftNeg (i ky F(HAHS(uy)) + F(HSHA(uy / r))))
+            vecd ur(N);
+            for (size_t i = 0; i < N; ++i) ur[i] = invYsg[i % ny] * uy[i];
+            mirror(uy, 1, E);
+            fftn(se, E, false);
+            mirror(ur, 2, F2);
+            fftn(se, F2, false);
+            for (int i = 0; i < nx; ++i)
+                for (int j = 0; j < nyE; ++j) {
+                    const size_t k = (size_t)i * nyE + j;
+                    E[k] = kappa[k] * yShNeg[j] * (I * kyE[j] * E[k] + F2[k]);
+                }
+            fftn(se, E, true);
+            trim(E, duydy);
+        }
+        for (size_t i = 0; i < N; ++i) {
+            const int xi = (int)(i / ny), yj = (int)(i % ny);
+            const double dtr = m.nonlinear ? dt * (2.0 * (rx[i] + ry[i]) + m.rho0[i]) : m.dtRho0[i];
+            rx[i] = pmlX[xi] * (pmlX[xi] * rx[i] - dtr * duxdx[i]);
+            ry[i] = pmlY[yj] * (pmlY[yj] * ry[i] - dtr * duydy[i]);
+        }
+        if (hasP && t < pOp.len()) {
+            source_matrix(pOp, t, mat);
+            if (pOp.mode == KW_SOURCE_DIRICHLET) {
+                for (size_t q = 0; q < pOp.idx.size(); ++q) { rx[pOp.idx[q]] = mat[pOp.idx[q]]; ry[pOp.idx[q]] = mat[pOp.idx[q]]; }
+            } else if (pOp.mode == KW_SOURCE_ADDITIVE_NO_CORRECTION) {
+                for (size_t i = 0; i < N; ++i) { rx[i] += mat[i]; ry[i] += mat[i]; }
+            } else {
+                filtered(mat, 0, [&](int i, int j) { return cd(skappa[(size_t)i * nyE + j], 0); }, t1);
+                for (size_t i = 0; i < N; ++i) { rx[i] += t1[i]; ry[i] += t1[i]; }
+            }
+        }
+        for (size_t i = 0; i < N; ++i) {
+            const double rt = rx[i] + ry[i];
+            double e = rt;
+            if (m.absorb) e += m.tau[i] * m.rho0[i] * (duxdx[i] + duydy[i]);
+            if (m.nonlinear) e += m.bona[i] * rt * rt / (2.0 * m.rho0[i]);
+            p[i] = m.c2[i] * e;
+        }
+        if (t == 0 && m.hasP0) {
+            p = m.p0f;
+            for (size_t i = 0; i < N; ++i) { rx[i] = m.p0f[i] / (2.0 * m.c2[i]); ry[i] = rx[i]; }
+            grads(p, gx, gy);
+            for (size_t i = 0; i < N; ++i) { ux[i] = dtorX[i] / 2.0 * gx[i]; uy[i] = dtorY[i] / 2.0 * gy[i]; }
+        }
+        if (m.haveSampler && m.recordP) {
+            vecd sp;
+            sample_field(m, p, sp);
+            pRec.push_back(sp);
+        }
+    }
+    auto* R = new kwref_result();
+    R->s = m.s; R->nt = m.nt; R->record = d->record; R->steps = steps;
+    R->loop_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - tstart).count();
+    R->fields.assign(KW_FIELD_COUNT, vecd());
+    R->present.assign(KW_FIELD_COUNT, 0);
+    R->nsensor = m.haveSampler ? m.nPts : 0;
+    R->fields[KW_FIELD_P_FINAL] = p;
+    R->present[KW_FIELD_P_FINAL] = 1;
+    if (!pRec.empty() && (d->record & KW_RECORD_P)) {
+        vecd series((size_t)m.nPts * pRec.size());
+        for (size_t tt = 0; tt < pRec.size(); ++tt)
+            for (int q = 0; q < m.nPts; ++q) series[(size_t)q * pRec.size() + tt] = pRec[tt][q];
+        R->fields[KW_FIELD_P] = series;
+        R->present[KW_FIELD_P] = 1;
+    }
+    *out = R;
+    return KW_OK;
+}
+
 extern "C" {
 
 const char* kwref_last_error(void) { return g_err.c_str(); }
@@ -802,13 +1023,15 @@ int kwref_smoothing_window(int dim, const int* n, double* out) {
 
 double kwref_db2neper(double alpha, double y) { return db2neper(alpha, y); }
 
-/* Run the simulation of `desc` in FP64. max_steps < 0 runs all nt steps; otherwise stops
- * after max_steps (used to time a bounded CPU sample). nthreads <= 0 uses every core. */
+/* Run the simulation of `desc` in FP64 (kspaceFirstOrderAS when desc->axisymmetric). max_steps < 0
+ * runs all nt steps; otherwise stops after max_steps (used to time a bounded CPU sample).
+ * nthreads <= 0 uses every core. */
 int kwref_run(const kw_sim_desc* d, int nthreads, int max_steps, kwref_result** out) {
     if (!d || !out) { g_err = "null argument"; return KW_ERR_INVALID; }
 #ifdef _OPENMP
     if (nthreads > 0) omp_set_num_threads(nthreads);
 #endif
+    if (d->axisymmetric) return run_as(d, max_steps, out);
     Model m;
     const int st0 = build_model(d, m);
     if (st0 != KW_OK) return st0;

@@ -62,7 +62,8 @@ def _dp(a):
 
 
 def run(builder, nthreads: int = 0, max_steps: int = -1):
-    """Run the oracle on a kwave.DescBuilder; returns (dict of float64 outputs, loop seconds)."""
+    """Run the oracle on a kwave.DescBuilder; returns (dict of float64 outputs, loop seconds)
+    (kspaceFirstOrderAS when the descriptor's axisymmetric flag is set)."""
     from kwave import abi
     from kwave.api import output_shape
     L = lib()

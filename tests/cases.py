@@ -11,6 +11,8 @@ from kwave import (AbsorptionMode, DescBuilder, DirectivityPattern, KWaveGrid, K
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 GOLDEN_CASES = ["1d_source_hetero", "2d_ivp", "2d_hetero_abs_nl", "2d_stokes_nc", "3d_hetero_src",
                 "2d_directivity_pressure", "2d_directivity_gradient"]
+# axisymmetric (kspaceFirstOrderAS) golden cases
+GOLDEN_AS_CASES = ["as_ivp", "as_add", "as_dir", "as_stokes", "as_nl", "as_uxs", "as_uys", "as_hetero"]
 
 
 def load_golden(name: str):
@@ -58,7 +60,7 @@ def builder_from_case(case) -> DescBuilder:
                                 smoothP0=bool(case.get("smooth_p0", True)),
                                 smoothC0=bool(case.get("smooth_c0", False)),
                                 smoothRho0=bool(case.get("smooth_rho0", False)))
-    return DescBuilder(grid, medium, source, sensor, options)
+    return DescBuilder(grid, medium, source, sensor, options, axisymmetric=bool(case.get("axisymmetric", 0)))
 
 
 def rel_l2(a, b) -> float:

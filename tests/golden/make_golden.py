@@ -436,12 +436,211 @@ def cases():
     return cs
 
 
+def simulate_as(case):
+    """kspaceFirstOrderAS (KSpaceFirstOrderAS.swift:19-309) in FP64 with numpy: x axial, y radial,
+    fields mirrored into a 4x radial expansion (p, ux: WSWA; uy: HAHS; uy / r: HSHA), one-sided
+    radial PML, uy / r divergence term on r = (j + 1/2) dy, Stokes absorption, B/A."""
+    nx, ny = case["shape"]
+    dx, dy = case["spacing"]
+    dt, nt = case["dt"], case["nt"]
+    shape = (nx, ny)
+    c0 = np.broadcast_to(np.asarray(case["c0"], dtype=np.float32).astype(float), shape).copy()
+    rho0 = np.broadcast_to(np.asarray(case["rho0"], dtype=np.float32).astype(float), shape).copy()
+    cref = c0.max()
+    nye = 4 * ny
+    kx, kye = kvec(nx, dx), kvec(nye, dy)
+    kmag = np.sqrt(kx[:, None] ** 2 + kye[None, :] ** 2)
+    arg = kmag * (cref * dt / 2)
+    with np.errstate(invalid="ignore", divide="ignore"):
+        kappa = np.where(arg == 0, 1.0, np.sin(arg) / arg)
+    skappa = np.cos(arg)
+    ddxp = (1j * kx * np.exp(1j * kx * dx / 2))[:, None]
+    ddxn = (1j * kx * np.exp(-1j * kx * dx / 2))[:, None]
+    ddyk = (1j * kye)[None, :]
+    ysp = np.exp(1j * kye * dy / 2)[None, :]
+    ysn = np.exp(-1j * kye * dy / 2)[None, :]
+    m, alpha = case["pml_size"], case.get("pml_alpha", 2.0)
+    pmlx = pml(nx, dx, dt, cref, m, alpha, False)[:, None]
+    pmlxs = pml(nx, dx, dt, cref, m, alpha, True)[:, None]
+
+    def pml_r(stag):
+        a = alpha * (cref / dy)
+        out = np.ones(ny)
+        for k in range(min(m, ny)):
+            x = k + 1.0
+            pos = (x + 0.5) / m if stag else x / m
+            out[ny - m + k] = math.exp(-a * dt / 2 * pos ** 4)
+        return out[None, :]
+    pmly, pmlys = pml_r(False), pml_r(True)
+    invr = (1.0 / ((np.arange(ny) + 0.5) * dy))[None, :]
+    c2 = c0 * c0
+    rmap = np.size(case["rho0"]) > 1
+
+    def sg(a):
+        if not rmap:
+            return rho0
+        r = np.moveaxis(rho0, a, 0)
+        return np.moveaxis(np.concatenate([0.5 * (r[:-1] + r[1:]), r[-1:]], axis=0), 0, a)
+    dtorx, dtory = dt / sg(0), dt / sg(1)
+    tau = None
+    if case.get("alpha_coeff") is not None and case.get("alpha_mode", NONE) != NONE:
+        tau = -2 * np.broadcast_to(np.asarray(case["alpha_coeff"], dtype=np.float32).astype(float), shape) \
+            * db2neper(1.0, 2.0) * c0
+    bona = None
+    if case.get("b_on_a") is not None:
+        b = np.broadcast_to(np.asarray(case["b_on_a"], dtype=np.float32).astype(float), shape)
+        bona = b if np.max(np.abs(b)) != 0 else None
+
+    def wswa(w):
+        tail = w[:, 1:][:, ::-1]
+        z = np.zeros((nx, 1))
+        return np.concatenate([w, z, -tail, -w, z, tail], axis=1)
+
+    def hahs(w):
+        f = w[:, ::-1]
+        return np.concatenate([w, f, -w, -f], axis=1)
+
+    def hsha(w):
+        f = w[:, ::-1]
+        return np.concatenate([w, -f, -w, f], axis=1)
+    F, IF = np.fft.fft2, np.fft.ifft2
+    src = case["source"]
+
+    def mk(mask, sig, scale):
+        if mask is None or sig is None:
+            return None
+        idx = np.flatnonzero(np.asarray(mask).reshape(-1) != 0)
+        if idx.size == 0:
+            return None
+        sig = np.asarray(sig, dtype=np.float32).astype(float)
+        sig = sig.reshape(1, -1) if sig.ndim <= 1 else sig
+        return idx, sig, scale(c0.reshape(-1)[idx])
+    pmode, umode = src.get("p_mode", ADDITIVE), src.get("u_mode", ADDITIVE)
+    psrc = mk(src.get("p_mask"), src.get("p"),
+              lambda c: 1 / (2 * c * c) if pmode == DIRICHLET else 2 * dt / (2 * c * dx))
+    uxs = mk(src.get("u_mask"), src.get("ux"), lambda c: np.ones_like(c) if umode == DIRICHLET else 2 * c * dt / dx)
+    uys = mk(src.get("u_mask"), src.get("uy"), lambda c: np.ones_like(c) if umode == DIRICHLET else 2 * c * dt / dy)
+
+    def mat_at(s_, t):
+        idx, sig, sc = s_
+        if t >= sig.shape[1]:
+            return None
+        v = (sig[0, t] if sig.shape[0] == 1 else sig[:, t]) * sc
+        b = np.zeros(nx * ny)
+        b[idx] = v
+        return b.reshape(shape), idx, v
+
+    def correct(mat, mir):
+        return np.real(IF(skappa * F(mir(mat))))[:, :ny]
+
+    def usrc(s_, u, t, mir):
+        if s_ is None:
+            return u
+        r = mat_at(s_, t)
+        if r is None:
+            return u
+        mat, idx, v = r
+        if umode == DIRICHLET:
+            u = u.reshape(-1).copy()
+            u[idx] = v
+            return u.reshape(shape)
+        if umode == ADDITIVE_NC:
+            return u + mat
+        return u + correct(mat, mir)
+
+    def grads(p):
+        pk = kappa * F(wswa(p))
+        return np.real(IF(ddxp * pk))[:, :ny], np.real(IF(ddyk * ysp * pk))[:, :ny]
+    p0 = None if src.get("p0") is None else np.asarray(src["p0"], dtype=np.float32).astype(float)
+    p = np.zeros(shape)
+    ux, uy, rx, ry = np.zeros(shape), np.zeros(shape), np.zeros(shape), np.zeros(shape)
+    sens = np.asarray(case["sensor_mask"], dtype=np.float32)
+    sidx = np.flatnonzero(sens.reshape(-1) != 0)
+    prec = []
+    for t in range(nt):
+        gx, gy = grads(p)
+        ux = pmlxs * (pmlxs * ux - dtorx * gx)
+        ux = usrc(uxs, ux, t, wswa)
+        uy = pmlys * (pmlys * uy - dtory * gy)
+        uy = usrc(uys, uy, t, hahs)
+        duxdx = np.real(IF(ddxn * kappa * F(wswa(ux))))[:, :ny]
+        uyk = ddyk * F(hahs(uy)) + F(hsha(invr * uy))
+        duydy = np.real(IF(kappa * ysn * uyk))[:, :ny]
+        if bona is not None:
+            dtr = dt * (2 * (rx + ry) + rho0)
+        else:
+            dtr = dt * rho0
+        rx = pmlx * (pmlx * rx - dtr * duxdx)
+        ry = pmly * (pmly * ry - dtr * duydy)
+        if psrc is not None:
+            r = mat_at(psrc, t)
+            if r is not None:
+                mat, idx, v = r
+                if pmode == DIRICHLET:
+                    rx, ry = rx.reshape(-1).copy(), ry.reshape(-1).copy()
+                    rx[idx] = v
+                    ry[idx] = v
+                    rx, ry = rx.reshape(shape), ry.reshape(shape)
+                elif pmode == ADDITIVE_NC:
+                    rx, ry = rx + mat, ry + mat
+                else:
+                    cm = correct(mat, wswa)
+                    rx, ry = rx + cm, ry + cm
+        rt = rx + ry
+        e = rt.copy()
+        if tau is not None:
+            e = e + tau * rho0 * (duxdx + duydy)
+        if bona is not None:
+            e = e + bona * rt * rt / (2 * rho0)
+        p = c2 * e
+        if t == 0 and p0 is not None:
+            p = p0.copy()
+            rx = p0 / (2 * c2)
+            ry = p0 / (2 * c2)
+            gx, gy = grads(p)
+            ux, uy = dtorx / 2 * gx, dtory / 2 * gy
+        prec.append(p.reshape(-1)[sidx])
+    return {"p": np.stack(prec, axis=1), "pFinal": p}
+
+
+def cases_as():
+    """Axisymmetric cases in the shapes of ParityAxisymmetricTests.swift: IVP, additive and
+    Dirichlet p sources, Stokes absorption, B/A, additive ux and uy sources."""
+    nx, ny = 48, 24
+    dx = 1e-4
+    dt = 0.3 * dx / 1500.0
+    base = dict(dim=2, shape=[nx, ny], spacing=[dx, dx], dt=dt, nt=60, pml_size=6, c0=np.float32(1500),
+                rho0=np.float32(1000), axisymmetric=1, smooth_p0=False, record=R["p"] | R["pFinal"])
+    mask = np.zeros((nx, ny), np.float32)
+    mask[30, 0:14] = 1
+    p0 = np.zeros((nx, ny), np.float32)
+    p0[20:25, 0:4] = 1.0
+    sm = np.zeros((nx, ny), np.float32)
+    sm[16, 0:3] = 1
+    sig = (toneBurst(1 / dt, 2e6, 2) * 1.0).astype(np.float32)
+    cs = {}
+    cs["as_ivp"] = dict(base, sensor_mask=mask, source=dict(p0=p0))
+    cs["as_add"] = dict(base, sensor_mask=mask, source=dict(p_mask=sm, p=sig, p_mode=ADDITIVE))
+    cs["as_dir"] = dict(base, sensor_mask=mask, source=dict(p_mask=sm, p=sig, p_mode=DIRICHLET))
+    cs["as_stokes"] = dict(base, sensor_mask=mask, alpha_coeff=np.float32(0.75), alpha_power=2.0, alpha_mode=STOKES,
+                           source=dict(p0=p0))
+    cs["as_nl"] = dict(base, sensor_mask=mask, b_on_a=np.float32(8.0), source=dict(p0=p0 * 3e6))
+    cs["as_uxs"] = dict(base, sensor_mask=mask, source=dict(u_mask=sm, ux=sig * 1e-3, u_mode=ADDITIVE))
+    cs["as_uys"] = dict(base, sensor_mask=mask, source=dict(u_mask=sm, uy=sig * 1e-3, u_mode=ADDITIVE))
+    rng = np.random.default_rng(20261203 + 40)
+    c = (1500 + 40 * rng.standard_normal((nx, ny))).astype(np.float32)
+    rho = (1000 + 30 * rng.standard_normal((nx, ny))).astype(np.float32)
+    cs["as_hetero"] = dict(base, sensor_mask=mask, c0=c, rho0=rho, dt=0.3 * dx / float(c.max()),
+                           source=dict(p0=p0, p_mask=sm, p=sig, p_mode=ADDITIVE))
+    return cs
+
+
 def main():
     only = set(sys.argv[1:])   # optional: regenerate only the named cases
-    for name, case in cases().items():
+    for name, case in list(cases().items()) + list(cases_as().items()):
         if only and name not in only:
             continue
-        out = simulate(case)
+        out = simulate_as(case) if case.get("axisymmetric") else simulate(case)
         flat = {}
         for k, v in case.items():
             if k == "source":

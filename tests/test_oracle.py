@@ -7,12 +7,12 @@ import numpy as np
 import pytest
 
 import oracle
-from cases import GOLDEN_CASES, builder_from_case, load_golden, rel_l2, rel_max
+from cases import GOLDEN_AS_CASES, GOLDEN_CASES, builder_from_case, load_golden, rel_l2, rel_max
 from kwave import (DescBuilder, KWaveGrid, KWaveMedium, KWaveSensor, KWaveSource, RecordField,
                    SimulationOptions, makeCircle, makeDisc, toneBurst)
 
 
-@pytest.mark.parametrize("name", GOLDEN_CASES)
+@pytest.mark.parametrize("name", GOLDEN_CASES + GOLDEN_AS_CASES)
 def test_oracle_matches_numpy_restatement(name):
     case, ref = load_golden(name)
     out, _ = oracle.run(builder_from_case(case))
