@@ -148,6 +148,10 @@ void Engine::build_plan(FFTPlanDev& pl, int n) {
 // one time step (KSFO:492-546)
 // ------------------------------------------------------------------------------------------
 void Engine::issue_step(bool first) {
+    if (as_mode_) {
+        issue_step_as(first);
+        return;
+    }
     const int D = dim_;
     const int sp1 = D == 1 ? 0 : 1;   // first output spectrum
 
@@ -907,8 +911,30 @@ void Engine::setup_sim(int s, const kw_sim_desc& d) {
 
 void Engine::create(const kw_sim_desc* descs, int n) {
     if (n <= 0) throw err(KW_ERR_INVALID, "no simulations");
-    for (int i = 0; i < n; ++i)
-        if (descs[i].axisymmetric) throw err(KW_ERR_UNSUPPORTED, "the axisymmetric solver is not available in this build");
+    // kspaceFirstOrderAS: one simulation, its preconditions (KSpaceFirstOrderAS.swift:35-38,87-95),
+    // p / pFinal recording only; a missing alphaPower means 2 there
+    kw_sim_desc as_desc;
+    bool as = false;
+    for (int i = 0; i < n; ++i) as = as || descs[i].axisymmetric;
+    if (as) {
+        if (n != 1) throw err(KW_ERR_UNSUPPORTED, "axisymmetric simulations run one at a time");
+        as_desc = descs[0];
+        if (as_desc.dim != 2) throw err(KW_ERR_INVALID, "axisymmetric solver requires a 2D grid (x axial, y radial)");
+        if (as_desc.nt <= 0) throw err(KW_ERR_INVALID, "call grid.makeTime(...) before running the solver");
+        if (!as_desc.p0 && !as_desc.p_mask && !as_desc.u_mask)
+            throw err(KW_ERR_INVALID, "axisymmetric solver requires source.p0 or a time-varying p/u source");
+        if (as_desc.alpha_coeff.data && as_desc.alpha_mode != KW_ABSORPTION_NONE) {
+            const double y = as_desc.alpha_mode == KW_ABSORPTION_STOKES ? 2.0
+                             : (std::isnan(as_desc.alpha_power) ? 2.0 : as_desc.alpha_power);
+            if (std::fabs(y - 2.0) >= 1e-10)
+                throw err(KW_ERR_INVALID, "axisymmetric absorption requires the Stokes model (alphaPower = 2)");
+            as_desc.alpha_mode = KW_ABSORPTION_STOKES;
+        }
+        as_desc.record &= (unsigned)(KW_RECORD_P | KW_RECORD_P_FINAL);
+        as_desc.directivity_angle = nullptr;
+        as_desc.axisymmetric = 0;
+        descs = &as_desc;
+    }
     check(cudaSetDevice(ctx_->device), "cudaSetDevice");
     sims_.resize(n);
     outs_.resize(n);
@@ -924,6 +950,7 @@ void Engine::create(const kw_sim_desc* descs, int n) {
     for (int i = 0; i < n; ++i) p0s[i] = sims_[i].p0s;
     d_p0s_ = (const float**)dalloc(sizeof(float*) * n);
     check(cudaMemcpyAsync(d_p0s_, p0s.data(), sizeof(float*) * n, cudaMemcpyHostToDevice, st()), "upload");
+    if (as) create_as_carrier();
     check(cudaStreamSynchronize(st()), "setup sync");
     reset();
 }

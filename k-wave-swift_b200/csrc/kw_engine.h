@@ -178,6 +178,13 @@ private:
     bool finalized_ = false;
     bool tape_mode_ = false;   // adjoint: steps are captured with the tape epilogues
     cudaStream_t st_override_ = nullptr;   // adjoint: the reverse sweep's own stream while it issues work
+    // axisymmetric solver (kw_axisym.cpp): sims_[0] is the [nx][ny] simulation, car_ / d_car_ the
+    // descriptor of its 4x radial expansion that the spectral jobs run on
+    bool as_mode_ = false;
+    SimHost car_;
+    SimDev* d_car_ = nullptr;
+    void create_as_carrier();
+    void issue_step_as(bool first);
     int finalized_t_ = -1;
     // finalised aggregate outputs per sim (device)
     struct Outs {

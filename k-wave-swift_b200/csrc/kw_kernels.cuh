@@ -72,6 +72,18 @@ void launch_row_c2r(cudaStream_t st, const SimDev* d_sims, const int* d_t, const
 void init_colop_attributes(int optin);
 void launch_colop(cudaStream_t st, const SimDev* d_sims, const int* d_t, const BlockWork* map, int nmap,
                   const ColJob& job, int n);
+// axisymmetric solver (kw_axisym.cu): radial mirror of an [nx][ny] field into the [nx][4 ny]
+// expansion (WSWA: p, ux; HAHS: uy; HSHA: uy / r with over_r), the trimmed updates, sources
+enum AsMirror { AS_WSWA = 0, AS_HAHS, AS_HSHA };
+void launch_as_mirror(cudaStream_t st, const SimDev* std_sim, const SimDev* car, long long n_exp, const float* src,
+                      float* dst, int kind, int over_r);
+void launch_as_vel(cudaStream_t st, const SimDev* std_sim, long long n, const float* g0, const float* g1, int nye, int init);
+void launch_as_den(cudaStream_t st, const SimDev* std_sim, long long n, const float* d0, const float* d1, const float* d2,
+                   int nye);
+void launch_as_eos(cudaStream_t st, const SimDev* std_sim, long long n);
+void launch_as_p0(cudaStream_t st, const SimDev* std_sim, long long n, const float* p0);
+void launch_as_src(cudaStream_t st, const SimDev* std_sim, const int* d_t, int nsrc, int target, float* buf);
+void launch_as_add(cudaStream_t st, const SimDev* std_sim, long long n, const float* g, int nye, float* f0, float* f1);
 // persistent, cp.async double-buffered register column passes for has_colop(n) lengths: in-place
 // forward / inverse, operator (with fan-out) and fan-in operator modes; same tiles as launch_colop
 // (colop_lines(n) consecutive columns of one plane)

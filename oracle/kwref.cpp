@@ -752,10 +752,16 @@ static void sample_field(const Model& m, const vecd& f, vecd& dst) {
  * ====================================================================================== */
 static int run_as(const kw_sim_desc* d, int max_steps, kwref_result** out) {
     if (d->dim != 2) { g_err = "axisymmetric solver requires a 2D grid (x axial, y radial)"; return KW_ERR_INVALID; }
+    kw_sim_desc da = *d;
+    if (da.alpha_coeff.data && da.alpha_mode != KW_ABSORPTION_NONE) {   // alphaPower ?? 2.0 (:89-93)
+        const double y = da.alpha_mode == KW_ABSORPTION_STOKES ? 2.0 : (std::isnan(da.alpha_power) ? 2.0 : da.alpha_power);
+        if (std::fabs(y - 2.0) >= 1e-10) { g_err = "axisymmetric absorption requires the Stokes model (alphaPower = 2)"; return KW_ERR_INVALID; }
+        da.alpha_mode = KW_ABSORPTION_STOKES;
+    }
+    d = &da;
     Model m;   // parsing of the medium, sources (signals, scales), p0, sensor (KSFO rules)
     const int st0 = build_model(d, m);
     if (st0 != KW_OK) return st0;
-    if (m.absorb && !m.stokes) { g_err = "axisymmetric absorption requires the Stokes model (alphaPower = 2)"; return KW_ERR_INVALID; }
     const int nx = m.s.n[0], ny = m.s.n[1], nyE = 4 * ny;
     const size_t N = m.N, NE = (size_t)nx * nyE;
     const double dx = m.s.d[0], dy = m.s.d[1], dt = m.dt;
