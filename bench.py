@@ -330,7 +330,10 @@ def run_adjoint(args) -> None:
     rep = replicas.init("nccl")   # one replica per GPU; no collective on the data path
     world, rank, local = rep.world, rep.rank, rep.local
     three_d = args.workload == ADJ3
-    bp, bt = workloads.adjoint3d() if three_d else workloads.adjoint2d()
+    if args.adjoint_nt:   # a shorter run of the same configuration (profiling captures)
+        bp, bt = workloads.adjoint3d(384, args.adjoint_nt) if three_d else workloads.adjoint2d(512, args.adjoint_nt)
+    else:
+        bp, bt = workloads.adjoint3d() if three_d else workloads.adjoint2d()
     nt, npts = bp.grid.nt, bp.grid.totalGridPoints
     ctx = Context(local)
     stream = torch.cuda.Stream()
@@ -539,6 +542,8 @@ def main() -> None:
     ap.add_argument("--cpu-steps", type=int, default=1)
     ap.add_argument("--ref-steps", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--adjoint-nt", type=int, default=0,
+                    help="adjoint workloads: time steps (default: the configuration's; shorter runs for profiling)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
