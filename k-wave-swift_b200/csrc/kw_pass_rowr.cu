@@ -28,8 +28,9 @@ namespace kw {
 // take more registers and the 384-point rows ran 1.4x slower with it).
 template <int M, int EPI, bool TAPE>
 constexpr int rowr_minb() {
-    if (EPI == EPI_ADJ_EOS) return 2;   // left alone it takes 152 registers at M = 192: one CTA per SM
-    return (M <= 128 && !TAPE && EPI != EPI_ADD_RHO) ? 3 : 0;
+    // left alone these take 129-152 registers at some lengths (one CTA per SM)
+    if (EPI == EPI_ADJ_EOS || EPI == EPI_ADD_RHO || TAPE || M >= 768) return 2;
+    return M <= 128 ? 3 : 0;
 }
 
 template <int M>
