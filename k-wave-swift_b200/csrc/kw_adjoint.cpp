@@ -34,6 +34,7 @@ void Engine::adjoint(const kw_sim_desc& din, kw_adjoint_desc& a) {
     if (din.p_mask && din.p.data && din.p_mode != KW_SOURCE_ADDITIVE)
         throw err(KW_ERR_UNSUPPORTED, "adjoint: only the k-space corrected additive pressure source is supported");
     if (din.directivity_angle) throw err(KW_ERR_UNSUPPORTED, "adjoint: directivity is not supported");
+    if (din.axisymmetric) throw err(KW_ERR_UNSUPPORTED, "adjoint: the axisymmetric solver is not supported");
     if ((din.smooth_c0 && din.sound_speed.len > 1) || (din.smooth_rho0 && din.density.len > 1))
         throw err(KW_ERR_UNSUPPORTED, "adjoint: smoothC0 / smoothRho0 maps are not supported");
     if (a.grad_p0 && !din.p0) throw err(KW_ERR_INVALID, "adjoint: grad_p0 needs source.p0");
@@ -167,7 +168,10 @@ void Engine::adjoint(const kw_sim_desc& din, kw_adjoint_desc& a) {
     check(cudaEventCreate(&e2), "event");
 
     // ---- 1. forward ----
-    set_tape_mode(store_all);
+    // The last segment (every step with store-all) fills the tape as it runs, so the reverse sweep
+    // starts with its reverse instead of recomputing it.
+    const int t_last = store_all ? 0 : (nck - 1) * K;
+    set_tape_mode(t_last == 0);
     reset();
     check(cudaEventRecord(e0, st()), "event");
     for (int t = 0; t < nt; ++t) {
@@ -177,8 +181,9 @@ void Engine::adjoint(const kw_sim_desc& din, kw_adjoint_desc& a) {
             if (t == 0) zero(ckf(c, 2 * D + 2));
             else cpy(ckf(c, 2 * D + 2), v.rho_sum);
         }
+        if (t == t_last && !tape_mode_) set_tape_mode(true);
         step(1);
-        if (store_all && t == 0) tape_copy();
+        if (tape_mode_ && t == 0) tape_copy();   // the t = 0 override follows the step's epilogues
         if (ck_step) {
             const int c = t / K;
             for (int b = 0; b < D; ++b) { cpy(ckf(c, b), v.u[b]); cpy(ckf(c, D + b), v.rho[b]); }
@@ -369,24 +374,27 @@ void Engine::adjoint(const kw_sim_desc& din, kw_adjoint_desc& a) {
             auto slot_free = [&](int t) {
                 if (overlap) check(cudaStreamWaitEvent(fs, ev_free[slot_of(t)], 0), "wait");
             };
-            slot_free(t0);
-            // restore the state after step t0 and rerun the segment, storing each step
-            for (int b = 0; b < D; ++b) { cpy(v.u[b], ckf(c, b)); cpy(v.rho[b], ckf(c, D + b)); }
-            cpy(v.rho_sum, ckf(c, 2 * D));
-            cpy(v.p, ckf(c, 2 * D + 1));
-            if (stokes) cpy(v.div_term, ckf(c, 2 * D + 3));
-            if (nonlin || disp) {   // d_a(t0) = D-_a u_a(t0), A2(S(t0)) of the restored state into its tape slot
-                launch_set_step(st(), d_t_, t0);
-                launch_adj_views(st(), d_sims_, d_table, t0);
-                if (nonlin) job_in(FS_U, ADJ_DDP, D, deriv(AO_DNEG), EPI_STORE, 0, "adj_du");
-                if (disp) job_in(FS_RHO_SUM, ADJ_Q2, 1, radial(RT_NU2), EPI_STORE, 0, "adj_q2");
-            }
-            launch_set_step(st(), d_t_, t0 + 1);
-            t_ = t0 + 1;
-            tape_copy();
-            for (int t = t0 + 1; t < t1; ++t) {
-                slot_free(t);
-                step(1);
+            // the last segment's tape is still in place from the forward
+            if (c < nck - 1) {
+                slot_free(t0);
+                // restore the state after step t0 and rerun the segment, storing each step
+                for (int b = 0; b < D; ++b) { cpy(v.u[b], ckf(c, b)); cpy(v.rho[b], ckf(c, D + b)); }
+                cpy(v.rho_sum, ckf(c, 2 * D));
+                cpy(v.p, ckf(c, 2 * D + 1));
+                if (stokes) cpy(v.div_term, ckf(c, 2 * D + 3));
+                if (nonlin || disp) {   // d_a(t0) = D-_a u_a(t0), A2(S(t0)) of the restored state into its tape slot
+                    launch_set_step(st(), d_t_, t0);
+                    launch_adj_views(st(), d_sims_, d_table, t0);
+                    if (nonlin) job_in(FS_U, ADJ_DDP, D, deriv(AO_DNEG), EPI_STORE, 0, "adj_du");
+                    if (disp) job_in(FS_RHO_SUM, ADJ_Q2, 1, radial(RT_NU2), EPI_STORE, 0, "adj_q2");
+                }
+                launch_set_step(st(), d_t_, t0 + 1);
+                t_ = t0 + 1;
+                tape_copy();
+                for (int t = t0 + 1; t < t1; ++t) {
+                    slot_free(t);
+                    step(1);
+                }
             }
             if (overlap) {
                 check(cudaEventRecord(ev_rec, fs), "event");

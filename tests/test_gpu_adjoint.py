@@ -81,8 +81,8 @@ def test_fan_in_sum_matches_per_component_sum(shape, kw, cola, monkeypatch):
 @pytest.mark.parametrize("shape,kw", [((40, 36), dict(absorb="powerlaw", nonlinear=True, nt=45)),
                                       ((16, 20, 32), dict(absorb="stokes", nonlinear=True, nt=30))])
 def test_overlapped_reverse_sweep_matches_sequential(shape, kw, monkeypatch):
-    # segment c + 1 reversed on a second stream while segment c is recomputed (two tape banks)
-    # gives the same gradient as running them one after the other
+    # segment c + 1 reversed on a second stream while segment c is recomputed (one tape bank whose
+    # slots alternate direction) gives the same gradient as running them one after the other
     c, p0, data, kw = problem(shape, **kw)
     monkeypatch.setenv("KW_ADJOINT_OVERLAP", "1")
     r1 = gpu_adjoint(shape, c, p0, data, kw, policy=abi.KW_CHECKPOINT_INTERVAL, interval=6)
@@ -114,6 +114,11 @@ def test_adjoint_rejects_unsupported():
     c, p0, data, kw = problem(shape, absorb="none")
     b = builder(shape, c, p0, **kw)
     b.desc.p_mode = 0   # Dirichlet pressure source
+    with pytest.raises(KWaveError) as e:
+        Context.default().adjoint(b, data)
+    assert e.value.status == abi.KW_ERR_UNSUPPORTED
+    b = builder(shape, c, p0, **kw)
+    b.desc.axisymmetric = 1
     with pytest.raises(KWaveError) as e:
         Context.default().adjoint(b, data)
     assert e.value.status == abi.KW_ERR_UNSUPPORTED
