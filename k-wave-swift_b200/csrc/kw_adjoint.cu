@@ -90,52 +90,65 @@ __global__ void k_adj_begin(SimDev* __restrict__ sims, int* __restrict__ d_t, co
     }
 }
 
-__global__ void k_adj_eos(const SimDev* __restrict__ sims, AdjStepArgs A, int* __restrict__ d_rev) {
+// Every input is loaded before the first store: the stores may alias the loads as far as the
+// compiler knows, and interleaving them would serialise the loads.
+__global__ void __launch_bounds__(256, 4) k_adj_eos(const SimDev* __restrict__ sims, AdjStepArgs A, int* __restrict__ d_rev) {
     const SimDev& S = sims[0];
     const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i == 0) *d_rev -= 1;   // every reader of this step's *d_rev (k_adj_begin) has finished
     if (i >= S.N) return;
     const int D = S.dim;
-    const float c2 = S.c2.at(i);
+    const float c2 = S.c2.at(i), lp = A.lam_p[i], sv = S.adj[ADJ_STP][i], r0 = S.rho0.at(i), pv = S.adj[ADJ_PTP][i];
+    float tau = 0.f, divp = 0.f, eta = 0.f, q2 = 0.f, bona = 0.f, a1 = 0.f, a2 = 0.f, spv = 0.f;
+    if (S.absorb == 1) { tau = S.tau.at(i); divp = S.adj[ADJ_DIVP][i]; }
+    if (S.absorb >= 2) a1 = A.a1[i];
+    if (S.absorb == 3) { eta = S.eta.at(i); q2 = S.adj[ADJ_Q2][i]; a2 = A.a2[i]; }
+    if (S.nonlinear) { bona = S.bona.at(i); spv = S.adj[ADJ_SPRP][i]; }
+    float lr[kMaxComp], dd[kMaxComp], pm[kMaxComp];
+#pragma unroll
+    for (int a = 0; a < kMaxComp; ++a) {
+        if (a >= D) break;
+        lr[a] = A.lam_r[a][i];
+        if (S.nonlinear) dd[a] = S.adj[ADJ_DDP + a][i];
+        pm[a] = __ldg(S.ax[a].pml + layout_coord(S, i, a));
+    }
+    double gcv = A.gc[i];
     const float c = sqrtf(c2);
-    const float lp = A.lam_p[i];
-    const float sv = S.adj[ADJ_STP][i];
-    const float r0 = S.rho0.at(i);
-    const float pv = S.adj[ADJ_PTP][i];
     double dpdc = 2.0 * (double)pv / c;
-    if (S.absorb == 1) dpdc += (double)c * S.tau.at(i) * S.adj[ADJ_DIVP][i];
+    if (S.absorb == 1) dpdc += (double)c * tau * divp;
     if (S.absorb >= 2) {
         // (y-1) tau A1(div) - y eta A2(S) = (y-1) E - eta A2(S), E = tau A1(div) - eta A2(S) = p / c^2 - S - B/A S^2 / (2 rho0)
         double E = (double)pv / c2 - sv;
-        if (S.nonlinear) E -= (double)S.bona.at(i) * sv * sv / (2.0 * r0);
+        if (S.nonlinear) E -= (double)bona * sv * sv / (2.0 * r0);
         double term = (double)(A.y - 1.f) * E;
-        if (S.absorb == 3) term -= (double)S.eta.at(i) * S.adj[ADJ_Q2][i];
+        if (S.absorb == 3) term -= (double)eta * q2;
         dpdc += (double)c * term;
     }
-    A.gc[i] += (double)lp * dpdc;
+    gcv += (double)lp * dpdc;
     const float lE = c2 * lp;
     float lS = lE;
-    if (S.nonlinear) lS += lE * S.bona.at(i) * sv / r0;
-    if (S.absorb == 3) lS -= A.a2[i];
+    if (S.nonlinear) lS += lE * bona * sv / r0;
+    if (S.absorb == 3) lS -= a2;
     float ldiv = 0.f;
-    if (S.absorb == 1) ldiv = S.tau.at(i) * lE;
-    else if (S.absorb >= 2) ldiv = A.a1[i];
-    const float nl = S.nonlinear ? (2.f * S.adj[ADJ_SPRP][i] + r0) / r0 : 1.f;
+    if (S.absorb == 1) ldiv = tau * lE;
+    else if (S.absorb >= 2) ldiv = a1;
+    const float nl = S.nonlinear ? (2.f * spv + r0) / r0 : 1.f;
     const float dtr = S.dt * r0;
-    float lam[kMaxComp], pm[kMaxComp];
+    float lam[kMaxComp], w[kMaxComp];
     float lsprev = 0.f, sig = 0.f;
 #pragma unroll
     for (int a = 0; a < kMaxComp; ++a) {
         if (a >= D) break;
-        pm[a] = __ldg(S.ax[a].pml + layout_coord(S, i, a));
-        lam[a] = A.lam_r[a][i] + lS;
-        A.w[a][i] = r0 * ldiv - pm[a] * dtr * nl * lam[a];
-        if (S.nonlinear) lsprev += -2.f * S.dt * pm[a] * S.adj[ADJ_DDP + a][i] * lam[a];
+        lam[a] = lr[a] + lS;
+        w[a] = r0 * ldiv - pm[a] * dtr * nl * lam[a];
+        if (S.nonlinear) lsprev += -2.f * S.dt * pm[a] * dd[a] * lam[a];
         sig += lam[a] * S.ax[a].inv_d;
     }
+    A.gc[i] = gcv;
 #pragma unroll
     for (int a = 0; a < kMaxComp; ++a) {
         if (a >= D) break;
+        A.w[a][i] = w[a];
         A.lam_r[a][i] = pm[a] * pm[a] * lam[a] + lsprev;
     }
     if (A.sig) A.sig[i] = sig;

@@ -304,7 +304,18 @@ __global__ void __launch_bounds__(256, rowr_minb<M, EPI, TAPE>()) k_rowr_c2r(con
                 st_state(w, e, wo);
             }
         } else if constexpr (EPI == EPI_ADJ_SUM) {
-            // lambda_p = sum_a d_a and the next reverse step's absorption inputs
+            // lambda_p = sum_a d_a and the next reverse step's absorption inputs (the medium of the
+            // MB pairs is loaded before the first store, which the compiler may not reorder)
+            float2 c2[MB], tau[MB], eta[MB];
+            if (S.absorb >= 2) {
+#pragma unroll
+                for (int b = 0; b < MB; ++b) {
+                    const long long e = rbase + 2 * (t + T * (m0 + b));
+                    c2[b] = ld_medium(S.c2, e);
+                    tau[b] = ld_medium(S.tau, e);
+                    if (S.absorb == 3) eta[b] = ld_medium(S.eta, e);
+                }
+            }
 #pragma unroll
             for (int b = 0; b < MB; ++b) {
                 const int m = m0 + b;
@@ -317,12 +328,9 @@ __global__ void __launch_bounds__(256, rowr_minb<M, EPI, TAPE>()) k_rowr_c2r(con
                 }
                 st_state(S.adj[ADJ_LP], e, s2);
                 if (S.absorb >= 2) {
-                    const float2 c2 = ld_medium(S.c2, e), tau = ld_medium(S.tau, e);
-                    st_state(S.adj[ADJ_X1], e, make_float2(tau.x * c2.x * s2.x, tau.y * c2.y * s2.y));
-                    if (S.absorb == 3) {
-                        const float2 eta = ld_medium(S.eta, e);
-                        st_state(S.adj[ADJ_X2], e, make_float2(eta.x * c2.x * s2.x, eta.y * c2.y * s2.y));
-                    }
+                    st_state(S.adj[ADJ_X1], e, make_float2(tau[b].x * c2[b].x * s2.x, tau[b].y * c2[b].y * s2.y));
+                    if (S.absorb == 3)
+                        st_state(S.adj[ADJ_X2], e, make_float2(eta[b].x * c2[b].x * s2.x, eta[b].y * c2[b].y * s2.y));
                 }
             }
         } else if constexpr (EPI == EPI_ADJ_EOS) {
