@@ -82,6 +82,7 @@ __device__ __forceinline__ float2 ld_medium(const FieldOrScalar& f, long long e)
     return f.ptr ? __ldg(reinterpret_cast<const float2*>(f.ptr + e)) : make_float2(f.s, f.s);
 }
 __device__ __forceinline__ float& half(float2& v, int h) { return h ? v.y : v.x; }
+__device__ __forceinline__ float2 ld_ro(const float* p, long long e) { return __ldg(reinterpret_cast<const float2*>(p + e)); }
 
 template <int M, int EPI, bool TAPE = false>
 __global__ void __launch_bounds__(256, rowr_minb<M, EPI, TAPE>()) k_rowr_c2r(const SimDev* __restrict__ sims, const int* __restrict__ d_t,
@@ -348,22 +349,24 @@ __global__ void __launch_bounds__(256, rowr_minb<M, EPI, TAPE>()) k_rowr_c2r(con
                 const int m = m0 + b;
                 const int n = t + T * m;
                 const long long e = rbase + 2 * n;
-                const float2 lp = ld_state(S.adj[ADJ_LP], e), pv = ld_state(S.adj[ADJ_PTP], e), sv = ld_state(S.adj[ADJ_STP], e);
+                // lambda_p and the tape are read-only here: loaded through the non-coherent path, so
+                // the compiler may issue them ahead of the previous pair's stores
+                const float2 lp = ld_ro(S.adj[ADJ_LP], e), pv = ld_ro(S.adj[ADJ_PTP], e), sv = ld_ro(S.adj[ADJ_STP], e);
                 const float2 c2 = ld_medium(S.c2, e), r0 = ld_medium(S.rho0, e), tau = ld_medium(S.tau, e);
                 float2 eta = make_float2(0.f, 0.f), bona = eta, spv = eta;
                 if (S.absorb == 3) eta = ld_medium(S.eta, e);
-                if (S.nonlinear) { bona = ld_medium(S.bona, e); spv = ld_state(S.adj[ADJ_SPRP], e); }
+                if (S.nonlinear) { bona = ld_medium(S.bona, e); spv = ld_ro(S.adj[ADJ_SPRP], e); }
                 float2 lr[kMaxComp], dd[kMaxComp];
 #pragma unroll
                 for (int a = 0; a < kMaxComp; ++a)
                     if (a < D) {
                         lr[a] = ld_state(S.adj[ADJ_LR + a], e);
-                        if (S.nonlinear) dd[a] = ld_state(S.adj[ADJ_DDP + a], e);
+                        if (S.nonlinear) dd[a] = ld_ro(S.adj[ADJ_DDP + a], e);
                     }
                 const float2 pmr = row_pair(S.ax[D - 1].pml, n);
                 const float2 a1 = dpair(0, m);
                 float2 a2 = make_float2(0.f, 0.f), q2 = a2;
-                if (S.absorb == 3) { a2 = dpair(1, m); q2 = ld_state(S.adj[ADJ_Q2], e); }
+                if (S.absorb == 3) { a2 = dpair(1, m); q2 = ld_ro(S.adj[ADJ_Q2], e); }
                 double2 gcv = *reinterpret_cast<const double2*>(S.adj_gc + e);
                 float2 lro[kMaxComp], wo[kMaxComp], sg2;
 #pragma unroll
