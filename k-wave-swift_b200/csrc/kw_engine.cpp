@@ -11,6 +11,7 @@
 #include <cmath>
 #include <cstring>
 #include <limits>
+#include <thread>
 
 namespace kw {
 
@@ -390,6 +391,27 @@ void Engine::capture_graph() {
 // ------------------------------------------------------------------------------------------
 // setup of one simulation
 // ------------------------------------------------------------------------------------------
+// fn(i) for i in [0, n) on the host's cores: the per-point setup (medium-derived fields, the
+// radial operator tables) is a pure function of the index, so the split changes no value
+template <typename F>
+static void parallel_for(long long n, F&& fn) {
+    const long long nt = std::min<long long>(std::max(1u, std::thread::hardware_concurrency()), 32);
+    if (n < (1LL << 16) || nt == 1) {
+        for (long long i = 0; i < n; ++i) fn(i);
+        return;
+    }
+    std::vector<std::thread> pool;
+    const long long chunk = (n + nt - 1) / nt;
+    for (long long k = 0; k < nt; ++k) {
+        const long long lo = k * chunk, hi = std::min(n, lo + chunk);
+        if (lo >= hi) break;
+        pool.emplace_back([lo, hi, &fn] {
+            for (long long i = lo; i < hi; ++i) fn(i);
+        });
+    }
+    for (auto& t : pool) t.join();
+}
+
 static std::vector<int> flat_nonzero(const float* m, long long N) {
     std::vector<int> r;
     for (long long i = 0; i < N; ++i)
@@ -548,18 +570,19 @@ void Engine::setup_sim(int s, const kw_sim_desc& d) {
             return interp(std::sqrt(r2));
         };
         std::vector<float> tab((size_t)h.Ns, 0.f);
-        for (int ia = 0; ia < h.A; ++ia)
-            for (int ib = 0; ib < h.B; ++ib)
-                for (int kc = 0; kc < h.Ch; ++kc) {
-                    int lay[3] = {ia, ib, kc}, ln[3] = {h.A, h.B, h.C};
-                    int m[3], mm[3];
-                    for (int a = 0; a < h.dim; ++a) {
-                        const int L = a + 3 - h.dim;
-                        m[a] = lay[L];
-                        mm[a] = (ln[L] - lay[L]) % ln[L];
-                    }
-                    tab[((size_t)ia * h.B + ib) * h.Cp + kc] = (float)(0.5 * (W(m) + W(mm)));
-                }
+        parallel_for((long long)h.A * h.B * h.Ch, [&](long long q) {
+            const int kc = (int)(q % h.Ch);
+            const long long r = q / h.Ch;
+            const int ib = (int)(r % h.B), ia = (int)(r / h.B);
+            int lay[3] = {ia, ib, kc}, ln[3] = {h.A, h.B, h.C};
+            int m[3], mm[3];
+            for (int a = 0; a < h.dim; ++a) {
+                const int L = a + 3 - h.dim;
+                m[a] = lay[L];
+                mm[a] = (ln[L] - lay[L]) % ln[L];
+            }
+            tab[((size_t)ia * h.B + ib) * h.Cp + kc] = (float)(0.5 * (W(m) + W(mm)));
+        });
         v.radial[RT_WINDOW] = upload(tab);
         build_tensor_maps(h, v);   // the smoothing jobs below run the TMA-fed column pass
     }
@@ -620,7 +643,7 @@ void Engine::setup_sim(int s, const kw_sim_desc& d) {
         FieldOrScalar r{nullptr, 0.f};
         if (!map) { r.s = (float)f(0); return r; }
         std::vector<float> tmp(N);
-        for (long long i = 0; i < N; ++i) tmp[i] = (float)f(i);
+        parallel_for(N, [&](long long i) { tmp[i] = (float)f(i); });
         r.ptr = upload(tmp);
         return r;
     };
@@ -761,19 +784,21 @@ void Engine::setup_sim(int s, const kw_sim_desc& d) {
         if (need_skappa) skap.assign(Ns, 0.f);
         if (v.absorb >= 2) { nu1.assign(Ns, 0.f); if (v.absorb == 3) nu2.assign(Ns, 0.f); }
         const double half = cref * dt / 2.0;
-        for (int ia = 0; ia < h.A; ++ia)
-            for (int ib = 0; ib < h.B; ++ib)
-                for (int kc = 0; kc < h.Ch; ++kc) {
-                    const size_t i = ((size_t)ia * h.B + ib) * h.Cp + kc;
-                    const double k = std::sqrt(kA[ia] * kA[ia] + kB[ib] * kB[ib] + kC[kc] * kC[kc]);
-                    const double arg = k * half;
-                    kap[i] = (float)(arg == 0.0 ? 1.0 : std::sin(arg) / arg);
-                    if (need_skappa) skap[i] = (float)std::cos(arg);
-                    if (v.absorb >= 2) {
-                        nu1[i] = (float)(k == 0.0 ? 0.0 : std::pow(k, y - 2.0));
-                        if (v.absorb == 3) nu2[i] = (float)(k == 0.0 ? 0.0 : std::pow(k, y - 1.0));
-                    }
-                }
+        const int absorb = v.absorb;
+        parallel_for((long long)h.A * h.B * h.Ch, [&](long long q) {
+            const int kc = (int)(q % h.Ch);
+            const long long r = q / h.Ch;
+            const int ib = (int)(r % h.B), ia = (int)(r / h.B);
+            const size_t i = ((size_t)ia * h.B + ib) * h.Cp + kc;
+            const double k = std::sqrt(kA[ia] * kA[ia] + kB[ib] * kB[ib] + kC[kc] * kC[kc]);
+            const double arg = k * half;
+            kap[i] = (float)(arg == 0.0 ? 1.0 : std::sin(arg) / arg);
+            if (need_skappa) skap[i] = (float)std::cos(arg);
+            if (absorb >= 2) {
+                nu1[i] = (float)(k == 0.0 ? 0.0 : std::pow(k, y - 2.0));
+                if (absorb == 3) nu2[i] = (float)(k == 0.0 ? 0.0 : std::pow(k, y - 1.0));
+            }
+        });
         v.radial[RT_KAPPA] = upload(kap);
         if (need_skappa) v.radial[RT_SKAPPA] = upload(skap);
         if (v.absorb >= 2) {
