@@ -6,12 +6,12 @@
 // KSFO:492-546: velocity update, velocity sources, density update, pressure sources, equation of
 // state, t = 0 initial-pressure override, sensor sampling.
 #include "kw_engine.h"
+#include "kw_host.h"
 
 #include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <limits>
-#include <thread>
 
 namespace kw {
 
@@ -391,27 +391,6 @@ void Engine::capture_graph() {
 // ------------------------------------------------------------------------------------------
 // setup of one simulation
 // ------------------------------------------------------------------------------------------
-// fn(i) for i in [0, n) on the host's cores: the per-point setup (medium-derived fields, the
-// radial operator tables) is a pure function of the index, so the split changes no value
-template <typename F>
-static void parallel_for(long long n, F&& fn) {
-    const long long nt = std::min<long long>(std::max(1u, std::thread::hardware_concurrency()), 32);
-    if (n < (1LL << 16) || nt == 1) {
-        for (long long i = 0; i < n; ++i) fn(i);
-        return;
-    }
-    std::vector<std::thread> pool;
-    const long long chunk = (n + nt - 1) / nt;
-    for (long long k = 0; k < nt; ++k) {
-        const long long lo = k * chunk, hi = std::min(n, lo + chunk);
-        if (lo >= hi) break;
-        pool.emplace_back([lo, hi, &fn] {
-            for (long long i = lo; i < hi; ++i) fn(i);
-        });
-    }
-    for (auto& t : pool) t.join();
-}
-
 static std::vector<int> flat_nonzero(const float* m, long long N) {
     std::vector<int> r;
     for (long long i = 0; i < N; ++i)
@@ -1120,8 +1099,7 @@ void Engine::get_output(int i, int f, float* dst, size_t count) {
         std::vector<float> tmp((size_t)T * np);
         d2h(dev, tmp.data(), tmp.size());
         check(cudaStreamSynchronize(st()), "sync");
-        for (size_t q = 0; q < np; ++q)
-            for (int t = 0; t < T; ++t) dst[q * T + t] = tmp[(size_t)t * np + q];
+        transpose_series(tmp.data(), dst, (size_t)T, np);
     };
     auto rms = [&](const float* ss) {
         std::vector<float> tmp(np);
