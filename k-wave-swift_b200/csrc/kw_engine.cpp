@@ -391,13 +391,6 @@ void Engine::capture_graph() {
 // ------------------------------------------------------------------------------------------
 // setup of one simulation
 // ------------------------------------------------------------------------------------------
-static std::vector<int> flat_nonzero(const float* m, long long N) {
-    std::vector<int> r;
-    for (long long i = 0; i < N; ++i)
-        if (m[i] != 0.0f) r.push_back((int)i);
-    return r;
-}
-
 void Engine::smooth_field(int s, float* field) {
     // smooth(..., restore_max): Re F^-1(W F(f)) * max|f| / max|out| (Filter/Filters.swift:273-347).
     // The window is applied as its Hermitian part (W(k) + W(-k))/2, which gives exactly the real

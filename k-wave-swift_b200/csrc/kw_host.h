@@ -48,4 +48,26 @@ inline void transpose_series(const float* src, float* dst, size_t T, size_t np) 
     }, min_parallel);
 }
 
+// Ascending flat indices of the non-zero entries of a mask (flatNonzeroIndices, KSFO:778-782):
+// the order of sensor points and source rows. Chunks are counted on the host's cores, then each
+// chunk writes its indices at its offset, so the result equals the sequential scan.
+inline std::vector<int> flat_nonzero(const float* m, long long n) {
+    constexpr long long CH = 1LL << 18;
+    const long long nch = (n + CH - 1) / CH;
+    std::vector<long long> cnt((size_t)nch + 1, 0);
+    parallel_for(nch, [&](long long c) {
+        long long k = 0;
+        for (long long i = c * CH, e = std::min(n, i + CH); i < e; ++i) k += m[i] != 0.0f;
+        cnt[(size_t)c + 1] = k;
+    }, 2);
+    for (long long c = 0; c < nch; ++c) cnt[(size_t)c + 1] += cnt[(size_t)c];
+    std::vector<int> r((size_t)cnt[(size_t)nch]);
+    parallel_for(nch, [&](long long c) {
+        long long o = cnt[(size_t)c];
+        for (long long i = c * CH, e = std::min(n, i + CH); i < e; ++i)
+            if (m[i] != 0.0f) r[(size_t)o++] = (int)i;
+    }, 2);
+    return r;
+}
+
 }  // namespace kw

@@ -1,7 +1,8 @@
 // Host-side helpers of the engine (k-wave-swift_b200/csrc/kw_host.h), checked without a GPU:
-// parallel_for visits every index once, and transpose_series turns the device's [T][np] sensor
-// rows into the [np][T] output exactly as the element-by-element loop does, on the serial
-// (small) and threaded (large) paths and for sensor counts that are not multiples of the block.
+// parallel_for visits every index once; flat_nonzero equals the sequential mask scan; and
+// transpose_series turns the device's [T][np] sensor rows into the [np][T] output exactly as the
+// element-by-element loop does, on the serial (small) and threaded (large) paths and for sensor
+// counts that are not multiples of the block.
 #include "kw_host.h"
 
 #include <cstdio>
@@ -30,6 +31,20 @@ int main() {
                 std::printf("parallel_for coverage wrong for n=%lld\n", n);
                 return 1;
             }
+    }
+    // flat_nonzero: chunked counts + offsets give the sequential scan's ascending indices
+    for (long long n : {0LL, 1LL, 17LL, 262144LL, 262145LL, 1000003LL}) {
+        for (int density : {0, 1, 50, 100}) {
+            std::vector<float> mask((size_t)n, 0.f);
+            for (auto& x : mask) x = (int)(rng() % 100) < density ? 1.f : 0.f;
+            std::vector<int> want;
+            for (long long i = 0; i < n; ++i)
+                if (mask[(size_t)i] != 0.0f) want.push_back((int)i);
+            if (kw::flat_nonzero(mask.data(), n) != want) {
+                std::printf("flat_nonzero mismatch for n=%lld density=%d\n", n, density);
+                return 1;
+            }
+        }
     }
     std::printf("ok\n");
     return 0;
