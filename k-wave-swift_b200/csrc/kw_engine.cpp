@@ -501,7 +501,7 @@ void Engine::setup_sim(int s, const kw_sim_desc& d) {
         std::vector<float> host(N);
         check(cudaMemcpyAsync(host.data(), f, fb, cudaMemcpyDeviceToHost, st()), "download");
         check(cudaStreamSynchronize(st()), "sync");
-        for (long long i = 0; i < N; ++i) dst[i] = host[i];
+        parallel_for(N, [&](long long i) { dst[i] = host[i]; });
         return f;
     };
     const bool need_window = (d.smooth_c0 && c0map) || (d.smooth_rho0 && rho0map) || (d.p0 && d.smooth_p0);
@@ -561,9 +561,9 @@ void Engine::setup_sim(int s, const kw_sim_desc& d) {
     float* d_c0 = nullptr;
     float* d_rho0 = nullptr;
     if (d.smooth_c0 && c0map) d_c0 = smooth_to_host(d.sound_speed.data, c0);
-    else for (size_t i = 0; i < c0.size(); ++i) c0[i] = d.sound_speed.data[i];
+    else parallel_for((long long)c0.size(), [&](long long i) { c0[i] = d.sound_speed.data[i]; });
     if (d.smooth_rho0 && rho0map) d_rho0 = smooth_to_host(d.density.data, rho0);
-    else for (size_t i = 0; i < rho0.size(); ++i) rho0[i] = d.density.data[i];
+    else parallel_for((long long)rho0.size(), [&](long long i) { rho0[i] = d.density.data[i]; });
     (void)d_c0;
     (void)d_rho0;
     if (d.p0) {
