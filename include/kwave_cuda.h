@@ -291,10 +291,11 @@ KW_API int kw_spectral_derivative(kw_context* ctx, int dim, int nx, int ny, int 
  * half-spectrum, twiddle tables, operator vector, tile maps) lives in one file-scope device array
  * of KW_NOALLOC_SCRATCH_BYTES that every GPU loading this library keeps until the process exits;
  * problems that need more are rejected with KW_ERR_INVALID and a message naming the limit (about
- * 2 M half-spectrum values: e.g. 2D 1024^2 or 3D 128^3 fit). The first call on a device looks up
- * the array's device address (cudaGetSymbolAddress); make that first call before any stream
- * capture. All calls share the array and it keeps the last call's contents (each call clears what
- * it uses); calls whose work overlaps on the GPU race on it. */
+ * 2 M half-spectrum values: e.g. 2D 1024^2 or 3D 128^3 fit). Every call looks up the array's
+ * device address (cudaGetSymbolAddress) with the context's device current, so a device whose
+ * context was reset and re-created is served from its new copy. All calls share the array and it
+ * keeps the last call's contents (each call clears what it uses); calls whose work overlaps on the
+ * GPU race on it. */
 #define KW_NOALLOC_SCRATCH_BYTES (16u * 1024u * 1024u)
 KW_API int kw_spectral_derivative_noalloc(kw_context* ctx, int dim, int nx, int ny, int nz, double dx, double dy,
                                           double dz, int axis, int shift, const float* d_in, float* d_out);

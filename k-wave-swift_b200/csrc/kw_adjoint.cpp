@@ -43,6 +43,7 @@ void Engine::adjoint(const kw_sim_desc& din, kw_adjoint_desc& a) {
         throw err(KW_ERR_INVALID, "adjoint: a sensor is required");
     kw_sim_desc d = din;
     d.record = KW_RECORD_P;   // the reverse sweep reads the p series only
+    precorrect_ok_ = false;   // the tape epilogues follow the per-step source job
     create(&d, 1);
     SimHost& h = sims_[0];
     SimDev& v = h.dev;
@@ -158,8 +159,10 @@ void Engine::adjoint(const kw_sim_desc& din, kw_adjoint_desc& a) {
     auto tape_copy = [&]() { launch_adj_tape(st(), d_sims_, d_t_, d_table, stokes, N); };
     auto set_tape_mode = [&](bool on) {
         tape_mode_ = on;
-        if (graph_exec_) { cudaGraphExecDestroy(graph_exec_); graph_exec_ = nullptr; }
-        if (graph_) { cudaGraphDestroy(graph_); graph_ = nullptr; }
+        for (int g = 0; g < 2; ++g) {
+            if (graph_exec_[g]) { cudaGraphExecDestroy(graph_exec_[g]); graph_exec_[g] = nullptr; }
+            if (graph_[g]) { cudaGraphDestroy(graph_[g]); graph_[g] = nullptr; }
+        }
     };
 
     cudaEvent_t e0, e1, e2;

@@ -45,12 +45,33 @@ __device__ __forceinline__ bool mbar_test_parity(uint64_t* bar, uint32_t parity)
     return ok != 0;
 }
 
-// Wait until the phase with the given parity has completed; false (and `err` set) after ~1 s.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int* err, int code) {
+// default limit of a bounded wait: ~1.1 s at 1.9 GHz
+constexpr long long kWaitCycles = 1LL << 31;
+
+// Wait until the phase with the given parity has completed; false (and `err` set) after `limit`
+// clock64 cycles.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int* err, int code,
+                                          long long limit = kWaitCycles) {
     if (mbar_test_parity(bar, parity)) return true;
     const long long t0 = clock64();
     while (!mbar_test_parity(bar, parity)) {
-        if (clock64() - t0 > (1LL << 31)) {   // ~1.1 s at 1.9 GHz
+        if (clock64() - t0 > limit) {
+            atomicCAS(err, 0, code);
+            return false;
+        }
+    }
+    return true;
+}
+
+// As mbar_wait, but also gives up (returning false without recording an error) once `*abort` is
+// set: the producer of a pass whose consumers have stopped stops issuing copies at once.
+__device__ __forceinline__ bool mbar_wait_or_abort(uint64_t* bar, uint32_t parity, int* err, int code,
+                                                   const volatile int* abort) {
+    if (mbar_test_parity(bar, parity)) return true;
+    const long long t0 = clock64();
+    while (!mbar_test_parity(bar, parity)) {
+        if (*abort) return false;
+        if (clock64() - t0 > kWaitCycles) {
             atomicCAS(err, 0, code);
             return false;
         }

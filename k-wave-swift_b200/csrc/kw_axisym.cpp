@@ -137,6 +137,8 @@ void Engine::create_as_carrier() {
         v.rho[a] = (float*)dalloc(fb);
     }
     v.nonfinite = d_flag_;
+    v.wait_cycles = wait_cycles_;
+    v.test_stall = test_stall_;
     build_tensor_maps(h, v);
     d_car_ = (SimDev*)dalloc(sizeof(SimDev));
     check(cudaMemcpyAsync(d_car_, &v, sizeof(SimDev), cudaMemcpyHostToDevice, st()), "upload sim");

@@ -131,6 +131,7 @@ enum Epilogue {
     EPI_ADJ_VEL,         // mu = lambda_u_a - d_a; lambda_u_a = sg_a^2 mu; w_a = sg_a dtor_a mu
     EPI_ADJ_SUM,         // lambda_p = sum_a d_a; x1 = tau c2 lambda_p; x2 = eta c2 lambda_p
     EPI_ADJ_EOS,         // the reverse equation of state (kw_adjoint.cu k_adj_eos) with d = A1, A2, A2(S)
+    EPI_DEN_SRC,         // EPI_DEN + rho_a += signal[t] psrc_q / d_a (precorrected pressure source active)
 };
 
 // Source operator of one field variable (SourceOp, KSpaceFirstOrder.swift:129-175).
@@ -222,10 +223,17 @@ struct SimDev {
     int eos_pointwise;     // EoS evaluated in the density epilogue / source kernels
 
     SourceDev psrc, usrc[kMaxComp];
+    // Additive pressure source with one signal row: the k-space corrected source of step t is
+    // signal[t] * Re F^-1(cos(c_ref dt k / 2) F(scale * mask)) (linearity; SourceOp.apply,
+    // KSpaceFirstOrder.swift:167-172), so that field is computed once at setup and the density
+    // epilogue adds signal[t] * psrc_q / d_a to each rho_a while the signal lasts (else null).
+    const float* psrc_q;
     int has_p, has_u[kMaxComp];
     int has_p0;
     SensorDev sensor;
     int* nonfinite;        // device flag
+    long long wait_cycles; // limit of a column pass consumer's wait for its tile (clock64 cycles)
+    int test_stall;        // test hook: the TMA column pass withholds its first tile copy
 };
 
 // One entry of a launch's block map: which simulation, which component, which tile.

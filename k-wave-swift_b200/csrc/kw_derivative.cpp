@@ -93,6 +93,8 @@ void Engine::create_derivative(int dim, const int* n, const double* d, int axis,
     v.p = const_cast<float*>(in);
     v.tmp[0] = out;
     v.nonfinite = d_flag_;
+    v.wait_cycles = wait_cycles_;
+    v.test_stall = test_stall_;
     build_tensor_maps(h, v);
     check(cudaMemcpyAsync(d_sims_, &v, sizeof(SimDev), cudaMemcpyHostToDevice, st()), "upload sim");
     deriv_axis_ = axis;

@@ -35,13 +35,19 @@ __device__ __forceinline__ float* field_ptr(const SimDev& S, int sel, int comp) 
 
 __device__ __forceinline__ bool gate_open(const SimDev& S, int gate, int comp, int t) {
     if (t >= S.nt) return false;
-    if (gate == GATE_PSRC) return S.has_p && t < S.psrc.len;
+    if (gate == GATE_PSRC) return S.has_p && !S.psrc_q && t < S.psrc.len;
     if (gate == GATE_USRC) return S.has_u[comp] && t < S.usrc[comp].len;
     if (gate == GATE_P0) return S.has_p0 != 0;
     if (gate == GATE_ABS) return comp == 0 ? S.absorb >= 2 : S.absorb == 3;
     if (gate == GATE_RECU) return S.sensor.kind != 0 && (S.sensor.record_u_series || S.sensor.record_u_agg);
     if (gate >= GATE_DIR) return gate - GATE_DIR < S.sensor.ndir;
     return true;
+}
+
+// Signal value at step t of a simulation's precorrected additive pressure source (SimDev::psrc_q);
+// 0 once the signal has ended or when the simulation has none.
+__device__ __forceinline__ float psrc_gain(const SimDev& S, int t) {
+    return (S.psrc_q && S.has_p && t < S.psrc.len) ? __ldg(S.psrc.signal + t) : 0.f;
 }
 
 // wavenumber index along reference axis `ax` for spectrum coordinates (ka, kb, kc)

@@ -25,6 +25,9 @@ void Engine::check(cudaError_t e, const char* what) {
 
 void* Engine::dalloc(size_t bytes) {
     if (bytes == 0) bytes = 16;
+    if (fail_alloc_ > 0 && ++nalloc_ == fail_alloc_)
+        throw err(KW_ERR_OOM, "device allocation of " + std::to_string(bytes) +
+                                  " bytes failed (KW_TEST_FAIL_ALLOC: simulated out-of-memory)");
     if (arena_) {
         // allocation-free mode: carve 256-byte aligned pieces out of the caller-provided region
         const size_t off = (arena_used_ + 255) & ~(size_t)255;
@@ -48,8 +51,12 @@ void* Engine::dalloc(size_t bytes) {
 }
 
 Engine::~Engine() {
-    if (graph_exec_) cudaGraphExecDestroy(graph_exec_);
-    if (graph_) cudaGraphDestroy(graph_);
+    if (poll_ev_) cudaEventDestroy(poll_ev_);
+    if (poll_host_) cudaFreeHost(poll_host_);
+    for (int v = 0; v < 2; ++v) {
+        if (graph_exec_[v]) cudaGraphExecDestroy(graph_exec_[v]);
+        if (graph_[v]) cudaGraphDestroy(graph_[v]);
+    }
     cudaStreamSynchronize(ctx_->stream);
     for (void* p : allocs_) cudaFree(p);
 }
@@ -194,7 +201,7 @@ void Engine::issue_step(bool first) {
     for (int a = 0; a < D; ++a) den.op[a] = OpSpec{AO_DNEG, (int8_t)a, RT_KAPPA, (int8_t)a};
     den.spec_in = sp1;
     den.spec_out = sp1;
-    den.epi = EPI_DEN;
+    den.epi = psrc_live() ? EPI_DEN_SRC : EPI_DEN;
     den.tape = tape_mode_ ? 1 : 0;
     den.coupled = 1;
     den.name = "den";
@@ -287,7 +294,7 @@ bool Engine::host_gate(const SimHost& h, int gate, int comp) const {
     const SimDev& S = h.dev;
     if (t_ >= h.nt) return false;
     switch (gate) {
-        case GATE_PSRC: return S.has_p && t_ < S.psrc.len;
+        case GATE_PSRC: return S.has_p && !S.psrc_q && t_ < S.psrc.len;
         case GATE_USRC: return comp < h.dim && S.has_u[comp] && t_ < S.usrc[comp].len;
         case GATE_P0: return S.has_p0 != 0;
         case GATE_ABS: return comp == 0 ? S.absorb >= 2 : S.absorb == 3;
@@ -309,8 +316,9 @@ double Engine::epi_bytes(const SimHost& h, int epi, int ncomp) const {
         case EPI_VEL_INIT: { double b = 0; for (int a = 0; a < ncomp; ++a) b += 4 + m(S.dtor[a]); return b; }
         case EPI_ADD_U: return 8.0 * ncomp;
         case EPI_DEN:
-            return 8.0 * D + 4 + m(S.rho0) +
-                   (S.absorb >= 1 ? 4 : 0) + (S.eos_pointwise ? eos : 0);
+        case EPI_DEN_SRC:
+            return 8.0 * D + 4 + m(S.rho0) + (S.absorb >= 1 ? 4 : 0) + (S.eos_pointwise ? eos : 0) +
+                   (epi == EPI_DEN_SRC && S.psrc_q && t_ < S.psrc.len ? 4 : 0);
         case EPI_ADD_RHO: return 8.0 * D + 4 + (S.eos_pointwise ? eos + (S.absorb == 1 ? 4 : 0) : 0);
         case EPI_EOS_ABS:
             return 8 + m(S.c2) + m(S.tau) + (S.absorb == 3 ? m(S.eta) : 0) + (S.nonlinear ? m(S.bona) + m(S.rho0) : 0);
@@ -328,6 +336,7 @@ int Engine::aux_slots(const SimHost& h, int epi) const {
         case EPI_VEL_INIT: return 1;
         case EPI_ADD_U: return 1;
         case EPI_DEN:
+        case EPI_DEN_SRC:
         case EPI_ADD_RHO:
             return h.dim + 1 + (S.eos_pointwise ? m(S.c2) + (S.absorb == 1 ? m(S.tau) + 1 : 0) + (S.nonlinear ? m(S.bona) : 0) : 0);
         case EPI_EOS_ABS:
@@ -370,10 +379,18 @@ std::vector<Engine::KernelTiming> Engine::profile_step(int reps) {
     return acc;
 }
 
-void Engine::capture_graph() {
-    if (graph_exec_ && graph_stream_ == st()) return;
-    if (graph_exec_) { cudaGraphExecDestroy(graph_exec_); graph_exec_ = nullptr; }
-    if (graph_) { cudaGraphDestroy(graph_); graph_ = nullptr; }
+// true while some simulation's precorrected pressure source still injects at step t_
+bool Engine::psrc_live() const {
+    for (const auto& h : sims_)
+        if (h.dev.psrc_q && h.dev.has_p && t_ < h.dev.psrc.len && t_ < h.nt) return true;
+    return false;
+}
+
+int Engine::capture_graph() {
+    const int var = psrc_live() ? 1 : 0;
+    if (graph_exec_[var] && graph_stream_[var] == st()) return var;
+    if (graph_exec_[var]) { cudaGraphExecDestroy(graph_exec_[var]); graph_exec_[var] = nullptr; }
+    if (graph_[var]) { cudaGraphDestroy(graph_[var]); graph_[var] = nullptr; }
     check(cudaStreamBeginCapture(st(), cudaStreamCaptureModeThreadLocal), "begin capture");
     try {
         issue_step(false);
@@ -383,9 +400,10 @@ void Engine::capture_graph() {
         if (g) cudaGraphDestroy(g);
         throw;
     }
-    check(cudaStreamEndCapture(st(), &graph_), "end capture");
-    check(cudaGraphInstantiate(&graph_exec_, graph_, 0), "graph instantiate");
-    graph_stream_ = st();
+    check(cudaStreamEndCapture(st(), &graph_[var]), "end capture");
+    check(cudaGraphInstantiate(&graph_exec_[var], graph_[var], 0), "graph instantiate");
+    graph_stream_[var] = st();
+    return var;
 }
 
 // ------------------------------------------------------------------------------------------
@@ -488,6 +506,8 @@ void Engine::setup_sim(int s, const kw_sim_desc& d) {
     }
     v.tmp[0] = (float*)dalloc(fb);
     v.nonfinite = d_flag_;
+    v.wait_cycles = wait_cycles_;
+    v.test_stall = test_stall_;
 
     // ---- medium; smoothing on the device (KSFO:367-373) ----
     const bool c0map = d.sound_speed.len > 1, rho0map = d.density.len > 1;
@@ -703,7 +723,9 @@ void Engine::setup_sim(int s, const kw_sim_desc& d) {
                 sd.scale[0] = upload(sc);
                 v.src_buf[0] = (float*)dalloc(fb);
                 need_skappa = true;
-                any_p_add_ = true;
+                // one signal row: the corrected source is signal[t] times a fixed field
+                h.psrc_precorrect = precorrect_ok_ && d.p.rows == 1 && d.p.len > 0;
+                if (!h.psrc_precorrect) any_p_add_ = true;
             }
             if (d.p_mode != KW_SOURCE_ADDITIVE) any_p_direct_ = true;
             v.has_p = sd.len > 0;
@@ -906,6 +928,30 @@ void Engine::setup_sim(int s, const kw_sim_desc& d) {
     check(cudaMemcpyAsync(d_sims_ + s, &v, sizeof(SimDev), cudaMemcpyHostToDevice, st()), "upload sim");
 }
 
+// The k-space corrected additive source of a single-row signal (SourceOp.apply .additive,
+// KSpaceFirstOrder.swift:167-172) is linear in the signal value: for axis a at step t it is
+// signal[t] Re F^-1(cos(c_ref dt k / 2) F(scale * mask)) / d_a with scale = 2 dt / (D c0). The
+// field Q = Re F^-1(cos(.) F(scale * mask)) is computed here once, into the simulation's source
+// buffer, and the density epilogue adds signal[t] Q / d_a to each rho_a: the per-step scatter and
+// transform job of the source disappear.
+void Engine::precorrect_psrc(int s) {
+    SimHost& h = sims_[s];
+    SimDev& v = h.dev;
+    launch_scatter(st(), v.src_buf[0], v.psrc.idx, v.psrc.scale[0], v.psrc.nsrc);
+    check(cudaGetLastError(), "source scatter");
+    SpecJob q;
+    q.in_field = FS_SRCBUF;
+    q.nin = 1;
+    q.nout = 1;
+    q.op[0] = OpSpec{AO_NONE, 0, RT_SKAPPA, 0};
+    q.epi = EPI_STORE;
+    q.out_field = FS_SRCBUF;
+    q.name = "psrc_q";
+    issue_job(q, s);
+    v.psrc_q = v.src_buf[0];
+    check(cudaMemcpyAsync(d_sims_ + s, &v, sizeof(SimDev), cudaMemcpyHostToDevice, st()), "upload sim");
+}
+
 void Engine::create(const kw_sim_desc* descs, int n) {
     if (n <= 0) throw err(KW_ERR_INVALID, "no simulations");
     // kspaceFirstOrderAS: one simulation, its preconditions (KSpaceFirstOrderAS.swift:35-38,87-95),
@@ -931,6 +977,7 @@ void Engine::create(const kw_sim_desc* descs, int n) {
         as_desc.directivity_angle = nullptr;
         as_desc.axisymmetric = 0;
         descs = &as_desc;
+        precorrect_ok_ = false;
     }
     check(cudaSetDevice(ctx_->device), "cudaSetDevice");
     sims_.resize(n);
@@ -943,6 +990,8 @@ void Engine::create(const kw_sim_desc* descs, int n) {
     d_flag_ = (int*)dalloc(2 * sizeof(int));   // [0] non-finite pressure, [1] device-side wait timeout
     d_red_ = (unsigned int*)dalloc(4 * sizeof(unsigned int));
     for (int i = 0; i < n; ++i) setup_sim(i, descs[i]);
+    for (int i = 0; i < n; ++i)
+        if (sims_[i].psrc_precorrect) precorrect_psrc(i);
     std::vector<const float*> p0s(n);
     for (int i = 0; i < n; ++i) p0s[i] = sims_[i].p0s;
     d_p0s_ = (const float**)dalloc(sizeof(float*) * n);
@@ -964,7 +1013,7 @@ void Engine::reset() {
             check(cudaMemsetAsync(v.rho[a], 0, fb, st()), "reset");
         }
         for (int a = 0; a < kMaxComp; ++a)
-            if (v.src_buf[a]) check(cudaMemsetAsync(v.src_buf[a], 0, fb, st()), "reset");
+            if (v.src_buf[a] && v.src_buf[a] != v.psrc_q) check(cudaMemsetAsync(v.src_buf[a], 0, fb, st()), "reset");
     }
     check(cudaMemsetAsync(d_t_, 0, sizeof(int), st()), "reset");
     check(cudaMemsetAsync(d_flag_, 0, 2 * sizeof(int), st()), "reset");
@@ -981,21 +1030,56 @@ void Engine::step(int nsteps) {
         if (t_ == 0) {
             issue_step(true);
         } else {
-            capture_graph();
-            check(cudaGraphLaunch(graph_exec_, st()), "graph launch");
+            const int var = capture_graph();
+            check(cudaGraphLaunch(graph_exec_[var], st()), "graph launch");
         }
         ++t_;
     }
     check(cudaGetLastError(), "launch");
 }
 
+// Test hooks, read once per engine from the environment (both off by default):
+//   KW_TEST_STALL_COLUMN_PASS=1  the TMA-fed column pass withholds the copy of each CTA's first
+//                                tile and its consumers wait at most ~20 us (40000 cycles) for it:
+//                                the bounded wait runs out, the kernel records KE_TIMEOUT_FULL and
+//                                returns, and the run reports KW_ERR_TIMEOUT;
+//   KW_TEST_FAIL_ALLOC=n         the n-th device allocation fails as if the device were out of
+//                                memory.
+Engine::Engine(Context* ctx) : ctx_(ctx) {
+    if (const char* w = std::getenv("KW_TEST_STALL_COLUMN_PASS"); w && w[0] == '1') {
+        test_stall_ = 1;
+        wait_cycles_ = 40000;
+    }
+    if (const char* f = std::getenv("KW_TEST_FAIL_ALLOC")) fail_alloc_ = std::max(0, std::atoi(f));
+}
+
+// kw_sim_run: every kFinitePoll steps the pressure of every simulation is checked for NaN / Inf
+// on the device; the host reads that check's flag one poll later (it has long completed by then,
+// so the stream never drains for it) and stops the run at the first poll that finds one, leaving
+// synchronize() to report KW_ERR_NONFINITE.
 void Engine::run(const kw_callbacks* cb) {
     reset();
     int tmax = 0;
     for (auto& h : sims_) tmax = std::max(tmax, h.nt);
     const int interval = cb && cb->monitor_interval > 0 ? cb->monitor_interval : 1;
     std::vector<float> host;
+    if (!poll_host_) {
+        check(cudaMallocHost(&poll_host_, sizeof(int)), "pinned flag");
+        check(cudaEventCreateWithFlags(&poll_ev_, cudaEventDisableTiming), "event");
+    }
+    bool poll_pending = false;
     for (int t = 0; t < tmax; ++t) {
+        if (t > 0 && t % kFinitePoll == 0) {
+            if (poll_pending) {
+                check(cudaEventSynchronize(poll_ev_), "poll");
+                if (*poll_host_) break;
+            }
+            const Map& m = map_elems(-1);
+            launch_check_finite(st(), d_sims_, d_t_, m.d, m.n);
+            check(cudaMemcpyAsync(poll_host_, d_flag_, sizeof(int), cudaMemcpyDeviceToHost, st()), "poll copy");
+            check(cudaEventRecord(poll_ev_, st()), "poll event");
+            poll_pending = true;
+        }
         step(1);
         if (cb && cb->monitor && t % interval == 0) {
             const SimHost& h = sims_[0];

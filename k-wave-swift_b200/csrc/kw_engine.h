@@ -9,6 +9,7 @@
 
 #include "../../include/kwave_cuda.h"
 #include "kw_common.h"
+#include "kw_async.cuh"
 #include "kw_kernels.cuh"
 
 namespace kw {
@@ -48,13 +49,14 @@ struct SimHost {
     bool record_p = false, record_u = false, record_ufinal = false;
     bool p_series = false, u_series = false, p_agg = false, u_agg = false;
     int npts = 0;
+    bool psrc_precorrect = false;  // single-row additive p source: corrected once at setup
     float* p0s = nullptr;          // smoothed initial pressure (device) or null
     SimDev dev{};
 };
 
 class Engine {
 public:
-    explicit Engine(Context* ctx) : ctx_(ctx) {}
+    explicit Engine(Context* ctx);
     ~Engine();
     void create(const kw_sim_desc* descs, int count);
     void reset();
@@ -150,7 +152,7 @@ private:
     const Map& map_planes(int ncomp, int sim_only);
     void issue_job(const SpecJob& job, int sim_only);
     void issue_step(bool first);
-    void capture_graph();
+    int capture_graph();   // returns the variant captured / in use for the current step
     void finalize_outputs();
 
     Context* ctx_;
@@ -168,15 +170,22 @@ private:
     bool any_abs_ = false, any_p0_ = false, any_recu_ = false, any_recp_ = false;
     int max_A_ = 1, max_B_ = 1, max_M_ = 1;
     std::map<std::tuple<int, int, int, int, int>, Map> maps_;
-    cudaGraph_t graph_ = nullptr;
-    cudaGraphExec_t graph_exec_ = nullptr;
-    cudaStream_t graph_stream_ = nullptr;
+    // the steady step as CUDA graphs: [1] while a precorrected pressure source of some simulation
+    // is still injecting (the density epilogue adds it), [0] otherwise
+    cudaGraph_t graph_[2] = {nullptr, nullptr};
+    cudaGraphExec_t graph_exec_[2] = {nullptr, nullptr};
+    cudaStream_t graph_stream_[2] = {nullptr, nullptr};
+    bool psrc_live() const;
     std::vector<ProfRec>* prof_ = nullptr;
     int deriv_axis_ = 0, deriv_shift_ = 1;
     char* arena_ = nullptr;
     size_t arena_size_ = 0, arena_used_ = 0;
     bool finalized_ = false;
     bool tape_mode_ = false;   // adjoint: steps are captured with the tape epilogues
+    // single-row additive pressure sources may be precorrected at setup (SimDev::psrc_q); the
+    // adjoint and the axisymmetric solver keep the per-step correction job
+    bool precorrect_ok_ = true;
+    void precorrect_psrc(int s);
     cudaStream_t st_override_ = nullptr;   // adjoint: the reverse sweep's own stream while it issues work
     // axisymmetric solver (kw_axisym.cpp): sims_[0] is the [nx][ny] simulation, car_ / d_car_ the
     // descriptor of its 4x radial expansion that the spectral jobs run on
@@ -186,6 +195,12 @@ private:
     void create_as_carrier();
     void issue_step_as(bool first);
     int finalized_t_ = -1;
+    static constexpr int kFinitePoll = 64;   // steps between the non-finite checks of run()
+    int* poll_host_ = nullptr;                // pinned copy of the non-finite flag
+    cudaEvent_t poll_ev_ = nullptr;
+    long long wait_cycles_ = kWaitCycles;     // SimDev::wait_cycles (test hook KW_TEST_STALL_COLUMN_PASS)
+    int test_stall_ = 0;                      // SimDev::test_stall (same hook)
+    int fail_alloc_ = 0, nalloc_ = 0;         // test hook KW_TEST_FAIL_ALLOC
     // finalised aggregate outputs per sim (device)
     struct Outs {
         float* iavg[kMaxComp] = {nullptr, nullptr, nullptr};

@@ -119,6 +119,7 @@ void launch_src_p(cudaStream_t st, const SimDev* d_sims, const int* d_t, int nsi
 void launch_sample(cudaStream_t st, const SimDev* d_sims, const int* d_t, int nsims, int max_pts, int which,
                    int comp);
 void launch_tick(cudaStream_t st, int* d_t);
+void launch_scatter(cudaStream_t st, float* dst, const int* idx, const float* val, int n);
 void launch_check_finite(cudaStream_t st, const SimDev* d_sims, const int* d_t, const BlockWork* map, int nblocks);
 
 // setup helpers on one field (single simulation)

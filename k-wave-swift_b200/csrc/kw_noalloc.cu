@@ -10,7 +10,7 @@
 // library holds until the process exits. All calls share it and it keeps the last call's contents;
 // the engine clears every piece it carves before use. Two calls whose work overlaps on the GPU
 // (different streams or threads) race on the array.
-#include <mutex>
+#include <string>
 
 #include "../../include/kwave_cuda.h"
 #include "kw_engine.h"
@@ -20,26 +20,22 @@ namespace kw {
 static __device__ __align__(256) unsigned char g_noalloc_scratch[KW_NOALLOC_SCRATCH_BYTES];
 
 // Device address of g_noalloc_scratch on `device`. In host code the array's name is only a host
-// stand-in, never a device address; the address comes from cudaGetSymbolAddress, once per
-// device, with that device current.
+// stand-in, never a device address; the address comes from cudaGetSymbolAddress with that device
+// current. It is looked up on every call rather than cached, so that a device whose context was
+// reset (cudaDeviceReset) and re-created gets the address of its new copy of the array.
 void* noalloc_scratch(int device) {
-    static std::mutex mu;
-    static void* addr[64] = {};
-    if (device < 0 || device >= 64) throw KwError{KW_ERR_INVALID, "device index out of range"};
-    std::lock_guard<std::mutex> lock(mu);
-    if (!addr[device]) {
-        int cur = 0;
-        cudaGetDevice(&cur);
-        if (cur != device) throw KwError{KW_ERR_STATE, "scratch set-up needs the context's device current"};
-        void* p = nullptr;
-        const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-        if (e != cudaSuccess || !p) {
-            cudaGetLastError();
-            throw KwError{KW_ERR_CUDA, std::string("cudaGetSymbolAddress of the scratch array failed: ") + cudaGetErrorString(e)};
-        }
-        addr[device] = p;
+    int cur = 0;
+    if (cudaGetDevice(&cur) != cudaSuccess || cur != device) {
+        cudaGetLastError();
+        throw KwError{KW_ERR_STATE, "scratch set-up needs the context's device current"};
     }
-    return addr[device];
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess || !p) {
+        cudaGetLastError();
+        throw KwError{KW_ERR_CUDA, std::string("cudaGetSymbolAddress of the scratch array failed: ") + cudaGetErrorString(e)};
+    }
+    return p;
 }
 
 }  // namespace kw

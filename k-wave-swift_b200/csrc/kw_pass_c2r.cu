@@ -20,9 +20,10 @@ __device__ __forceinline__ AuxPlan aux_plan(const SimDev& S, const RowC2RJob& jo
         case EPI_VEL_INIT: a.src[AX_F1] = S.dtor[comp0].ptr; break;
         case EPI_ADD_U: a.src[AX_F0] = S.u[comp0]; break;
         case EPI_DEN:
+        case EPI_DEN_SRC:
         case EPI_ADD_RHO:
             for (int d = 0; d < S.dim; ++d) a.src[AX_F0 + d] = S.rho[d];
-            if (S.nonlinear || S.absorb >= 1 || job.epi == EPI_DEN) a.src[AX_RHO0] = S.rho0.ptr;
+            if (S.nonlinear || S.absorb >= 1 || job.epi != EPI_ADD_RHO) a.src[AX_RHO0] = S.rho0.ptr;
             if (S.eos_pointwise) {
                 a.src[AX_C2] = S.c2.ptr;
                 if (S.absorb == 1) a.src[AX_TAU] = S.tau.ptr;
@@ -89,7 +90,8 @@ __device__ __forceinline__ void c2r_stage_aux(const SimDev& S, const AuxPlan& a,
 // epilogue at one grid point; staged inputs come from `av(field)` (the value of that field here)
 template <class AV>
 __device__ __forceinline__ void epi_point(const SimDev& S, const RowC2RJob& job, int comp0, int ncomp, long long i,
-                                          int ca, int cb, int cc, const float* d, AV av, const AdjTapeEntry* te) {
+                                          int ca, int cb, int cc, const float* d, AV av, const AdjTapeEntry* te,
+                                          float sgain) {
     auto coord = [&](int ax) { const int L = ax + 3 - S.dim; return L == 0 ? ca : (L == 1 ? cb : cc); };
     auto c2_at = [&]() { return S.c2.ptr ? av(AX_C2) : S.c2.s; };
     auto rho0_at = [&]() { return S.rho0.ptr ? av(AX_RHO0) : S.rho0.s; };
@@ -119,7 +121,8 @@ __device__ __forceinline__ void epi_point(const SimDev& S, const RowC2RJob& job,
         case EPI_ADD_U:
             S.u[comp0][i] = av(AX_F0) + d[0];
             break;
-        case EPI_DEN: {  // KSpaceFirstOrder.swift:457-465 (+ EoS when pointwise)
+        case EPI_DEN:
+        case EPI_DEN_SRC: {  // KSpaceFirstOrder.swift:457-465 (+ EoS when pointwise)
             const float r0v = rho0_at();
             float nl = 1.f;
             if (S.nonlinear) {
@@ -132,7 +135,9 @@ __device__ __forceinline__ void epi_point(const SimDev& S, const RowC2RJob& job,
             for (int a = 0; a < S.dim; ++a) {
                 const float pm = __ldg(S.ax[a].pml + coord(a));
                 const float mass = S.nonlinear ? dtr * d[a] * nl : dtr * d[a];
-                const float r = pm * (pm * av(AX_F0 + a) - mass);
+                float r = pm * (pm * av(AX_F0 + a) - mass);
+                // precorrected additive pressure source (SimDev::psrc_q)
+                if (sgain != 0.f) r = r + (sgain * __ldg(S.psrc_q + i)) * S.ax[a].inv_d;
                 S.rho[a][i] = r;
                 if (te && S.nonlinear) te->dd[a][i] = d[a];   // the adjoint's recompute keeps d_a
                 rs = a == 0 ? r : rs + r;
@@ -187,7 +192,7 @@ __device__ __forceinline__ void epi_point(const SimDev& S, const RowC2RJob& job,
 
 template <int MT>
 __device__ __forceinline__ void c2r_compute(const SimDev& S, const BlockWork bw, const RowC2RJob& job, const AdjTapeEntry* te, float2* buf,
-                                            float2* tmp, const float* aux, const AuxPlan& a) {
+                                            float2* tmp, const float* aux, const AuxPlan& a, int t) {
     constexpr bool FIX = MT > 0;
     constexpr int LT = FIX ? c2r_lines(MT) : 1;
     const RowTile r = c2r_tile(S, job, bw);
@@ -241,6 +246,7 @@ __device__ __forceinline__ void c2r_compute(const SimDev& S, const BlockWork bw,
 
     cp_wait<1>();        // this tile's staged epilogue inputs have landed
     __syncthreads();
+    const float sgain = job.epi == EPI_DEN_SRC ? psrc_gain(S, t) : 0.f;
     const int rowsz = r.RPC * C;
     const int B = S.B;
     for (int w = threadIdx.x; w < nl * M; w += blockDim.x) {
@@ -260,13 +266,13 @@ __device__ __forceinline__ void c2r_compute(const SimDev& S, const BlockWork bw,
             const long long i0 = (long long)row * C + 2 * m;
             const int e0 = l * C + 2 * m;
             epi_point(S, job, r.comp0, ncomp, i0, ca, cb, 2 * m, d0,
-                      [&](int f) { return aux[a.slot[f] * rowsz + e0]; }, te);
+                      [&](int f) { return aux[a.slot[f] * rowsz + e0]; }, te, sgain);
             epi_point(S, job, r.comp0, ncomp, i0 + 1, ca, cb, 2 * m + 1, d1,
-                      [&](int f) { return aux[a.slot[f] * rowsz + e0 + 1]; }, te);
+                      [&](int f) { return aux[a.slot[f] * rowsz + e0 + 1]; }, te, sgain);
         } else {
             const int e0 = l * C + m;
             epi_point(S, job, r.comp0, ncomp, (long long)row * C + m, ca, cb, m, d0,
-                      [&](int f) { return aux[a.slot[f] * rowsz + e0]; }, te);
+                      [&](int f) { return aux[a.slot[f] * rowsz + e0]; }, te, sgain);
         }
     }
 }
@@ -298,7 +304,7 @@ __global__ void __launch_bounds__(256) k_row_c2r(const SimDev* __restrict__ sims
         cp_commit();
         cp_wait<2>();                                                // spectrum of tile k
         __syncthreads();
-        if (open) c2r_compute<MT>(S, bw, job, job.tape ? S.tape + t : nullptr, sm + (k & 1) * te, tmp, aux, a);
+        if (open) c2r_compute<MT>(S, bw, job, job.tape ? S.tape + t : nullptr, sm + (k & 1) * te, tmp, aux, a, t);
         __syncthreads();
     }
     cp_wait<0>();

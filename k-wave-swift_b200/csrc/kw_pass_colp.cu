@@ -47,7 +47,9 @@ __global__ void __launch_bounds__(288, ColpCfg<N>::MINB) k_colp(const SimDev* __
     float2* sh = reinterpret_cast<float2*>(smem + NS * Cfg::STAGE);
     uint64_t* full = reinterpret_cast<uint64_t*>(smem + Cfg::BAR_OFF);
     uint64_t* empty = full + NS;
+    __shared__ volatile int abort;   // set by the consumers when one of their waits ran out
     if (threadIdx.x == 0) {
+        abort = 0;
         for (int s = 0; s < NS; ++s) {
             mbar_init(full + s, 1);
             mbar_init(empty + s, 8);
@@ -62,26 +64,32 @@ __global__ void __launch_bounds__(288, ColpCfg<N>::MINB) k_colp(const SimDev* __
         // ---------------- producer ----------------
         if (threadIdx.x != 256) return;
         int k = 0;
+        bool withheld = false;   // test hook (SimDev::test_stall): the first tile's copy was not issued
         for (int idx = blockIdx.x; idx < nmap; idx += gridDim.x) {
             const BlockWork bw = map[idx];
             const SimDev& S = sims[bw.sim];
             if (!gate_open(S, job.gate, bw.comp, tstep)) continue;
             const int s = k % NS;
-            if (k >= NS && !mbar_wait(empty + s, ((k / NS) & 1) ^ 1, err, KE_TIMEOUT_EMPTY)) break;
+            if (k >= NS && !mbar_wait_or_abort(empty + s, ((k / NS) & 1) ^ 1, err, KE_TIMEOUT_EMPTY, &abort)) break;
             const int inner = axisA ? S.B * S.Cp : S.Cp;
             const int nch = (inner + TW - 1) / TW;
             const int o = bw.tile / nch;
             const int c0 = (bw.tile - o * nch) * TW;
             const int comp_in = job.fanout ? 0 : bw.comp;
             unsigned char* st = smem + s * Cfg::STAGE;
-            mbar_arrive_expect_tx(full + s, Cfg::STAGE);
-            const CUtensorMap* tm = S.tmaps + tmap_spec(job.spec_in + comp_in, job.layout_axis);
-            if (axisA) tma_load_2d(st, tm, c0, 0, full + s);
-            else tma_load_3d(st, tm, c0, 0, o, full + s);
+            if (S.test_stall && k == 0) {
+                withheld = true;   // its consumers' bounded wait runs out: nothing completes the barrier
+            } else {
+                mbar_arrive_expect_tx(full + s, Cfg::STAGE);
+                const CUtensorMap* tm = S.tmaps + tmap_spec(job.spec_in + comp_in, job.layout_axis);
+                if (axisA) tma_load_2d(st, tm, c0, 0, full + s);
+                else tma_load_3d(st, tm, c0, 0, o, full + s);
+            }
             ++k;
         }
         // every issued copy must have landed before this CTA's shared memory is released
-        for (int j = k > NS ? k - NS : 0; j < k; ++j) mbar_wait(full + j % NS, (j / NS) & 1, err, KE_TIMEOUT_DRAIN);
+        for (int j = k > NS ? k - NS : 0; j < k; ++j)
+            if (!(withheld && j == 0)) mbar_wait(full + j % NS, (j / NS) & 1, err, KE_TIMEOUT_DRAIN);
         return;
     }
 
@@ -95,12 +103,17 @@ __global__ void __launch_bounds__(288, ColpCfg<N>::MINB) k_colp(const SimDev* __
         const SimDev& S = sims[bw.sim];
         if (!gate_open(S, job.gate, bw.comp, tstep)) continue;
         const int s = k % NS;
-        const bool ok = mbar_wait(full + s, (k / NS) & 1, err, KE_TIMEOUT_FULL);
+        // (the limit is the simulation's: a test shortens it to make this wait run out; the
+        // producer's waits keep the default, so it still drains its copies before exiting)
+        const bool ok = mbar_wait(full + s, (k / NS) & 1, err, KE_TIMEOUT_FULL, S.wait_cycles);
         // all consumers agree before anyone touches the stage or a barrier
         int all_ok;
         asm volatile("{\n\t.reg .pred p, q;\n\tsetp.ne.u32 p, %1, 0;\n\tbar.red.and.pred q, 1, 256, p;\n\tselp.u32 %0, 1, 0, q;\n\t}"
                      : "=r"(all_ok) : "r"((unsigned)ok) : "memory");
-        if (!all_ok) return;
+        if (!all_ok) {
+            if (threadIdx.x == 0) abort = 1;
+            return;
+        }
         const float2* tile = reinterpret_cast<const float2*>(smem + s * Cfg::STAGE);
 
         const int inner = axisA ? S.B * S.Cp : S.Cp;

@@ -30,6 +30,8 @@ template <int M, int EPI, bool TAPE>
 constexpr int rowr_minb() {
     // left alone these take 129-152 registers at some lengths (one CTA per SM)
     if (EPI == EPI_ADJ_EOS || EPI == EPI_ADD_RHO || TAPE || M >= 768) return 2;
+    // the density update with the precorrected source reads one field more (spills at 85 registers)
+    if (EPI == EPI_DEN_SRC) return 2;
     return M <= 128 ? 3 : 0;
 }
 
@@ -91,7 +93,8 @@ __global__ void __launch_bounds__(256, rowr_minb<M, EPI, TAPE>()) k_rowr_c2r(con
     using Lay = RowLayout<P, M>;
     constexpr int R1 = P::R1, T = P::T, TW = P::LINES;
     // pairs whose inputs are loaded together (the density update reads the most fields)
-    constexpr int MB = (EPI == EPI_DEN || EPI == EPI_ADJ_EOS || R1 < 4) ? 2 : 4;
+    constexpr bool DEN = EPI == EPI_DEN || EPI == EPI_DEN_SRC;
+    constexpr int MB = (DEN || EPI == EPI_ADJ_EOS || R1 < 4) ? 2 : 4;
     __shared__ float2 sh[Lay::SLOTS];
     extern __shared__ __align__(16) float2 parked[];   // coupled epilogues: [ncomp - 1][R1][256]
     if (blockIdx.x >= nmap) return;
@@ -137,6 +140,12 @@ __global__ void __launch_bounds__(256, rowr_minb<M, EPI, TAPE>()) k_rowr_c2r(con
     // is read at samples 2n, 2n+1
     auto row_const = [&](const float* vec, int a) { return __ldg(vec + (a + 3 - D == 0 ? ca : cb)); };
     auto row_pair = [&](const float* vec, int n) { return __ldg(reinterpret_cast<const float2*>(vec) + n); };
+    // precorrected additive pressure source: rho_a += signal[t] psrc_q / d_a while it lasts
+    // (sg_d[a] = signal[t] / d_a; the field is not read, and 0 is added, once the signal has ended)
+    const float sgain = EPI == EPI_DEN_SRC ? psrc_gain(S, *d_t) : 0.f;
+    float sg_d[kMaxComp];
+#pragma unroll
+    for (int a = 0; a < kMaxComp; ++a) sg_d[a] = (EPI == EPI_DEN_SRC && a < S.dim) ? sgain * S.ax[a].inv_d : 0.f;
 
 #pragma unroll
     for (int m0 = 0; m0 < R1; m0 += MB) {
@@ -176,15 +185,15 @@ __global__ void __launch_bounds__(256, rowr_minb<M, EPI, TAPE>()) k_rowr_c2r(con
                 }
                 st_state(u, rbase + 2 * (t + T * (m0 + b)), o);
             }
-        } else if constexpr (EPI == EPI_DEN || EPI == EPI_ADD_RHO) {
+        } else if constexpr (DEN || EPI == EPI_ADD_RHO) {
             // density (KSpaceFirstOrder.swift:457-465) or additive pressure source
             // (KSpaceFirstOrder.swift:167-172), then the pointwise equation of state when there is one
-            float2 ro[kMaxComp][MB], pmr[MB], r0[MB], c2[MB], tau[MB], bona[MB], eta[MB];
+            float2 ro[kMaxComp][MB], pmr[MB], r0[MB], c2[MB], tau[MB], bona[MB], eta[MB], sq[MB];
             float pmc[kMaxComp - 1];
 #pragma unroll
             for (int a = 0; a < kMaxComp - 1; ++a)
-                if (EPI == EPI_DEN && a < D - 1) pmc[a] = row_const(S.ax[a].pml, a);
-            const bool need_r0 = EPI == EPI_DEN || S.nonlinear;
+                if (DEN && a < D - 1) pmc[a] = row_const(S.ax[a].pml, a);
+            const bool need_r0 = DEN || S.nonlinear;
 #pragma unroll
             for (int b = 0; b < MB; ++b) {
                 const int n = t + T * (m0 + b);
@@ -192,7 +201,8 @@ __global__ void __launch_bounds__(256, rowr_minb<M, EPI, TAPE>()) k_rowr_c2r(con
 #pragma unroll
                 for (int a = 0; a < kMaxComp; ++a)
                     if (a < D) ro[a][b] = ld_state(S.rho[a], e);
-                if (EPI == EPI_DEN) pmr[b] = row_pair(S.ax[D - 1].pml, n);
+                if (DEN) pmr[b] = row_pair(S.ax[D - 1].pml, n);
+                if (EPI == EPI_DEN_SRC) sq[b] = sgain != 0.f ? ld_ro(S.psrc_q, e) : make_float2(0.f, 0.f);
                 if (need_r0) r0[b] = ld_medium(S.rho0, e);
                 if (S.eos_pointwise) {
                     c2[b] = ld_medium(S.c2, e);
@@ -210,7 +220,7 @@ __global__ void __launch_bounds__(256, rowr_minb<M, EPI, TAPE>()) k_rowr_c2r(con
                 for (int h = 0; h < 2; ++h) {
                     const float r0v = need_r0 ? half(r0[b], h) : 0.f;
                     float rs = 0.f, divterm = 0.f;
-                    if (EPI == EPI_DEN) {
+                    if (DEN) {
                         float nl = 1.f;
                         if (S.nonlinear) {
                             float rp = 0.f;
@@ -228,7 +238,8 @@ __global__ void __launch_bounds__(256, rowr_minb<M, EPI, TAPE>()) k_rowr_c2r(con
                                 const float d = half(dp, h);
                                 const float pmv = a == D - 1 ? half(pmr[b], h) : pmc[a < kMaxComp - 1 ? a : 0];
                                 const float mass = S.nonlinear ? dtr * d * nl : dtr * d;
-                                const float r = pmv * (pmv * half(ro[a][b], h) - mass);
+                                float r = pmv * (pmv * half(ro[a][b], h) - mass);
+                                if (EPI == EPI_DEN_SRC) r = r + sg_d[a] * half(sq[b], h);
                                 half(rn[a], h) = r;
                                 rs = a == 0 ? r : rs + r;
                                 dv = a == 0 ? d : dv + d;
@@ -258,11 +269,11 @@ __global__ void __launch_bounds__(256, rowr_minb<M, EPI, TAPE>()) k_rowr_c2r(con
                 for (int a = 0; a < kMaxComp; ++a)
                     if (a < D) st_state(S.rho[a], e, rn[a]);
                 st_state(S.rho_sum, e, rs2);
-                if (EPI == EPI_DEN && S.absorb >= 1) st_state(S.div_term, e, dv2);
+                if (DEN && S.absorb >= 1) st_state(S.div_term, e, dv2);
                 if (S.eos_pointwise) st_state(S.p, e, p2);
                 if constexpr (TAPE) {   // the adjoint's recompute: d_a = D-_a u_a, and S, p, div when they are final here
                     const AdjTapeEntry& te = S.tape[*d_t];
-                    if (EPI == EPI_DEN && S.nonlinear) {
+                    if (DEN && S.nonlinear) {
 #pragma unroll
                         for (int a = 0; a < kMaxComp; ++a)
                             if (a < D) st_state(te.dd[a], e, dpair(a, m));
@@ -271,7 +282,7 @@ __global__ void __launch_bounds__(256, rowr_minb<M, EPI, TAPE>()) k_rowr_c2r(con
                         st_state(te.s, e, rs2);
                         st_state(te.p, e, p2);
                     }
-                    if (EPI == EPI_DEN && S.absorb == 1) st_state(te.div, e, dv2);
+                    if (DEN && S.absorb == 1) st_state(te.div, e, dv2);
                 }
             }
         } else if constexpr (EPI == EPI_ADJ_VEL) {
@@ -468,6 +479,7 @@ static void set_rowr_attrs(int optin) {
 
 void init_rowr_attributes(int optin) {
     set_rowr_attrs<EPI_DEN>(optin);
+    set_rowr_attrs<EPI_DEN_SRC>(optin);
     set_rowr_attrs<EPI_EOS_ABS>(optin);
     set_rowr_attrs<EPI_DEN, true>(optin);
     set_rowr_attrs<EPI_EOS_ABS, true>(optin);
@@ -500,6 +512,7 @@ static void launch_c2r_m(cudaStream_t st, const SimDev* d_sims, const int* d_t, 
             if (job.tape) k_rowr_c2r<M, EPI_DEN, true><<<nmap, 256, smem, st>>>(d_sims, d_t, map, nmap, job);
             else k_rowr_c2r<M, EPI_DEN><<<nmap, 256, smem, st>>>(d_sims, d_t, map, nmap, job);
             break;
+        case EPI_DEN_SRC: k_rowr_c2r<M, EPI_DEN_SRC><<<nmap, 256, smem, st>>>(d_sims, d_t, map, nmap, job); break;
         case EPI_ADD_RHO:
             if (job.tape) k_rowr_c2r<M, EPI_ADD_RHO, true><<<nmap, 256, smem, st>>>(d_sims, d_t, map, nmap, job);
             else k_rowr_c2r<M, EPI_ADD_RHO><<<nmap, 256, smem, st>>>(d_sims, d_t, map, nmap, job);

@@ -68,6 +68,7 @@ __global__ void k_src_p(const SimDev* __restrict__ sims, const int* __restrict__
     if (q >= s.nsrc || t >= s.len) return;
     const bool additive = s.mode == 1;
     if (additive != (scatter_only != 0)) return;
+    if (S.psrc_q) return;   // precorrected: added by the density epilogue
     const float sig = src_value(s, q, t);
     const int i = __ldg(s.idx + q);
     if (additive) {
@@ -84,6 +85,16 @@ __global__ void k_src_p(const SimDev* __restrict__ sims, const int* __restrict__
     }
     S.rho_sum[i] = rs;
     if (S.eos_pointwise) S.p[i] = eos_point(S, i, rs, S.absorb == 1 ? S.div_term[i] : 0.f);
+}
+
+// dst[idx[q]] = val[q] (setup: the scaled source mask of a precorrected pressure source)
+__global__ void k_scatter(float* __restrict__ dst, const int* __restrict__ idx, const float* __restrict__ val, int n) {
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q < n) dst[__ldg(idx + q)] = __ldg(val + q);
+}
+
+void launch_scatter(cudaStream_t st, float* dst, const int* idx, const float* val, int n) {
+    if (n > 0) k_scatter<<<(n + 255) / 256, 256, 0, st>>>(dst, idx, val, n);
 }
 
 // sensor sampling + recording (Recording.swift:37-45, 129-168). which = 0: p, 1: velocity
