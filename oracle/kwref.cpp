@@ -1032,7 +1032,14 @@ double kwref_db2neper(double alpha, double y) { return db2neper(alpha, y); }
 /* Run the simulation of `desc` in FP64 (kspaceFirstOrderAS when desc->axisymmetric). max_steps < 0
  * runs all nt steps; otherwise stops after max_steps (used to time a bounded CPU sample).
  * nthreads <= 0 uses every core. */
+int kwref_run_timed(const kw_sim_desc* d, int nthreads, int max_steps, int timed_from, kwref_result** out);
 int kwref_run(const kw_sim_desc* d, int nthreads, int max_steps, kwref_result** out) {
+    return kwref_run_timed(d, nthreads, max_steps, 0, out);
+}
+
+/* As kwref_run; kwref_loop_seconds then covers the steps from `timed_from` on (the earlier ones are
+ * untimed warm-up steps of a benchmark window). */
+int kwref_run_timed(const kw_sim_desc* d, int nthreads, int max_steps, int timed_from, kwref_result** out) {
     if (!d || !out) { g_err = "null argument"; return KW_ERR_INVALID; }
 #ifdef _OPENMP
     if (nthreads > 0) omp_set_num_threads(nthreads);
@@ -1061,6 +1068,7 @@ int kwref_run(const kw_sim_desc* d, int nthreads, int max_steps, kwref_result** 
     auto t0 = std::chrono::steady_clock::now();
     vecc spec(N), work(N);
     for (int t = 0; t < steps; ++t) {
+        if (t == timed_from && t > 0) t0 = std::chrono::steady_clock::now();
         forward_step(m, st, t, spec, work);
         // sampling (KSFO:523-540)
         if (m.haveSampler) {
@@ -1168,13 +1176,17 @@ int kwref_run(const kw_sim_desc* d, int nthreads, int max_steps, kwref_result** 
  * symmetric), the k-space corrected additive pressure source (symmetric cos filter), the PML
  * density update (nl from the previous densities), the staggered derivatives (the transpose of
  * Re F^-1(H F .) is Re F^-1(conj(H) F .)), the PML velocity update, and finally the t = 0
- * override of an initial pressure. Gradients: dL/dc0 (pointwise field) and dL/dp0 (the
- * initial pressure after smoothing). The whole forward is kept in memory, so this is for small
+ * override of an initial pressure. Gradients: dL/dc0 (pointwise field), dL/dp0 (the
+ * initial pressure after smoothing) and dL/drho0 (pointwise field; a scalar density is treated as
+ * a uniform map: the scalar derivative is the sum of the field). rho0 enters the step through
+ * dt rho0 (d/drho0 of dt rho0 nl = dt (2 S(t-1) + rho0) is dt), rho0 div in the absorption input,
+ * B/A S^2 / (2 rho0), and dt / rho_sg with rho_sg = staggerDensity(rho0) (KSFO:799-806) in the
+ * velocity update and the t = 0 override. The whole forward is kept in memory, so this is for small
  * grids. Unsupported (KW_ERR_UNSUPPORTED): velocity sources, Dirichlet or uncorrected pressure
  * sources, directivity, smoothing of c0.
  * ====================================================================================== */
 int kwref_adjoint(const kw_sim_desc* d, const double* data, int nthreads, double* misfit, double* grad_c0,
-                  double* grad_p0) {
+                  double* grad_p0, double* grad_rho0) {
     if (!d || !data) { g_err = "null argument"; return KW_ERR_INVALID; }
 #ifdef _OPENMP
     if (nthreads > 0) omp_set_num_threads(nthreads);
@@ -1188,6 +1200,8 @@ int kwref_adjoint(const kw_sim_desc* d, const double* data, int nthreads, double
     }
     if (m.directivity) { g_err = "adjoint: directivity is not supported"; return KW_ERR_UNSUPPORTED; }
     if (d->smooth_c0 && d->sound_speed.len > 1) { g_err = "adjoint: smoothC0 is not supported"; return KW_ERR_UNSUPPORTED; }
+    if (grad_rho0 && d->smooth_rho0 && d->density.len > 1) { g_err = "adjoint: grad_rho0 with smoothRho0 is not supported"; return KW_ERR_UNSUPPORTED; }
+    const bool want_rho = grad_rho0 != nullptr;
     if (!m.haveSampler || m.nPts == 0) { g_err = "adjoint: a sensor is required"; return KW_ERR_INVALID; }
     const Shape& s = m.s;
     const size_t N = m.N;
@@ -1204,7 +1218,7 @@ int kwref_adjoint(const kw_sim_desc* d, const double* data, int nthreads, double
         P[t] = st.p;
         Ssum[t] = st.rhoTot;
         Div[t] = st.divU;
-        if (m.nonlinear) DU[t] = st.dU;
+        if (m.nonlinear || want_rho) DU[t] = st.dU;
         sample_field(m, st.p, Y[t]);
     }
     double L = 0;
@@ -1219,6 +1233,13 @@ int kwref_adjoint(const kw_sim_desc* d, const double* data, int nthreads, double
 
     // ---- reverse sweep ----
     vecd gc(N, 0.0), lp(N, 0.0), tmp, tmp2;
+    // dL/drho0 (direct terms) and dL/d(dt / rho_sg_a) per axis
+    vecd gr(want_rho ? N : 0, 0.0);
+    std::vector<vecd> gdtor(want_rho ? ndim : 0, vecd(N, 0.0));
+    // D+_a p (kappa included), the velocity update's derivative of a pressure field
+    auto grad_p = [&](const vecd& p, int a, vecd& out) {
+        apply_op(m, p, out, [&](size_t i) { return m.ddPos[a][s.idx(i, a)] * m.kappa[i]; });
+    };
     std::vector<vecd> lu(ndim, vecd(N, 0.0)), lr(ndim, vecd(N, 0.0));
     const double y = m.y;
     auto scatter_residual = [&](int t) {
@@ -1253,6 +1274,11 @@ int kwref_adjoint(const kw_sim_desc* d, const double* data, int nthreads, double
             gc[i] += lp[i] * dpdc;
             lE[i] = m.c2[i] * lp[i];
             lS[i] = lE[i] + (m.nonlinear ? lE[i] * m.bona[i] * S[i] / m.rho0[i] : 0.0);
+            // d p / d rho0: B/A S^2 / (2 rho0) and, for Stokes, c^2 tau rho0 div
+            if (want_rho) {
+                if (m.nonlinear) gr[i] -= lE[i] * m.bona[i] * S[i] * S[i] / (2.0 * m.rho0[i] * m.rho0[i]);
+                if (m.absorb && m.stokes) gr[i] += lE[i] * m.tau[i] * Div[t][i];
+            }
         }
         if (m.dispersion) {
             vecd x(N);
@@ -1268,6 +1294,9 @@ int kwref_adjoint(const kw_sim_desc* d, const double* data, int nthreads, double
                 for (size_t i = 0; i < N; ++i) x[i] = m.tau[i] * lE[i];
                 apply_op(m, x, tmp, [&](size_t i) { return cd(m.nabla1[i], 0.0); });
                 for (size_t i = 0; i < N; ++i) lDiv[i] = m.rho0[i] * tmp[i];
+                // the absorption input rho0 div
+                if (want_rho)
+                    for (size_t i = 0; i < N; ++i) gr[i] += tmp[i] * Div[t][i];
             }
         }
         // adjoint of the split densities after the source
@@ -1295,6 +1324,7 @@ int kwref_adjoint(const kw_sim_desc* d, const double* data, int nthreads, double
                 const double pm = m.pml[a][s.idx(i, a)];
                 lDu[a][i] = lDiv[i] - pm * m.dtRho0[i] * nl * Lam[a][i];
                 if (m.nonlinear) lSprev[i] += -2.0 * m.dt * pm * DU[t][a][i] * Lam[a][i];
+                if (want_rho) gr[i] -= pm * m.dt * DU[t][a][i] * Lam[a][i];   // d(dt rho0 nl)/d rho0 = dt
             }
             for (int a = 0; a < ndim; ++a) {
                 const double pm = m.pml[a][s.idx(i, a)];
@@ -1310,6 +1340,10 @@ int kwref_adjoint(const kw_sim_desc* d, const double* data, int nthreads, double
         vecd lpNew(N, 0.0);
         for (int a = 0; a < ndim; ++a) {
             vecd x(N);
+            if (want_rho && t > 0) {   // d u_a / d(dt / rho_sg_a) = -sg D+_a p(t-1); p(-1) = 0
+                grad_p(P[t - 1], a, tmp2);
+                for (size_t i = 0; i < N; ++i) gdtor[a][i] -= m.pmlSg[a][s.idx(i, a)] * tmp2[i] * lu[a][i];
+            }
             for (size_t i = 0; i < N; ++i) {
                 const double sg = m.pmlSg[a][s.idx(i, a)];
                 x[i] = -sg * m.dtOverRho[a][i] * lu[a][i];
@@ -1333,6 +1367,10 @@ int kwref_adjoint(const kw_sim_desc* d, const double* data, int nthreads, double
         }
         for (int a = 0; a < ndim; ++a) {
             vecd x(N);
+            if (want_rho) {   // u_a = (dt / rho_sg_a) / 2 D+_a p0
+                grad_p(m.p0f, a, tmp2);
+                for (size_t i = 0; i < N; ++i) gdtor[a][i] += 0.5 * tmp2[i] * lu[a][i];
+            }
             for (size_t i = 0; i < N; ++i) x[i] = m.dtOverRho[a][i] / 2.0 * lu[a][i];
             apply_op(m, x, tmp, [&](size_t i) { return std::conj(m.ddPos[a][s.idx(i, a)]) * m.kappa[i]; });
             for (size_t i = 0; i < N; ++i) gp[i] += tmp[i];
@@ -1340,6 +1378,21 @@ int kwref_adjoint(const kw_sim_desc* d, const double* data, int nthreads, double
     }
     if (grad_c0) for (size_t i = 0; i < N; ++i) grad_c0[i] = gc[i];
     if (grad_p0) for (size_t i = 0; i < N; ++i) grad_p0[i] = gp[i];
+    if (want_rho) {
+        // dt / rho_sg: d/d rho_sg = -(dt / rho_sg)^2 / dt; rho_sg_a[i] = (rho0[i] + rho0[i + e_a]) / 2,
+        // the last index along a replicated (staggerDensity, KSFO:799-806)
+        for (int a = 0; a < ndim; ++a) {
+            const size_t stride = s.stride[a];
+            const int na = s.n[a];
+            for (size_t i = 0; i < N; ++i) {
+                const double q = m.dtOverRho[a][i];
+                const double g = -gdtor[a][i] * q * q / m.dt;
+                if (s.idx(i, a) == na - 1) gr[i] += g;
+                else { gr[i] += 0.5 * g; gr[i + stride] += 0.5 * g; }
+            }
+        }
+        for (size_t i = 0; i < N; ++i) grad_rho0[i] = gr[i];
+    }
     return KW_OK;
 }
 

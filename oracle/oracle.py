@@ -31,6 +31,8 @@ def lib():
         L = C.CDLL(LIB)
         L.kwref_run.restype = C.c_int
         L.kwref_run.argtypes = [C.POINTER(abi.kw_sim_desc), C.c_int, C.c_int, C.POINTER(C.c_void_p)]
+        L.kwref_run_timed.restype = C.c_int
+        L.kwref_run_timed.argtypes = [C.POINTER(abi.kw_sim_desc), C.c_int, C.c_int, C.c_int, C.POINTER(C.c_void_p)]
         L.kwref_output_size.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_size_t)]
         L.kwref_get_output.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_double), C.c_size_t]
         L.kwref_free.argtypes = [C.c_void_p]
@@ -46,7 +48,8 @@ def lib():
         L.kwref_smoothing_window.argtypes = [C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_double)]
         L.kwref_adjoint.restype = C.c_int
         L.kwref_adjoint.argtypes = [C.POINTER(abi.kw_sim_desc), C.POINTER(C.c_double), C.c_int,
-                                    C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_double)]
+                                    C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_double),
+                                    C.POINTER(C.c_double)]
         L.kwref_db2neper.restype = C.c_double
         L.kwref_db2neper.argtypes = [C.c_double, C.c_double]
         _lib = L
@@ -61,14 +64,15 @@ def _dp(a):
     return a.ctypes.data_as(C.POINTER(C.c_double))
 
 
-def run(builder, nthreads: int = 0, max_steps: int = -1):
+def run(builder, nthreads: int = 0, max_steps: int = -1, timed_from: int = 0):
     """Run the oracle on a kwave.DescBuilder; returns (dict of float64 outputs, loop seconds)
-    (kspaceFirstOrderAS when the descriptor's axisymmetric flag is set)."""
+    (kspaceFirstOrderAS when the descriptor's axisymmetric flag is set). The loop seconds cover
+    the time steps from `timed_from` on (the earlier ones are untimed warm-up steps)."""
     from kwave import abi
     from kwave.api import output_shape
     L = lib()
     h = C.c_void_p()
-    st = L.kwref_run(C.byref(builder.desc), int(nthreads), int(max_steps), C.byref(h))
+    st = L.kwref_run_timed(C.byref(builder.desc), int(nthreads), int(max_steps), int(timed_from), C.byref(h))
     if st != 0:
         raise OracleError(f"status {st}: {L.kwref_last_error().decode()}")
     try:
@@ -97,18 +101,23 @@ def run(builder, nthreads: int = 0, max_steps: int = -1):
         L.kwref_free(h)
 
 
-def adjoint(builder, data: np.ndarray, nthreads: int = 0):
+def adjoint(builder, data: np.ndarray, nthreads: int = 0, grad_rho0: bool = False):
     """FP64 discrete adjoint: (misfit, dL/dc0, dL/dp0) of L = 1/2 sum (p_sensor - data)^2, with
-    `data` shaped like the p series [n_sensor, nt]."""
+    `data` shaped like the p series [n_sensor, nt]; with grad_rho0, (misfit, dL/dc0, dL/dp0,
+    dL/drho0)."""
     L = lib()
     d = np.ascontiguousarray(data, dtype=np.float64)
     shape = builder.shape
     gc = np.zeros(int(np.prod(shape)))
     gp = np.zeros(int(np.prod(shape)))
+    gr = np.zeros(int(np.prod(shape))) if grad_rho0 else None
     mis = C.c_double()
-    st = L.kwref_adjoint(C.byref(builder.desc), _dp(d), int(nthreads), C.byref(mis), _dp(gc), _dp(gp))
+    st = L.kwref_adjoint(C.byref(builder.desc), _dp(d), int(nthreads), C.byref(mis), _dp(gc), _dp(gp),
+                         _dp(gr) if grad_rho0 else None)
     if st != 0:
         raise OracleError(f"status {st}: {L.kwref_last_error().decode()}")
+    if grad_rho0:
+        return mis.value, gc.reshape(shape), gp.reshape(shape), gr.reshape(shape)
     return mis.value, gc.reshape(shape), gp.reshape(shape)
 
 

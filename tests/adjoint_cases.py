@@ -8,17 +8,23 @@ from kwave import (AbsorptionMode, DescBuilder, KWaveGrid, KWaveMedium, KWaveSen
 DT = 1.5e-8
 
 
-def builder(shape, c, p0, absorb="none", nonlinear=False, source=True, cartesian=True, nt=50, seed=1):
-    """Heterogeneous medium (fixed seed), optional power-law / Stokes absorption and B/A, an initial
-    pressure p0 (or None) and an additive line source, a Cartesian ring or binary sensor row."""
-    dim = len(shape)
+def density(shape, seed=1):
+    """The heterogeneous density of `builder` (fixed seed)."""
     rng = np.random.default_rng(seed)
+    return (1000 + 30 * rng.standard_normal(shape)).astype(np.float32)
+
+
+def builder(shape, c, p0, absorb="none", nonlinear=False, source=True, cartesian=True, nt=50, seed=1, rho=None):
+    """Heterogeneous medium (fixed seed, or the density `rho`), optional power-law / Stokes
+    absorption and B/A, an initial pressure p0 (or None) and an additive line source, a Cartesian
+    ring or binary sensor row."""
+    dim = len(shape)
     args = []
     for n in shape:
         args += [n, 1e-4]
     g = KWaveGrid(*args)
     g.setTime(nt, DT)
-    rho = (1000 + 30 * rng.standard_normal(shape)).astype(np.float32)
+    rho = density(shape, seed) if rho is None else np.asarray(rho, np.float32)
     kw = {}
     if absorb == "powerlaw":
         kw = dict(alphaCoeff=0.5, alphaPower=1.5, alphaMode=AbsorptionMode.powerLaw)
@@ -73,12 +79,15 @@ def problem(shape, seed=5, **kw):
 def fd_misfit_diff(shape, c, p0, data, v, eps, which, kw):
     """Central difference L(x + eps v) - L(x - eps v) of the FP64 oracle misfit, with the exact
     float32 perturbation that the descriptor arrays see."""
-    base = c if which == "c" else p0
+    base = c if which == "c" else (p0 if which == "p" else density(shape).astype(np.float64))
     xp = (base + eps * v).astype(np.float32).astype(np.float64)
     xm = (base - eps * v).astype(np.float32).astype(np.float64)
     if which == "c":
         lp = oracle.adjoint(builder(shape, xp, p0, **kw), data)[0]
         lm = oracle.adjoint(builder(shape, xm, p0, **kw), data)[0]
+    elif which == "rho":
+        lp = oracle.adjoint(builder(shape, c, p0, rho=xp, **kw), data)[0]
+        lm = oracle.adjoint(builder(shape, c, p0, rho=xm, **kw), data)[0]
     else:
         lp = oracle.adjoint(builder(shape, c, xp, **kw), data)[0]
         lm = oracle.adjoint(builder(shape, c, xm, **kw), data)[0]

@@ -4,7 +4,7 @@ with them).
 
 Tolerance: relative error of the directional derivative <= 2e-6 against central differences
 extrapolated (Richardson) from steps 0.2 and 0.1 m/s (sound speed), 2 and 1 x 1e3 Pa (initial
-pressure).
+pressure), 0.2 and 0.1 kg/m^3 (density).
 """
 import numpy as np
 import pytest
@@ -36,11 +36,13 @@ def richardson_error(shape, c, p0, data, g, v, eps, which, kw):
 def test_oracle_adjoint_matches_central_differences(shape, kw):
     rng = np.random.default_rng(11)
     c, p0, data, kw = problem(shape, **kw)
-    L, gc, gp = oracle.adjoint(builder(shape, c, p0, **kw), data)
+    L, gc, gp, gr = oracle.adjoint(builder(shape, c, p0, **kw), data, grad_rho0=True)
     assert L > 0
     assert richardson_error(shape, c, p0, data, gc, rng.standard_normal(shape), 0.2, "c", kw) < 2e-6
     if p0 is not None:
         assert richardson_error(shape, c, p0, data, gp, rng.standard_normal(shape) * 1e3, 2.0, "p", kw) < 2e-6
+    # density: steps 0.2 and 0.1 kg/m^3
+    assert richardson_error(shape, c, p0, data, gr, rng.standard_normal(shape), 0.2, "rho", kw) < 2e-6
 
 
 def test_oracle_adjoint_rejects_unsupported_sources():
