@@ -6,7 +6,8 @@
 Default workload: hetero3d_256 — 256^3 heterogeneous (12 spheres) nonlinear (B/A 6) power-law
 absorbing (alpha 0.75, y 1.5) forward with an additive 1 MPa tone-burst plane source and a full
 xy sensor plane recording p and pMax, FP32 on the device. A "step" is one time step of that
-simulation. The metric is grid-point-steps per second over the whole job.
+simulation; the window is steps W .. W+K-1 (K = 20 by default; --steps 0 times the rest of the
+simulation). The metric is grid-point-steps per second over the whole job.
 
 `value`   device throughput: K time steps timed with CUDA events on the library's stream, inputs
           resident in HBM (every field is 67 MB, far above the 126 MB L2 in aggregate).
@@ -16,15 +17,22 @@ simulation. The metric is grid-point-steps per second over the whole job.
           duration per launch, against the measured HBM copy bandwidth of this pool.
 `cpu_baseline` the FP64 oracle (a restatement of the reference's update equations; the Swift/MLX
           reference cannot run here) on this host's cores for a bounded sample of the workload.
-With --gpus N > 1 (torchrun), every rank runs an independent replica (no collective on the data
-path): "scaling": "weak", value = all ranks' grid-point-steps / max-over-ranks time.
+`batched_over_plain` the 64-simulation uneven 2D batch in one engine against the same simulations
+          run one at a time (grid-point-steps/s ratio); `grad_over_forward` the 512^2 adjoint
+          gradient time over the forward time of the same simulation. Both are measured in the same
+          process after the main window (--no-extras skips them).
+--impl reference times the FP64 oracle on the host cores over the same window (W untimed warm-up
+          steps, then K timed ones) and prints the same config.
+With --gpus N > 1 every rank runs an independent replica (no collective on the data path):
+"scaling": "weak", value = all ranks' grid-point-steps / max-over-ranks time. Without torchrun's
+environment, --gpus N > 1 relaunches this script under torch.distributed.run with N local ranks.
 """
 from __future__ import annotations
 
 import argparse
 import json
-import math
 import os
+import socket
 import statistics
 import subprocess
 import sys
@@ -36,6 +44,9 @@ sys.path.insert(0, os.path.join(ROOT, "k-wave-swift_b200"))
 
 METRIC = "grid-pt-steps/s"
 UNIT = "grid-pt-steps/s"
+BATCH = "batch2d_64"
+ADJ = "adjoint2d_512"
+ADJ3 = "adjoint3d_384"
 
 
 def measured_peak_gbs() -> tuple[float, str]:
@@ -105,31 +116,52 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(rows)}
 
 
-def workload(name: str, steps_needed: int):
+def workload(name: str):
     from kwave import workloads
     if name == "hetero3d_256":
-        b = workloads.hetero3d(256)
-    elif name == "hetero3d_128":
-        b = workloads.hetero3d(128)
-    elif name == "ivp2d_128":
-        b = workloads.ivp2d_128()
-    else:
-        raise SystemExit(f"unknown workload {name}")
-    if b.grid.nt < steps_needed:
-        raise SystemExit(f"workload has nt={b.grid.nt} < warmup+steps={steps_needed}")
-    return b
+        return workloads.hetero3d(256)
+    if name == "hetero3d_128":
+        return workloads.hetero3d(128)
+    if name == "ivp2d_128":
+        return workloads.ivp2d_128()
+    raise SystemExit(f"unknown workload {name}")
 
 
-def cpu_sample(builder, steps: int, threads: int) -> dict:
-    """Time the FP64 oracle on this host for `steps` time steps (time loop only)."""
+def window(args, nt: int) -> tuple[int, int]:
+    """(W, K): W untimed warm-up steps, then K timed ones (K = 0 asks for the rest of the run)."""
+    W = args.warmup
+    K = args.steps if args.steps else nt - W
+    if W + K > nt:
+        raise SystemExit(f"workload has nt={nt} < warmup+steps={W + K}")
+    return W, K
+
+
+def forward_config(args, b) -> dict:
+    """The `config` of both arms for the forward workloads (identical dicts)."""
+    hetero = args.workload.startswith("hetero")
+    npts = b.grid.totalGridPoints
+    return {"workload": args.workload, "grid": list(b.grid.shape), "nt": b.grid.nt,
+            "window": "time steps warmup .. warmup+steps-1 of the simulation (source active)" if hetero
+            else "time steps warmup .. warmup+steps-1 of the simulation",
+            "physics": "heterogeneous c0/rho0, power law y=1.5 with dispersion, B/A=6, additive p source"
+            if hetero else "homogeneous IVP",
+            "l2": "inputs larger than L2 (every field >= 67 MB)" if npts >= 2 ** 24 else "small grid",
+            "parallelism": f"replicas{args.gpus}"}
+
+
+def cpu_sample(builder, warm: int, steps: int, threads: int) -> dict:
+    """Time the FP64 oracle on this host: `warm` untimed steps, then `steps` timed ones."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle
-    _, loop_s = oracle.run(builder, nthreads=threads, max_steps=steps)
+    _, loop_s = oracle.run(builder, nthreads=threads, max_steps=warm + steps, timed_from=warm)
     n = builder.grid.totalGridPoints
     return {"value": n * steps / loop_s, "unit": UNIT, "cores": threads, "kind": "port",
             "seconds": loop_s, "steps": steps}
 
 
+# ---------------------------------------------------------------------------------------------
+# reference arm: the FP64 oracle (the reference's update equations) on the host cores
+# ---------------------------------------------------------------------------------------------
 def run_reference(args) -> None:
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -139,24 +171,20 @@ def run_reference(args) -> None:
         return run_reference_batch(args, threads)
     if args.workload in (ADJ, ADJ3):
         return run_reference_adjoint(args, threads)
-    b = workload(args.workload, 1)
-    steps = max(1, min(args.steps or args.ref_steps, args.ref_steps))
-    r = cpu_sample(b, steps, threads)
-    sample = (f"{args.workload}: first {steps} time step(s) of the workload (additive source active, "
-              f"power law + B/A) in FP64 on {threads} threads; time loop only")
+    b = workload(args.workload)
+    W, K = window(args, b.grid.nt)
+    r = cpu_sample(b, W, K, threads)
+    sample = (f"{args.workload}: time steps {W} .. {W + K - 1} of the workload after {W} untimed warm-up "
+              f"steps, FP64 oracle on {threads} threads, time loop only")
     line = {
         "impl": "reference", "metric": METRIC, "value": r["value"], "unit": UNIT, "n_gpus": args.gpus,
-        "steps": steps, "warmup": 0, "ms_per_step": 1e3 * r["seconds"] / steps, "higher_is_better": True,
+        "steps": K, "warmup": W, "ms_per_step": 1e3 * r["seconds"] / K, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": args.workload, "grid": list(b.grid.shape), "nt": b.grid.nt,
-                   "l2": "inputs larger than L2"},
+        "config": forward_config(args, b),
         "cpu_baseline": {"value": r["value"], "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
         "e2e": {"value": r["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
-
-
-BATCH = "batch2d_64"
 
 
 def run_reference_batch(args, threads: int) -> None:
@@ -165,13 +193,13 @@ def run_reference_batch(args, threads: int) -> None:
     from kwave import workloads
     builders = workloads.batch2d()
     seen, work, secs = set(), 0.0, 0.0
-    steps = max(1, min(args.steps or args.ref_steps, args.ref_steps)) * 5
+    steps = max(1, args.steps or 20) * 5
     for b in builders:
         n = b.grid.shape[0]
         if n in seen:
             continue
         seen.add(n)
-        r = cpu_sample(b, steps, threads)
+        r = cpu_sample(b, 0, steps, threads)
         work += b.grid.totalGridPoints * steps
         secs += r["seconds"]
     value = work / secs
@@ -179,7 +207,7 @@ def run_reference_batch(args, threads: int) -> None:
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
         "steps": steps, "warmup": 0, "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": BATCH, "sims": len(builders), "sizes": sorted(seen), "l2": "small grids (L2-resident)"},
+        "config": batch_config(args, builders),
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
                          "sample": f"first {steps} steps of one simulation per grid size {sorted(seen)}, FP64, "
                                    f"{threads} threads, time loop only"},
@@ -188,113 +216,14 @@ def run_reference_batch(args, threads: int) -> None:
     print(json.dumps(line), flush=True)
 
 
-def run_batch(args) -> None:
-    """C3: 64 independent uneven 2D forwards, all in one engine (one launch per pass and size class,
-    the steady step a CUDA graph) against the same 64 run one after another through the
-    single-simulation path. Work = sum over simulations of grid points x time steps."""
-    import torch
-
-    from kwave import workloads
-    from kwave.runtime import Context
-
-    from kwave import replicas
-    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
-    rep = replicas.init("nccl")   # one replica per GPU; no collective on the data path
-    world, rank, local = rep.world, rep.rank, rep.local
-    builders = workloads.batch2d()
-    W = args.warmup
-    work = float(sum(b.grid.totalGridPoints * b.grid.nt for b in builders))
-    ctx = Context(local)
-    stream = torch.cuda.Stream()
-    torch.cuda.set_stream(stream)
-    ctx.set_stream(stream.cuda_stream)
-
-    def ev():
-        return torch.cuda.Event(enable_timing=True)
-
-    # batched: warm up W steps, restart, then time the whole batch (max nt steps)
-    batch = ctx.create_batch(builders)
-    batch.step(W)
-    batch.reset()
-    torch.cuda.synchronize()
-    rep.barrier()
-    gpu_id = "GPU-" + str(torch.cuda.get_device_properties(local).uuid)
-    steps = max(b.grid.nt for b in builders)
-    e0, e1 = ev(), ev()
-    with ClockSampler(gpu_id) as clk:
-        e0.record(stream)
-        batch.step(steps)
-        e1.record(stream)
-        torch.cuda.synchronize()
-    ms_batch = e0.elapsed_time(e1)
-    batch.close()
-
-    # plain: one simulation at a time (each warmed up W steps, reset, then timed over its nt steps)
-    ms_plain = 0.0
-    for b in builders:
-        sim = ctx.create_sim(b)
-        sim.step(W)
-        sim.reset()
-        torch.cuda.synchronize()
-        a, z = ev(), ev()
-        a.record(stream)
-        sim.step(b.grid.nt)
-        z.record(stream)
-        torch.cuda.synchronize()
-        ms_plain += a.elapsed_time(z)
-        sim.close()
-
-    # end to end through the public API from host buffers: create + run + sensor data, batched
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    batch = ctx.create_batch(builders)
-    batch.run()
-    outs = [batch.output(i, "p", b.grid.nt, 256) for i, b in enumerate(builders)]
-    t1 = time.perf_counter()
-    batch.close()
-    h2d = sum(sum(a.nbytes for a in b.keep) for b in builders)
-    d2h = sum(o.nbytes for o in outs if o is not None)
-
-    ms_batch = rep.max_over_ranks(ms_batch, device="cuda")
-    ms_plain = rep.max_over_ranks(ms_plain, device="cuda")
-    if rank == 0:
-        peak, peak_kind = measured_peak_gbs()
-        sizes = sorted({b.grid.shape[0] for b in builders})
-        value = work * world / (ms_batch / 1e3)
-        line = {
-            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": steps, "warmup": W,
-            "ms_per_step": ms_batch / steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f32", "data": "synthetic",
-            "config": {"workload": BATCH, "sims": len(builders), "sizes": sizes,
-                       "grid_pt_steps": work, "l2": "small grids (each simulation's fields are L2-resident)",
-                       "parallelism": f"replicas{world}"},
-            "plain": {"value": work * world / (ms_plain / 1e3), "unit": UNIT, "ms": ms_plain,
-                      "what": "the same simulations run one after another through the single-simulation path"},
-            "batched_over_plain": ms_plain / ms_batch,
-            "roofline": None,
-            "cpu_baseline": None,
-            "e2e": {"value": work * world / (t1 - t0), "unit": UNIT, "h2d_bytes_per_step": h2d / steps,
-                    "d2h_bytes_per_step": d2h / steps, "seconds": t1 - t0},
-            "clocks": clk.summary(),
-            "peak_gbs": peak, "peak_source": peak_kind,
-        }
-        print(json.dumps(line), flush=True)
-    ctx.close()
-    rep.close()
-
-
-ADJ = "adjoint2d_512"
-ADJ3 = "adjoint3d_384"
-
-
 def run_reference_adjoint(args, threads: int) -> None:
     """The FP64 oracle adjoint (forward + reverse) on this host over a bounded sample: the first
-    steps of the same 512^2 problem."""
+    steps of the same problem."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle
     from kwave import workloads
     three_d = args.workload == ADJ3
-    steps = 2 if three_d else max(2, min(args.steps or args.ref_steps, args.ref_steps) * 2)
+    steps = 2 if three_d else max(2, (args.steps or 20) // 5)
     bp, bt = workloads.adjoint3d(384, steps) if three_d else workloads.adjoint2d(512, steps)
     data, _ = oracle.run(bt, nthreads=threads)
     t0 = time.perf_counter()
@@ -305,8 +234,7 @@ def run_reference_adjoint(args, threads: int) -> None:
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": steps,
         "warmup": 0, "ms_per_step": 1e3 * secs / steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": args.workload, "grid": list(bp.shape),
-                   "what": "misfit gradient (forward + adjoint) per time step"},
+        "config": adjoint_config(args, bp),
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
                          "sample": f"first {steps} steps of the {args.workload} problem: FP64 oracle forward + "
                                    f"discrete adjoint, {threads} threads"},
@@ -315,30 +243,113 @@ def run_reference_adjoint(args, threads: int) -> None:
     print(json.dumps(line), flush=True)
 
 
-def run_adjoint(args) -> None:
-    """C4: the sound-speed gradient of a 512^2 sensor-data misfit by the discrete adjoint with
-    sqrt(nt) checkpointing, against the forward run of the same simulation. Value = grid points x
-    time steps / gradient time (forward with checkpoints + reverse sweep with recompute)."""
+# ---------------------------------------------------------------------------------------------
+# GPU arm
+# ---------------------------------------------------------------------------------------------
+def _gpu_setup():
+    import torch
+
+    from kwave import replicas
+    from kwave.runtime import Context
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    rep = replicas.init("nccl")   # one replica per GPU; no collective on the data path
+    ctx = Context(rep.local)
+    # a dedicated (non-default) stream shared by the library and the CUDA events
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    ctx.set_stream(stream.cuda_stream)
+    try:
+        gpu_id = "GPU-" + str(torch.cuda.get_device_properties(rep.local).uuid)
+    except Exception:
+        gpu_id = str(rep.local)
+    return rep, ctx, stream, gpu_id
+
+
+def _event():
+    import torch
+    return torch.cuda.Event(enable_timing=True)
+
+
+def batch_config(args, builders) -> dict:
+    return {"workload": BATCH, "sims": len(builders), "sizes": sorted({b.grid.shape[0] for b in builders}),
+            "grid_pt_steps": float(sum(b.grid.totalGridPoints * b.grid.nt for b in builders)),
+            "l2": "small grids (each simulation's fields are L2-resident)", "parallelism": f"replicas{args.gpus}"}
+
+
+def measure_batch(ctx, stream, rep, W: int, clk=None) -> dict:
+    """C3: 64 independent uneven 2D forwards in one engine (one launch per pass and size class, the
+    steady step a CUDA graph) against the same 64 run one after another through the
+    single-simulation path. Work = sum over simulations of grid points x time steps."""
+    import torch
+
+    from kwave import workloads
+    builders = workloads.batch2d()
+    work = float(sum(b.grid.totalGridPoints * b.grid.nt for b in builders))
+    batch = ctx.create_batch(builders)
+    batch.step(W)
+    batch.reset()
+    torch.cuda.synchronize()
+    rep.barrier()
+    steps = max(b.grid.nt for b in builders)
+    e0, e1 = _event(), _event()
+    e0.record(stream)
+    batch.step(steps)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms_batch = e0.elapsed_time(e1)
+    batch.close()
+    ms_plain = 0.0
+    for b in builders:
+        sim = ctx.create_sim(b)
+        sim.step(W)
+        sim.reset()
+        torch.cuda.synchronize()
+        a, z = _event(), _event()
+        a.record(stream)
+        sim.step(b.grid.nt)
+        z.record(stream)
+        torch.cuda.synchronize()
+        ms_plain += a.elapsed_time(z)
+        sim.close()
+    # end to end through the public API from host buffers: create + run + sensor data, batched
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    batch = ctx.create_batch(builders)
+    batch.run()
+    outs = [batch.output(i, "p", b.grid.nt, 256) for i, b in enumerate(builders)]
+    t1 = time.perf_counter()
+    batch.close()
+    ms_batch = rep.max_over_ranks(ms_batch, device="cuda")
+    ms_plain = rep.max_over_ranks(ms_plain, device="cuda")
+    return {"builders": builders, "work": work, "steps": steps, "ms_batch": ms_batch, "ms_plain": ms_plain,
+            "e2e_s": t1 - t0, "h2d": sum(sum(a.nbytes for a in b.keep) for b in builders),
+            "d2h": sum(o.nbytes for o in outs if o is not None)}
+
+
+def adjoint_config(args, bp) -> dict:
+    three_d = len(bp.shape) == 3
+    nt = bp.grid.nt
+    if three_d:
+        return {"workload": ADJ3, "grid": list(bp.shape), "nt": nt, "sensor": "128x128 receive plane",
+                "physics": "3 layers + 8 spheres, power law y=1.5 with dispersion, B/A=5, focused 32x32 array",
+                "l2": "inputs larger than L2", "parallelism": f"replicas{args.gpus}"}
+    return {"workload": ADJ, "grid": list(bp.shape), "nt": nt, "sensor": "512-point Cartesian ring",
+            "physics": "power law y=1.1 with dispersion, heterogeneous c0, p0",
+            "l2": "small grid (fields L2-resident)", "parallelism": f"replicas{args.gpus}"}
+
+
+def measure_adjoint(ctx, stream, rep, W: int, three_d: bool, adjoint_nt: int = 0, store_all: bool = True) -> dict:
+    """C4 / C5: the sound-speed gradient of a sensor-data misfit by the discrete adjoint against the
+    forward run of the same simulation."""
     import numpy as np
     import torch
 
     from kwave import abi, workloads
-    from kwave.runtime import Context
-
-    from kwave import replicas
-    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
-    rep = replicas.init("nccl")   # one replica per GPU; no collective on the data path
-    world, rank, local = rep.world, rep.rank, rep.local
-    three_d = args.workload == ADJ3
-    if args.adjoint_nt:   # a shorter run of the same configuration (profiling captures)
-        bp, bt = workloads.adjoint3d(384, args.adjoint_nt) if three_d else workloads.adjoint2d(512, args.adjoint_nt)
+    if adjoint_nt:   # a shorter run of the same configuration (profiling captures)
+        bp, bt = workloads.adjoint3d(384, adjoint_nt) if three_d else workloads.adjoint2d(512, adjoint_nt)
     else:
         bp, bt = workloads.adjoint3d() if three_d else workloads.adjoint2d()
     nt, npts = bp.grid.nt, bp.grid.totalGridPoints
-    ctx = Context(local)
-    stream = torch.cuda.Stream()
-    torch.cuda.set_stream(stream)
-    ctx.set_stream(stream.cuda_stream)
     # observed data: the forward run at the true sound speed
     sim = ctx.create_sim(bt)
     sim.run()
@@ -346,59 +357,87 @@ def run_adjoint(args) -> None:
     sim.close()
     # forward time of the perturbed model (warm-up, restart, the whole run)
     sim = ctx.create_sim(bp)
-    sim.step(args.warmup)
+    sim.step(W)
     sim.reset()
     torch.cuda.synchronize()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    gpu_id = "GPU-" + str(torch.cuda.get_device_properties(local).uuid)
-    with ClockSampler(gpu_id) as clk:
-        e0.record(stream)
-        sim.step(nt)
-        e1.record(stream)
-        torch.cuda.synchronize()
-        fwd_ms = e0.elapsed_time(e1)
-        sim.close()
-        if three_d:
-            # the checkpoint schedule sized to the free device memory (less room for the
-            # simulation's own fields and the adjoint's work fields)
-            torch.cuda.empty_cache()
-            free, _ = torch.cuda.mem_get_info()
-            budget = free - 40 * npts * 4 - (4 << 30)
-            opts = dict(policy=abi.KW_CHECKPOINT_BUDGET, memory_budget=float(budget))
-        else:
-            opts = dict(policy=abi.KW_CHECKPOINT_SQRT)
-            ctx.adjoint(bp, data, **opts)   # warm-up of the adjoint path
-        t0 = time.perf_counter()
-        r = ctx.adjoint(bp, data, **opts)
-        e2e_s = time.perf_counter() - t0
-        r_all = None if three_d else ctx.adjoint(bp, data, policy=abi.KW_CHECKPOINT_STORE_ALL)
+    e0, e1 = _event(), _event()
+    e0.record(stream)
+    sim.step(nt)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    fwd_ms = e0.elapsed_time(e1)
+    sim.close()
+    if three_d:
+        # the checkpoint schedule sized to the free device memory (less room for the simulation's
+        # own fields and the adjoint's work fields)
+        torch.cuda.empty_cache()
+        free, _ = torch.cuda.mem_get_info()
+        budget = free - 40 * npts * 4 - (4 << 30)
+        opts = dict(policy=abi.KW_CHECKPOINT_BUDGET, memory_budget=float(budget))
+    else:
+        opts = dict(policy=abi.KW_CHECKPOINT_SQRT)
+        ctx.adjoint(bp, data, **opts)   # warm-up of the adjoint path
+    t0 = time.perf_counter()
+    r = ctx.adjoint(bp, data, **opts)
+    e2e_s = time.perf_counter() - t0
+    r_all = ctx.adjoint(bp, data, policy=abi.KW_CHECKPOINT_STORE_ALL) if (store_all and not three_d) else None
     grad_ms = r["forward_ms"] + r["reverse_ms"]
     all_ms = r_all["forward_ms"] + r_all["reverse_ms"] if r_all else None
     grad_ms = rep.max_over_ranks(grad_ms, device="cuda")
     fwd_ms = rep.max_over_ranks(fwd_ms, device="cuda")
-    if rank == 0:
-        g = r["grad_c0"]
+    g = r["grad_c0"]
+    return {"bp": bp, "nt": nt, "npts": npts, "fwd_ms": fwd_ms, "grad_ms": grad_ms, "all_ms": all_ms, "r": r,
+            "e2e_s": e2e_s, "grad_c0_l2": float(np.sqrt(np.sum(g.astype(np.float64) ** 2))),
+            "h2d": sum(a.nbytes for a in bp.keep) + data.nbytes, "d2h": g.nbytes + npts * 4}
+
+
+def run_batch(args) -> None:
+    rep, ctx, stream, gpu_id = _gpu_setup()
+    with ClockSampler(gpu_id) as clk:
+        m = measure_batch(ctx, stream, rep, args.warmup)
+    if rep.rank == 0:
+        world, steps, work = rep.world, m["steps"], m["work"]
         line = {
-            "metric": METRIC, "value": npts * nt * world / (grad_ms / 1e3), "unit": UNIT, "n_gpus": world,
-            "steps": nt, "warmup": args.warmup, "ms_per_step": grad_ms / nt, "higher_is_better": True,
+            "metric": METRIC, "value": work * world / (m["ms_batch"] / 1e3), "unit": UNIT, "n_gpus": world,
+            "steps": steps, "warmup": args.warmup, "ms_per_step": m["ms_batch"] / steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": ({"workload": ADJ3, "grid": list(bp.shape), "nt": nt, "sensor": "128x128 receive plane",
-                        "physics": "3 layers + 8 spheres, power law y=1.5 with dispersion, B/A=5, focused 32x32 array",
-                        "l2": "inputs larger than L2", "parallelism": f"replicas{world}"} if three_d else
-                       {"workload": ADJ, "grid": [512, 512], "nt": nt, "sensor": "512-point Cartesian ring",
-                        "physics": "power law y=1.1 with dispersion, heterogeneous c0, p0",
-                        "l2": "small grid (fields L2-resident)", "parallelism": f"replicas{world}"}),
-            "grad_over_forward": grad_ms / fwd_ms,
-            "forward_ms": fwd_ms,
+            "config": batch_config(args, m["builders"]),
+            "plain": {"value": work * world / (m["ms_plain"] / 1e3), "unit": UNIT, "ms": m["ms_plain"],
+                      "what": "the same simulations run one after another through the single-simulation path"},
+            "batched_over_plain": m["ms_plain"] / m["ms_batch"],
+            "roofline": None, "cpu_baseline": None,
+            "e2e": {"value": work * world / m["e2e_s"], "unit": UNIT, "h2d_bytes_per_step": m["h2d"] / steps,
+                    "d2h_bytes_per_step": m["d2h"] / steps, "seconds": m["e2e_s"]},
+            "clocks": clk.summary(),
+        }
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    rep.close()
+
+
+def run_adjoint(args) -> None:
+    rep, ctx, stream, gpu_id = _gpu_setup()
+    three_d = args.workload == ADJ3
+    with ClockSampler(gpu_id) as clk:
+        m = measure_adjoint(ctx, stream, rep, args.warmup, three_d, args.adjoint_nt)
+    if rep.rank == 0:
+        world, nt, npts, r = rep.world, m["nt"], m["npts"], m["r"]
+        line = {
+            "metric": METRIC, "value": npts * nt * world / (m["grad_ms"] / 1e3), "unit": UNIT, "n_gpus": world,
+            "steps": nt, "warmup": args.warmup, "ms_per_step": m["grad_ms"] / nt, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": adjoint_config(args, m["bp"]),
+            "grad_over_forward": m["grad_ms"] / m["fwd_ms"],
+            "forward_ms": m["fwd_ms"],
             "gradient_ms": {"checkpointed_forward": r["forward_ms"], "reverse_sweep": r["reverse_ms"]},
             "checkpointing": {"policy": "memory budget" if three_d else "sqrt(nt)", "interval": r["interval"],
                               "checkpoints": r["checkpoints"]},
-            "store_all": {"gradient_ms": all_ms, "grad_over_forward": all_ms / fwd_ms} if all_ms else None,
-            "misfit": r["misfit"], "grad_c0_l2": float(np.sqrt(np.sum(g.astype(np.float64) ** 2))),
+            "store_all": {"gradient_ms": m["all_ms"], "grad_over_forward": m["all_ms"] / m["fwd_ms"]}
+            if m["all_ms"] else None,
+            "misfit": r["misfit"], "grad_c0_l2": m["grad_c0_l2"],
             "roofline": None, "cpu_baseline": None,
-            "e2e": {"value": npts * nt * world / e2e_s, "unit": UNIT,
-                    "h2d_bytes_per_step": (sum(a.nbytes for a in bp.keep) + data.nbytes) / nt,
-                    "d2h_bytes_per_step": g.nbytes / nt + npts * 4 / nt, "seconds": e2e_s},
+            "e2e": {"value": npts * nt * world / m["e2e_s"], "unit": UNIT,
+                    "h2d_bytes_per_step": m["h2d"] / nt, "d2h_bytes_per_step": m["d2h"] / nt, "seconds": m["e2e_s"]},
             "clocks": clk.summary(),
         }
         print(json.dumps(line), flush=True)
@@ -407,36 +446,19 @@ def run_adjoint(args) -> None:
 
 
 def run_ours(args) -> None:
-    import numpy as np
     import torch
-
-    from kwave.runtime import Context
-
-    from kwave import replicas
-    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
-    rep = replicas.init("nccl")   # one replica per GPU; no collective on the data path
-    world, rank, local = rep.world, rep.rank, rep.local
-    W = args.warmup
-    b = workload(args.workload, (args.steps or 1) + W)
-    # default: the whole simulation (every time step after the warm-up ones)
-    K = args.steps if args.steps else b.grid.nt - W
+    rep, ctx, stream, gpu_id = _gpu_setup()
+    world, rank = rep.world, rep.rank
+    b = workload(args.workload)
+    W, K = window(args, b.grid.nt)
     npts = b.grid.totalGridPoints
 
-    ctx = Context(local)
-    # a dedicated (non-default) stream shared by the library and the CUDA events below
-    stream = torch.cuda.Stream()
-    torch.cuda.set_stream(stream)
-    ctx.set_stream(stream.cuda_stream)
     sim = ctx.create_sim(b)
     sim.step(W)
     torch.cuda.synchronize()
-    try:
-        gpu_id = "GPU-" + str(torch.cuda.get_device_properties(local).uuid)
-    except Exception:
-        gpu_id = str(local)
     rep.barrier()
     torch.cuda.synchronize()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0, e1 = _event(), _event()
     with ClockSampler(gpu_id) as clk:
         e0.record(stream)
         sim.step(K)
@@ -444,12 +466,11 @@ def run_ours(args) -> None:
         torch.cuda.synchronize()
     rep.barrier()
     torch.cuda.synchronize()
-    ms = e0.elapsed_time(e1)
-    ms = rep.max_over_ranks(ms, device="cuda")
+    ms = rep.max_over_ranks(e0.elapsed_time(e1), device="cuda")
     value = npts * K * world / (ms / 1e3)
 
     # per-launch device profile of a step, taken on a restarted run right after its warm-up steps
-    # (source still active; not part of `value`)
+    # (the same steps as the window's start; not part of `value`)
     sim.reset()
     sim.step(W)
     prof = sim.profile_step(3)
@@ -463,16 +484,15 @@ def run_ours(args) -> None:
         g["launches"] += 1
     # the dominant kernel: the single launch of a step with the longest device time
     top = max(prof, key=lambda k: k["ms"])
-    dom_name, dom = top["name"], {"ms": top["ms"], "bytes": top["bytes"]}
     peak, peak_kind = measured_peak_gbs()
-    achieved = dom["bytes"] / (dom["ms"] / 1e3) / 1e9 if dom["ms"] > 0 else 0.0
+    achieved = top["bytes"] / (top["ms"] / 1e3) / 1e9 if top["ms"] > 0 else 0.0
     step_bytes = sum(k["bytes"] for k in prof)
     step_ms = sum(k["ms"] for k in prof)
     traffic = None
     tfile = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(tfile):
         try:
-            traffic = json.load(open(tfile)).get(args.workload, {}).get(dom_name)
+            traffic = json.load(open(tfile)).get(args.workload, {}).get(top["name"])
         except Exception:
             traffic = None
     sim.close()
@@ -490,63 +510,95 @@ def run_ours(args) -> None:
     sim2.close()
     e2e_val = npts * K * world / (t1 - t0)
 
+    # the other two ratios of the metric, in the same process (every rank runs them: replicas)
+    extras = {}
+    if not args.no_extras:
+        with ClockSampler(gpu_id) as clk2:
+            mb = measure_batch(ctx, stream, rep, W)
+            ma = measure_adjoint(ctx, stream, rep, W, three_d=False, store_all=False)
+        extras = {
+            "batched_over_plain": mb["ms_plain"] / mb["ms_batch"],
+            "batched": {"workload": BATCH, "value": mb["work"] * world / (mb["ms_batch"] / 1e3),
+                        "plain_value": mb["work"] * world / (mb["ms_plain"] / 1e3), "unit": UNIT,
+                        "ms_batch": mb["ms_batch"], "ms_plain": mb["ms_plain"]},
+            "grad_over_forward": ma["grad_ms"] / ma["fwd_ms"],
+            "adjoint": {"workload": ADJ, "forward_ms": ma["fwd_ms"], "gradient_ms": ma["grad_ms"],
+                        "checkpoints": ma["r"]["checkpoints"], "interval": ma["r"]["interval"]},
+            "extras_clocks": clk2.summary(),
+        }
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
-        steps = args.cpu_steps
-        r = cpu_sample(b, steps, threads)
+        cw, cs = args.cpu_warmup, args.cpu_steps
+        r = cpu_sample(b, cw, cs, threads)
         cpu = {"value": r["value"], "unit": UNIT, "cores": threads, "kind": "port",
-               "sample": f"{args.workload}: first {steps} time step(s) in FP64 (oracle restatement) on "
-                         f"{threads} threads, time loop only ({r['seconds']:.1f} s)"}
+               "sample": f"{args.workload}: time steps {cw} .. {cw + cs - 1} (after {cw} untimed) in FP64 "
+                         f"(oracle restatement) on {threads} threads, time loop only ({r['seconds']:.1f} s)"}
 
     if rank == 0:
+        hetero = args.workload.startswith("hetero3d")
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,
             "ms_per_step": ms / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32", "data": "synthetic",
-            "config": {"workload": args.workload, "grid": list(b.grid.shape), "nt": b.grid.nt,
-                       "physics": "heterogeneous c0/rho0, power law y=1.5 with dispersion, B/A=6, additive p source"
-                       if args.workload.startswith("hetero") else "homogeneous IVP",
-                       "l2": "inputs larger than L2 (every field >= 67 MB)" if npts >= 2 ** 24 else "small grid",
-                       "parallelism": f"replicas{world}"},
-            "roofline": {"bound": "hbm", "kernel": dom_name, "achieved": achieved, "peak": peak,
+            "config": forward_config(args, b),
+            "roofline": {"bound": "hbm", "kernel": top["name"], "achieved": achieved, "peak": peak,
                          "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
                          "peak_source": peak_kind,
                          "step_achieved": step_bytes / (ms / K / 1e3) / 1e9,
                          "step_bytes_per_pt": step_bytes / npts,
-                         "kernel_share": dom["ms"] / step_ms if step_ms else None,
+                         "kernel_share": top["ms"] / step_ms if step_ms else None,
                          # the step against the fixed algorithmic byte model of a maximally fused
                          # 3D nonlinear absorbing step (332 B per grid point and step, source off)
-                         "model_bytes_per_pt": 332 if args.workload.startswith("hetero3d") else None,
-                         "model_frac": (value * 332 / 1e9 / peak) if args.workload.startswith("hetero3d") else None},
+                         "model_bytes_per_pt": 332 if hetero else None,
+                         "model_frac": (value / world * 332 / 1e9 / peak) if hetero else None},
             "cpu_baseline": cpu,
-            "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": h2d / K, "d2h_bytes_per_step": d2h / K,
-                    "seconds": t1 - t0},
+            "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": h2d / K,
+                    "d2h_bytes_per_step": d2h / K, "seconds": t1 - t0,
+                    "what": "kw_sim_create from host buffers + `steps` time steps + copy-out of p, pMax, pFinal"},
             "gpu_launches": launches_per_step * K,
             "clocks": clk.summary(),
             "kernels": {k: {"ms": round(v["ms"], 4), "GBps": round(v["bytes"] / (v["ms"] / 1e3) / 1e9, 1) if v["ms"] > 0 else 0,
                             "launches": v["launches"]} for k, v in groups.items()},
+            **extras,
         }
         print(json.dumps(line), flush=True)
     ctx.close()
     rep.close()
 
 
+def _relaunch_under_torchrun(args) -> int:
+    """--gpus N > 1 without torchrun's environment: run this script as N local ranks."""
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", f"--nproc-per-node={args.gpus}",
+           "--master-addr", "127.0.0.1", "--master-port", str(port), os.path.abspath(__file__), *sys.argv[1:]]
+    return subprocess.call(cmd)
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=0, help="timed steps (default: the rest of the simulation)")
+    ap.add_argument("--steps", type=int, default=20, help="timed steps (0: the rest of the simulation)")
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="hetero3d_256")
-    ap.add_argument("--cpu-steps", type=int, default=1)
-    ap.add_argument("--ref-steps", type=int, default=2)
+    ap.add_argument("--cpu-warmup", type=int, default=1)
+    ap.add_argument("--cpu-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extras", action="store_true", help="skip the batched/plain and gradient/forward ratios")
     ap.add_argument("--adjoint-nt", type=int, default=0,
                     help="adjoint workloads: time steps (default: the configuration's; shorter runs for profiling)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
+    world = int(os.environ.get("WORLD_SIZE", "0"))
+    if args.gpus > 1 and world == 0:
+        sys.exit(_relaunch_under_torchrun(args))
+    if world and world != args.gpus:
+        sys.exit(f"--gpus {args.gpus} but WORLD_SIZE={world}")
     if args.impl == "reference":
         run_reference(args)
     elif args.workload == BATCH:
