@@ -561,6 +561,9 @@ def run_ours(args) -> None:
             "clocks": clk.summary(),
             "kernels": {k: {"ms": round(v["ms"], 4), "GBps": round(v["bytes"] / (v["ms"] / 1e3) / 1e9, 1) if v["ms"] > 0 else 0,
                             "launches": v["launches"]} for k, v in groups.items()},
+            # every launch of one step in issue order: mean event time and algorithmic GB/s
+            "step_profile": [[k["name"], round(k["ms"], 4), round(k["bytes"] / (k["ms"] / 1e3) / 1e9, 1) if k["ms"] > 0 else 0]
+                             for k in prof],
             **extras,
         }
         print(json.dumps(line), flush=True)

@@ -315,9 +315,10 @@ KW_API void kw_batch_destroy(kw_batch* batch);
 
 /* ---- adjoint gradient of a sensor-data misfit --------------------------------------------------
  * Gradients of L = 1/2 sum_t sum_q (p_q(t) - data_q(t))^2 (p_q: the pressure the forward
- * kw_sim_run records at sensor point q) with respect to the sound speed c0 (one value per grid
- * point) and the initial pressure p0, by the exact discrete adjoint of the time step: every
- * operator of the step transposed in reverse order. The reference has no adjoint; this is the
+ * kw_sim_run records at sensor point q) with respect to the sound speed c0 and the density rho0
+ * (one value per grid point; a scalar c0 or rho0 is differentiated as a uniform map, whose
+ * scalar derivative is the sum of the field) and the initial pressure p0, by the exact discrete
+ * adjoint of the time step: every operator of the step transposed in reverse order. The reference has no adjoint; this is the
  * kspaceFirstOrderAdjoint entry a Swift adapter would expose next to kspaceFirstOrder
  * (Sources/KWave/Solver/KSpaceFirstOrder.swift:79-107 is the forward it differentiates).
  * The reverse sweep needs the forward states in reverse order; they are recomputed segment by
@@ -325,13 +326,18 @@ KW_API void kw_batch_destroy(kw_batch* batch);
  * Supported: 1D/2D/3D, heterogeneous c0/rho0, lossless / Stokes / power law (with or without
  * dispersion), B/A, source.p0 and k-space corrected additive pressure sources, binary or
  * Cartesian sensors. KW_ERR_UNSUPPORTED: velocity sources, Dirichlet or uncorrected pressure
- * sources, directivity, smoothC0 / smoothRho0 maps, grad_p0 with smoothP0, grad_rho0. */
+ * sources, directivity, smoothC0 / smoothRho0 maps, grad_p0 with smoothP0. */
 typedef enum kw_checkpoint_policy {
     KW_CHECKPOINT_SQRT = 0,      /* ceil(sqrt(nt)) steps between checkpoints, segments recomputed */
     KW_CHECKPOINT_INTERVAL = 1,  /* checkpoint_interval steps between checkpoints */
     KW_CHECKPOINT_BUDGET = 2,    /* keep every state when that fits memory_budget bytes, else the
                                     interval that needs the least memory */
-    KW_CHECKPOINT_STORE_ALL = 3  /* keep every state of the forward run (no recompute) */
+    KW_CHECKPOINT_STORE_ALL = 3, /* keep every state of the forward run (no recompute) */
+    KW_CHECKPOINT_REVOLVE = 4    /* binomial (revolve) schedule: checkpoint_interval > 0 snapshots of
+                                    the state, else as many as memory_budget holds; one tape slot;
+                                    a step is recomputed at most r times, r the least with
+                                    C(snapshots + r, r) >= nt (BUDGET falls back to it when no
+                                    uniform interval fits the budget) */
 } kw_checkpoint_policy;
 
 typedef struct kw_adjoint_desc {
@@ -342,7 +348,8 @@ typedef struct kw_adjoint_desc {
     double memory_budget;         /* KW_CHECKPOINT_BUDGET, bytes of device memory for states */
     float* grad_c0;               /* out: dL/dc0 on the grid (same layout as sound_speed), or NULL */
     float* grad_p0;               /* out: dL/dp0 on the grid, or NULL (needs source.p0) */
-    float* grad_rho0;             /* must be NULL (not implemented) */
+    float* grad_rho0;             /* out: dL/drho0 on the grid, or NULL (rho0 enters dt rho0 nl,
+                                     dt / staggerDensity(rho0), rho0 div and B/A S^2 / (2 rho0)) */
     double misfit;                /* out: L */
     double forward_ms;            /* out: device time of the forward run that stores checkpoints */
     double reverse_ms;            /* out: device time of the reverse sweep (recompute included) */

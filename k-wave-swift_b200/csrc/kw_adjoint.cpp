@@ -20,16 +20,41 @@
 #include <vector>
 
 #include "kw_adjoint.h"
+
+#include <functional>
+#include <map>
 #include "kw_engine.h"
 
 namespace kw {
 
 static KwError err(int code, const std::string& m) { return KwError{code, m}; }
 
+// Binomial checkpointing (Griewank's treeverse): with s free snapshot slots and the state before a
+// stretch held, l steps are reversed with each step recomputed at most r times, r the least with
+// beta(s, r) = C(s + r, s) >= l. A stretch is split at m: the states up to m are advanced once and
+// the right part (l - m steps, s - 1 slots) needs l - m <= beta(s - 1, r), the left part (m steps,
+// s slots, one repetition used) m <= beta(s, r - 1); any m between keeps the bound, the midpoint
+// is taken.
+static double binom_beta(int s, int r) {
+    if (s < 0 || r < 0) return 0.0;
+    double b = 1.0;   // C(s + r, s), capped far above any step count
+    for (int i = 1; i <= r && b < 1e15; ++i) b = b * (s + i) / i;
+    return b;
+}
+static int binom_reps(int l, int s) {
+    int r = 0;
+    while (binom_beta(s, r) < l) ++r;
+    return r;
+}
+static int binom_split(int l, int s) {
+    const int r = binom_reps(l, s);
+    const int lo = std::max(1, (int)std::max(1.0, l - binom_beta(s - 1, r)));
+    const int hi = (int)std::min((double)(l - 1), binom_beta(s, r - 1));
+    return hi < lo ? lo : (lo + hi) / 2;
+}
 void Engine::adjoint(const kw_sim_desc& din, kw_adjoint_desc& a) {
     if (a.abi_version != KW_ABI_VERSION) throw err(KW_ERR_INVALID, "adjoint descriptor abi_version mismatch");
     if (!a.data) throw err(KW_ERR_INVALID, "adjoint: data is required");
-    if (a.grad_rho0) throw err(KW_ERR_UNSUPPORTED, "adjoint: the density gradient is not implemented");
     if (din.u_mask) throw err(KW_ERR_UNSUPPORTED, "adjoint: velocity sources are not supported");
     if (din.p_mask && din.p.data && din.p_mode != KW_SOURCE_ADDITIVE)
         throw err(KW_ERR_UNSUPPORTED, "adjoint: only the k-space corrected additive pressure source is supported");
@@ -39,6 +64,7 @@ void Engine::adjoint(const kw_sim_desc& din, kw_adjoint_desc& a) {
         throw err(KW_ERR_UNSUPPORTED, "adjoint: smoothC0 / smoothRho0 maps are not supported");
     if (a.grad_p0 && !din.p0) throw err(KW_ERR_INVALID, "adjoint: grad_p0 needs source.p0");
     if (a.grad_p0 && din.smooth_p0) throw err(KW_ERR_UNSUPPORTED, "adjoint: grad_p0 with smoothP0 is not supported");
+    const bool grho = a.grad_rho0 != nullptr;
     if (din.sensor_kind != KW_SENSOR_BINARY && din.sensor_kind != KW_SENSOR_CARTESIAN)
         throw err(KW_ERR_INVALID, "adjoint: a sensor is required");
     kw_sim_desc d = din;
@@ -60,7 +86,7 @@ void Engine::adjoint(const kw_sim_desc& din, kw_adjoint_desc& a) {
 
     // ---- work fields ----
     for (int k = 0; k < ADJ_COUNT; ++k)
-        if (!adj_is_view(k)) v.adj[k] = (float*)dalloc(fb);
+        if (!adj_is_view(k) && (grho || k < ADJ_GP || k >= ADJ_GP + 3)) v.adj[k] = (float*)dalloc(fb);
     // the absorption job of the reverse step has three components, so it needs three spectra
     // (a 1D simulation allocates two)
     for (int k = 0; k < 3; ++k)
@@ -82,13 +108,24 @@ void Engine::adjoint(const kw_sim_desc& din, kw_adjoint_desc& a) {
     v.adj_gc = gc;
     v.adj_rev = d_rev;
     v.adj_y = y;
+    // density gradient: the direct terms and dL/d(dt / rho_sg_a), accumulated in FP64
+    if (grho) {
+        v.adj_gr = (double*)dalloc((size_t)N * sizeof(double));
+        for (int b = 0; b < D; ++b) v.adj_gdtor[b] = (double*)dalloc((size_t)N * sizeof(double));
+    }
+    const bool keep_dd = nonlin || grho;   // the tape keeps d_a = D-_a u_a
     check(cudaMemcpyAsync(d_sims_, &v, sizeof(SimDev), cudaMemcpyHostToDevice, st()), "upload sim");
 
     // ---- checkpoint policy ----
     const bool stokes = v.absorb == 1;   // the Stokes term reads div(t); the power law only p(t), S(t)
-    const int ck_fields = 2 * D + 3 + (stokes ? 1 : 0);   // u_a, rho_a, S, p, S(t-1), div
-    const int tp_fields = 2 + (stokes ? 1 : 0) + (nonlin ? D : 0) + (disp ? 1 : 0);   // p, S, div, d_a, A2(S)
+    const int ck_fields = 2 * D + 3 + (stokes ? 1 : 0) + (grho ? 1 : 0);   // u_a, rho_a, S, p, S(t-1), div, p(t-1)
+    const int CK_PPREV = 2 * D + 3 + (stokes ? 1 : 0);
+    const int tp_fields = 2 + (stokes ? 1 : 0) + (keep_dd ? D : 0) + (disp ? 1 : 0);   // p, S, div, d_a, A2(S)
     bool store_all = a.policy == KW_CHECKPOINT_STORE_ALL;
+    bool revolve = a.policy == KW_CHECKPOINT_REVOLVE;
+    int nsnap = 0;   // revolve: snapshot slots (the held base state included)
+    const double ck_bytes = (double)ck_fields * fb, tp_bytes = (double)tp_fields * fb;
+    auto snaps_in = [&](double budget) { return (int)std::floor((budget - tp_bytes - 2.0 * fb) / ck_bytes); };
     // With checkpoints, segment c's recompute runs on the library's stream while segment c + 1 is
     // reversed on a second stream (the reverse sweep has its own spectra). The K tape slots are
     // walked forwards by even segments and backwards by odd ones, so the recompute of segment c
@@ -109,14 +146,27 @@ void Engine::adjoint(const kw_sim_desc& din, kw_adjoint_desc& a) {
                 const double m = (double)((nt + k - 1) / k) * ck_fields * fb + (double)k * tp_fields * fb;
                 if (m < best) { best = m; K = k; }
             }
-            if (best > a.memory_budget) throw err(KW_ERR_OOM, "adjoint: the smallest checkpoint schedule needs more than memory_budget");
+            if (best > a.memory_budget) {   // no uniform interval fits: the binomial schedule
+                revolve = true;
+                nsnap = snaps_in(a.memory_budget);
+                if (nsnap < 1)
+                    throw err(KW_ERR_OOM, "adjoint: one state snapshot and one tape slot need more than memory_budget");
+            }
         }
+    } else if (revolve) {
+        nsnap = a.checkpoint_interval > 0 ? a.checkpoint_interval : snaps_in(a.memory_budget);
+        if (nsnap < 1) throw err(KW_ERR_OOM, "adjoint: one state snapshot and one tape slot need more than memory_budget");
     } else if (!store_all) throw err(KW_ERR_INVALID, "adjoint: unknown checkpoint policy");
+    if (revolve) {
+        nsnap = std::min(nsnap, nt);   // more slots than steps are never used
+        K = 1;
+        overlap = false;
+    }
     if (store_all) K = nt;
     if (K < 1 || K > nt) throw err(KW_ERR_INVALID, "adjoint: checkpoint_interval must be in [1, nt]");
-    const int nck = store_all ? 0 : (nt + K - 1) / K;
+    const int nck = revolve ? nsnap : (store_all ? 0 : (nt + K - 1) / K);
     if (nck < 2) overlap = false;
-    a.interval = K;
+    a.interval = revolve ? 0 : K;
     a.checkpoints = nck;
 
     // tape: K slots of tp_fields fields; checkpoints: nck of ck_fields fields
@@ -128,13 +178,16 @@ void Engine::adjoint(const kw_sim_desc& din, kw_adjoint_desc& a) {
     std::vector<float*> tape = alloc_fields((size_t)K * tp_fields);
     std::vector<float*> ck = alloc_fields((size_t)nck * ck_fields);
     auto tslot = [&](int slot, int f) { return tape[(size_t)slot * tp_fields + f]; };   // f: 0 p, 1 S, 2 div, then d_a, A2(S)
-    const int TF_DIV = 2, TF_DD = stokes ? 3 : 2, TF_Q2 = TF_DD + (nonlin ? D : 0);
+    const int TF_DIV = 2, TF_DD = stokes ? 3 : 2, TF_Q2 = TF_DD + (keep_dd ? D : 0);
     auto ckf = [&](int c, int f) { return ck[(size_t)c * ck_fields + f]; };   // u_a, rho_a, S, p, S(t-1), div
     auto cpy = [&](float* dst, const float* src) {
         check(cudaMemcpyAsync(dst, src, fb, cudaMemcpyDeviceToDevice, st()), "adjoint copy");
     };
     auto zero = [&](float* x) { check(cudaMemsetAsync(x, 0, fb, st()), "adjoint zero"); };
     float* zero_field = (float*)dalloc(fb);   // S(-1): the state before step 0 is zero
+    // revolve: S(t-1) and p(t-1) of the step whose tape the single slot holds
+    float* rv_sprev = revolve ? (float*)dalloc(fb) : nullptr;
+    float* rv_pprev = revolve && grho ? (float*)dalloc(fb) : nullptr;
 
     // tape slot of step t: even segments walk the slots forwards, odd ones backwards
     auto slot_of = [&](int t) { return store_all ? t : ((t / K) % 2 == 0 ? t % K : K - 1 - t % K); };
@@ -146,9 +199,15 @@ void Engine::adjoint(const kw_sim_desc& din, kw_adjoint_desc& a) {
         e.p = tslot(slot, 0);
         e.s = tslot(slot, 1);
         e.div = stokes ? tslot(slot, TF_DIV) : nullptr;
-        for (int b = 0; b < kMaxComp; ++b) e.dd[b] = nonlin && b < D ? tslot(slot, TF_DD + b) : nullptr;
+        for (int b = 0; b < kMaxComp; ++b) e.dd[b] = keep_dd && b < D ? tslot(slot, TF_DD + b) : nullptr;
         e.q2 = disp ? tslot(slot, TF_Q2) : nullptr;
+        e.pprev = !grho ? nullptr
+                        : (t == 0 ? zero_field : (store_all || t % K > 0 ? tslot(slot_of(t - 1), 0) : ckf(t / K, CK_PPREV)));
         e.sprev = t == 0 ? zero_field : (store_all || t % K > 0 ? tslot(slot_of(t - 1), 1) : ckf(t / K, 2 * D + 2));
+        if (revolve && t > 0) {
+            e.sprev = rv_sprev;
+            if (grho) e.pprev = rv_pprev;
+        }
     }
     const AdjTapeEntry* d_table = upload(table);
     v.tape = d_table;
@@ -173,22 +232,39 @@ void Engine::adjoint(const kw_sim_desc& din, kw_adjoint_desc& a) {
     // ---- 1. forward ----
     // The last segment (every step with store-all) fills the tape as it runs, so the reverse sweep
     // starts with its reverse instead of recomputing it.
-    const int t_last = store_all ? 0 : (nck - 1) * K;
+    const int t_last = revolve ? nt : (store_all ? 0 : (nck - 1) * K);
     set_tape_mode(t_last == 0);
     reset();
+    // revolve: the residual sweep stores the snapshots of the schedule's right spine (the base state
+    // of the reversed steps, then each first split of the remaining stretch with one slot fewer)
+    const int t_stop = has_p0 ? 1 : 0;
+    std::map<int, int> spine;   // step t -> snapshot slot holding the state after step t
+    if (revolve) {
+        int lo = t_stop, s_free = nsnap - 1;
+        spine[lo] = 0;
+        while (nt - lo > 1 && s_free > 0) {
+            lo += binom_split(nt - lo, s_free);
+            spine[lo] = nsnap - s_free;
+            --s_free;
+        }
+    }
     check(cudaEventRecord(e0, st()), "event");
     for (int t = 0; t < nt; ++t) {
-        const bool ck_step = !store_all && t % K == 0;
+        const bool ck_step = revolve ? spine.count(t) > 0 : (!store_all && t % K == 0);
         if (ck_step) {
-            const int c = t / K;
+            const int c = revolve ? spine[t] : t / K;
             if (t == 0) zero(ckf(c, 2 * D + 2));
             else cpy(ckf(c, 2 * D + 2), v.rho_sum);
+            if (grho) {
+                if (t == 0) zero(ckf(c, CK_PPREV));
+                else cpy(ckf(c, CK_PPREV), v.p);
+            }
         }
         if (t == t_last && !tape_mode_) set_tape_mode(true);
         step(1);
         if (tape_mode_ && t == 0) tape_copy();   // the t = 0 override follows the step's epilogues
         if (ck_step) {
-            const int c = t / K;
+            const int c = revolve ? spine[t] : t / K;
             for (int b = 0; b < D; ++b) { cpy(ckf(c, b), v.u[b]); cpy(ckf(c, D + b), v.rho[b]); }
             cpy(ckf(c, 2 * D), v.rho_sum);
             cpy(ckf(c, 2 * D + 1), v.p);
@@ -219,8 +295,12 @@ void Engine::adjoint(const kw_sim_desc& din, kw_adjoint_desc& a) {
     any_recp_ = false;
     set_tape_mode(true);
     for (int k = 0; k < ADJ_COUNT; ++k)
-        if (!adj_is_view(k)) zero(v.adj[k]);
+        if (!adj_is_view(k) && v.adj[k]) zero(v.adj[k]);
     check(cudaMemsetAsync(gc, 0, (size_t)N * sizeof(double), st()), "zero");
+    if (grho) {
+        check(cudaMemsetAsync(v.adj_gr, 0, (size_t)N * sizeof(double), st()), "zero");
+        for (int b = 0; b < D; ++b) check(cudaMemsetAsync(v.adj_gdtor[b], 0, (size_t)N * sizeof(double), st()), "zero");
+    }
 
     // The overlapped sweep: the reverse steps are issued on their own stream against a copy of the
     // simulation descriptor with its own spectra (and tensor maps), step counter and tape views.
@@ -318,14 +398,26 @@ void Engine::adjoint(const kw_sim_desc& din, kw_adjoint_desc& a) {
         launch_adj_begin(st(), d_sims_, d_t_, d_rev, d_table, d_resid, npts);   // also sets the step counter the pass kernels gate on
         A.sig = src_on ? v.adj[ADJ_SIG] : nullptr;
         if (powerlaw && fused && eos_fused) {   // the absorption filters with the reverse EoS as epilogue
-            job(ADJ_X1, ADJ_A1, disp ? 2 : 1, absorption_op, EPI_ADJ_EOS, 1, "adj_eos");
+            job(ADJ_X1, ADJ_A1, disp ? 2 : 1, absorption_op, grho ? EPI_ADJ_EOS_RHO : EPI_ADJ_EOS, 1, "adj_eos");
         } else {
             if (powerlaw) job(ADJ_X1, ADJ_A1, disp ? 2 : 1, absorption_op, EPI_STORE, 0, "adj_abs");
-            launch_adj_eos(st(), d_sims_, N, A, d_rev);
+            launch_adj_eos(st(), d_sims_, N, A, d_rev, grho);
         }
         if (src_on) {
             job(ADJ_SIG, ADJ_GSIG, 1, radial(RT_SKAPPA), EPI_STORE, 0, "adj_src");
             launch_adj_src(st(), d_sims_, v.psrc.nsrc, v.adj[ADJ_GSIG], d_t_, gc);
+        }
+        if (grho) {   // g_a = D+_a p(t-1) of the velocity update, for dL/d(dt / rho_sg_a)
+            SpecJob gj;
+            gj.in_field = FS_ADJ + ADJ_PPREV;
+            gj.nin = 1;
+            gj.fanout = 1;
+            gj.nout = D;
+            for (int b = 0; b < D; ++b) gj.op[b] = OpSpec{AO_DPOS, (int8_t)b, RT_KAPPA, 0};
+            gj.epi = EPI_STORE;
+            gj.out_field = FS_ADJ + ADJ_GP;
+            gj.name = "adj_gp";
+            issue_job(gj, -1);
         }
         if (fused) {
             job(ADJ_W, ADJ_E, D, deriv(AO_DPOS), EPI_ADJ_VEL, 0, "adj_vel");
@@ -365,9 +457,96 @@ void Engine::adjoint(const kw_sim_desc& din, kw_adjoint_desc& a) {
         check(cudaGraphLaunch(rgraph[var], st()), "graph launch");
     };
 
-    const int t_stop = has_p0 ? 1 : 0;
     on_reverse([&] { launch_set_step(st(), d_rev, nt - 1); });
-    if (store_all) {
+    if (revolve) {
+        // snapshot c holds the state after some step t (u, rho, S, p, div) and S(t-1), p(t-1)
+        set_tape_mode(false);
+        std::vector<int> free_slots;
+        for (int c = nsnap - 1; c >= 1; --c) {
+            bool used = false;
+            for (auto& kv : spine) used = used || kv.second == c;
+            if (!used) free_slots.push_back(c);
+        }
+        auto restore = [&](int c, int t) {   // the state after step t, from snapshot c
+            for (int b = 0; b < D; ++b) { cpy(v.u[b], ckf(c, b)); cpy(v.rho[b], ckf(c, D + b)); }
+            cpy(v.rho_sum, ckf(c, 2 * D));
+            cpy(v.p, ckf(c, 2 * D + 1));
+            if (stokes) cpy(v.div_term, ckf(c, 2 * D + 3));
+            launch_set_step(st(), d_t_, t + 1);
+            t_ = t + 1;
+        };
+        // advance from the state after step a (snapshot ca) to the state after step m; with
+        // cm >= 0 store it in snapshot cm, else leave it live with S(m-1), p(m-1) in rv_sprev / rv_pprev
+        auto advance = [&](int ca, int a0, int m, int cm) {
+            restore(ca, a0);
+            for (int t = a0 + 1; t <= m; ++t) {
+                if (t == m) {
+                    cpy(cm >= 0 ? ckf(cm, 2 * D + 2) : rv_sprev, v.rho_sum);
+                    if (grho) cpy(cm >= 0 ? ckf(cm, CK_PPREV) : rv_pprev, v.p);
+                }
+                step(1);
+            }
+            if (cm >= 0) {
+                for (int b = 0; b < D; ++b) { cpy(ckf(cm, b), v.u[b]); cpy(ckf(cm, D + b), v.rho[b]); }
+                cpy(ckf(cm, 2 * D), v.rho_sum);
+                cpy(ckf(cm, 2 * D + 1), v.p);
+                if (stokes) cpy(ckf(cm, 2 * D + 3), v.div_term);
+            }
+        };
+        // the tape of step t from the live state after step t (S(t-1), p(t-1) already in place)
+        auto tape_live = [&](int t) {
+            if (keep_dd || disp) {
+                launch_set_step(st(), d_t_, t);
+                launch_adj_views(st(), d_sims_, d_table, t);
+                if (keep_dd) job_in(FS_U, ADJ_DDP, D, deriv(AO_DNEG), EPI_STORE, 0, "adj_du");
+                if (disp) job_in(FS_RHO_SUM, ADJ_Q2, 1, radial(RT_NU2), EPI_STORE, 0, "adj_q2");
+            }
+            launch_set_step(st(), d_t_, t + 1);
+            t_ = t + 1;
+            tape_copy();
+        };
+        auto tape_from = [&](int c, int t) {
+            restore(c, t);
+            if (t > 0) {
+                cpy(rv_sprev, ckf(c, 2 * D + 2));
+                if (grho) cpy(rv_pprev, ckf(c, CK_PPREV));
+            }
+            tape_live(t);
+        };
+        // reverse steps b, b-1, ..., a with the state after step a in snapshot ca and s free slots
+        std::function<void(int, int, int, int)> rev = [&](int a0, int b, int s, int ca) {
+            if (a0 == b) {
+                tape_from(ca, a0);
+                reverse_step(a0);
+                return;
+            }
+            if (s == 0) {
+                for (int t = b; t > a0; --t) {
+                    advance(ca, a0, t, -1);
+                    tape_live(t);
+                    reverse_step(t);
+                }
+                tape_from(ca, a0);
+                reverse_step(a0);
+                return;
+            }
+            const int m = a0 + binom_split(b - a0 + 1, s);
+            int cm;
+            auto it = spine.find(m);
+            if (it != spine.end() && it->first != t_stop) {
+                cm = it->second;   // stored by the residual sweep
+                spine.erase(it);
+            } else {
+                cm = free_slots.back();
+                free_slots.pop_back();
+                advance(ca, a0, m, cm);
+            }
+            rev(m, b, s - 1, cm);
+            free_slots.push_back(cm);
+            rev(a0, m - 1, s, ca);
+        };
+        if (nt - 1 >= t_stop) rev(t_stop, nt - 1, nsnap - 1, spine[t_stop]);
+    } else if (store_all) {
         for (int t = nt - 1; t >= t_stop; --t) reverse_step(t);
     } else {
         for (int c = nck - 1; c >= 0; --c) {
@@ -385,10 +564,10 @@ void Engine::adjoint(const kw_sim_desc& din, kw_adjoint_desc& a) {
                 cpy(v.rho_sum, ckf(c, 2 * D));
                 cpy(v.p, ckf(c, 2 * D + 1));
                 if (stokes) cpy(v.div_term, ckf(c, 2 * D + 3));
-                if (nonlin || disp) {   // d_a(t0) = D-_a u_a(t0), A2(S(t0)) of the restored state into its tape slot
+                if (keep_dd || disp) {   // d_a(t0) = D-_a u_a(t0), A2(S(t0)) of the restored state into its tape slot
                     launch_set_step(st(), d_t_, t0);
                     launch_adj_views(st(), d_sims_, d_table, t0);
-                    if (nonlin) job_in(FS_U, ADJ_DDP, D, deriv(AO_DNEG), EPI_STORE, 0, "adj_du");
+                    if (keep_dd) job_in(FS_U, ADJ_DDP, D, deriv(AO_DNEG), EPI_STORE, 0, "adj_du");
                     if (disp) job_in(FS_RHO_SUM, ADJ_Q2, 1, radial(RT_NU2), EPI_STORE, 0, "adj_q2");
                 }
                 launch_set_step(st(), d_t_, t0 + 1);
@@ -419,6 +598,20 @@ void Engine::adjoint(const kw_sim_desc& din, kw_adjoint_desc& a) {
     if (has_p0) {
         // t = 0 override: p = p0, rho_a = p0 / (D c^2), u_a = dtor_a / 2 D+_a p0
         launch_adj_begin(st(), d_sims_, d_t_, d_rev, d_table, d_resid, npts);   // *d_rev is 0 here: residual r_0
+        if (grho) {   // u_a = dtor_a / 2 D+_a p0: g_a = D+_a p0 into ADJ_GP, then dL/d dtor_a += lambda_u_a g_a / 2
+            check(cudaMemcpyAsync(v.adj[ADJ_GP], h.p0s, fb, cudaMemcpyDeviceToDevice, st()), "p0 copy");
+            SpecJob gj;
+            gj.in_field = FS_ADJ + ADJ_GP;
+            gj.nin = 1;
+            gj.fanout = 1;
+            gj.nout = D;
+            for (int b = 0; b < D; ++b) gj.op[b] = OpSpec{AO_DPOS, (int8_t)b, RT_KAPPA, 0};
+            gj.epi = EPI_STORE;
+            gj.out_field = FS_ADJ + ADJ_GP;
+            gj.name = "adj_gp0";
+            issue_job(gj, -1);
+            launch_adj_rho_p0(st(), d_sims_, N);
+        }
         launch_adj_half_dtor(st(), d_sims_, N, A);
         job(ADJ_W, ADJ_E, D, deriv(AO_DNEG), EPI_STORE, 0, "adj_p0");
         float* gp = a.grad_p0 ? v.adj[ADJ_GSIG] : nullptr;
@@ -433,6 +626,10 @@ void Engine::adjoint(const kw_sim_desc& din, kw_adjoint_desc& a) {
     if (a.grad_c0) {
         launch_adj_store_grad(st(), gc, v.adj[ADJ_SIG], N);
         check(cudaMemcpyAsync(a.grad_c0, v.adj[ADJ_SIG], fb, cudaMemcpyDeviceToHost, st()), "grad c0");
+    }
+    if (grho) {
+        launch_adj_rho_final(st(), d_sims_, N, v.adj[ADJ_GSIG]);
+        check(cudaMemcpyAsync(a.grad_rho0, v.adj[ADJ_GSIG], fb, cudaMemcpyDeviceToHost, st()), "grad rho0");
     }
     check(cudaGetLastError(), "adjoint launch");
     check(cudaStreamSynchronize(st()), "adjoint sync");

@@ -43,6 +43,7 @@ __device__ __forceinline__ void set_views(SimDev& S, const AdjTapeEntry& e) {
     S.adj[ADJ_DIVP] = e.div;
     for (int b = 0; b < kMaxComp; ++b) S.adj[ADJ_DDP + b] = e.dd[b];
     S.adj[ADJ_Q2] = e.q2;
+    S.adj[ADJ_PPREV] = e.pprev;
 }
 
 __global__ void k_adj_tape(const SimDev* __restrict__ sims, const int* __restrict__ d_t,
@@ -91,7 +92,9 @@ __global__ void k_adj_begin(SimDev* __restrict__ sims, int* __restrict__ d_t, co
 }
 
 // Every input is loaded before the first store: the stores may alias the loads as far as the
-// compiler knows, and interleaving them would serialise the loads.
+// compiler knows, and interleaving them would serialise the loads. GRHO: also the direct terms of
+// dL/drho0 (rho0 enters dt rho0 nl, the absorption input rho0 div, B/A S^2 / (2 rho0)).
+template <bool GRHO>
 __global__ void __launch_bounds__(256, 4) k_adj_eos(const SimDev* __restrict__ sims, AdjStepArgs A, int* __restrict__ d_rev) {
     const SimDev& S = sims[0];
     const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -109,7 +112,7 @@ __global__ void __launch_bounds__(256, 4) k_adj_eos(const SimDev* __restrict__ s
     for (int a = 0; a < kMaxComp; ++a) {
         if (a >= D) break;
         lr[a] = A.lam_r[a][i];
-        if (S.nonlinear) dd[a] = S.adj[ADJ_DDP + a][i];
+        if (S.nonlinear || GRHO) dd[a] = S.adj[ADJ_DDP + a][i];
         pm[a] = __ldg(S.ax[a].pml + layout_coord(S, i, a));
     }
     double gcv = A.gc[i];
@@ -145,6 +148,17 @@ __global__ void __launch_bounds__(256, 4) k_adj_eos(const SimDev* __restrict__ s
         sig += lam[a] * S.ax[a].inv_d;
     }
     A.gc[i] = gcv;
+    if constexpr (GRHO) {
+        // d p / d rho0 = c^2 (tau A1 or tau (Stokes)) sum_a d_a - c^2 B/A S^2 / (2 rho0^2);
+        // d rho_a / d rho0 = -pm_a dt d_a (d(dt rho0 nl) / d rho0 = dt)
+        float sd = 0.f;
+        for (int a = 0; a < D; ++a) sd += dd[a];
+        double g = 0.0;
+        if (S.absorb >= 1) g += (double)ldiv * sd;
+        if (S.nonlinear) g -= (double)lE * bona * sv * sv / (2.0 * (double)r0 * r0);
+        for (int a = 0; a < D; ++a) g -= (double)pm[a] * S.dt * dd[a] * lam[a];
+        S.adj_gr[i] += g;
+    }
 #pragma unroll
     for (int a = 0; a < kMaxComp; ++a) {
         if (a >= D) break;
@@ -168,7 +182,8 @@ __global__ void k_adj_src(const SimDev* __restrict__ sims, const float* __restri
     gc[i] += (double)gsig[i] * sg * (-(double)__ldg(s.scale[0] + q) / c);
 }
 
-// mu_a = lambda_u_a - e_a; lambda_u_a <- sg_a^2 mu_a; w_a <- sg_a dtor_a mu_a
+// mu_a = lambda_u_a - e_a; lambda_u_a <- sg_a^2 mu_a; w_a <- sg_a dtor_a mu_a; with the density
+// gradient also dL/d dtor_a += -sg_a g_a mu_a (g_a = D+_a p(t-1) in ADJ_GP)
 __global__ void k_adj_vel(const SimDev* __restrict__ sims, AdjStepArgs A) {
     const SimDev& S = sims[0];
     const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -176,6 +191,7 @@ __global__ void k_adj_vel(const SimDev* __restrict__ sims, AdjStepArgs A) {
     for (int a = 0; a < S.dim; ++a) {
         const float mu = A.lam_u[a][i] - A.e[a][i];
         const float sg = __ldg(S.ax[a].pml_sg + layout_coord(S, i, a));
+        if (S.adj_gr) S.adj_gdtor[a][i] -= (double)sg * S.adj[ADJ_GP + a][i] * mu;
         A.lam_u[a][i] = sg * sg * mu;
         A.w[a][i] = sg * S.dtor[a].at(i) * mu;
     }
@@ -225,6 +241,36 @@ __global__ void k_adj_store_grad(const double* __restrict__ gc, float* __restric
     if (i < n) out[i] = (float)gc[i];
 }
 
+// t = 0 override u_a = dtor_a / 2 D+_a p0: dL/d dtor_a += lambda_u_a g_a / 2 (g_a in ADJ_GP)
+__global__ void k_adj_rho_p0(const SimDev* __restrict__ sims) {
+    const SimDev& S = sims[0];
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= S.N) return;
+    for (int a = 0; a < S.dim; ++a) S.adj_gdtor[a][i] += 0.5 * (double)S.adj[ADJ_LU + a][i] * S.adj[ADJ_GP + a][i];
+}
+
+// dL/drho0: the direct terms plus, per axis, staggerDensity^T (KSpaceFirstOrder.swift:799-806:
+// rho_sg_a[i] = (rho0[i] + rho0[i + e_a]) / 2, the last index along a replicated) of
+// dL/d rho_sg_a = dL/d dtor_a * d(dt / rho_sg) / d rho_sg = -dL/d dtor_a dtor_a^2 / dt
+__global__ void k_adj_rho_final(const SimDev* __restrict__ sims, float* __restrict__ out) {
+    const SimDev& S = sims[0];
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= S.N) return;
+    double g = S.adj_gr[i];
+    for (int a = 0; a < S.dim; ++a) {
+        const int L = a + 3 - S.dim;
+        const long long stride = L == 0 ? (long long)S.B * S.C : (L == 1 ? (long long)S.C : 1LL);
+        const int ia = layout_coord(S, i, a), n = S.ax[a].n;
+        auto gsg = [&](long long j) {
+            const double q = S.dtor[a].at(j);
+            return -S.adj_gdtor[a][j] * q * q / (double)S.dt;
+        };
+        g += (ia == n - 1 ? 1.0 : 0.5) * gsg(i);   // rho_sg_a[i] holds rho0[i]
+        if (ia >= 1) g += 0.5 * gsg(i - stride);    // rho_sg_a[i - e_a] holds rho0[i]
+    }
+    out[i] = (float)g;
+}
+
 // ---------------------------------------------------------------------------------------------
 static unsigned blocks(long long n) { return (unsigned)((n + 255) / 256); }
 
@@ -239,8 +285,9 @@ void launch_adj_tape(cudaStream_t st, SimDev* d_sims, const int* d_t, const AdjT
 void launch_adj_views(cudaStream_t st, SimDev* d_sims, const AdjTapeEntry* table, int t) {
     k_adj_views<<<1, 1, 0, st>>>(d_sims, table, t);
 }
-void launch_adj_eos(cudaStream_t st, const SimDev* d_sims, long long N, const AdjStepArgs& a, int* d_rev) {
-    k_adj_eos<<<blocks(N), 256, 0, st>>>(d_sims, a, d_rev);
+void launch_adj_eos(cudaStream_t st, const SimDev* d_sims, long long N, const AdjStepArgs& a, int* d_rev, bool grho) {
+    if (grho) k_adj_eos<true><<<blocks(N), 256, 0, st>>>(d_sims, a, d_rev);
+    else k_adj_eos<false><<<blocks(N), 256, 0, st>>>(d_sims, a, d_rev);
 }
 void launch_adj_src(cudaStream_t st, const SimDev* d_sims, int nsrc, const float* gsig, const int* d_t, double* gc) {
     if (nsrc > 0) k_adj_src<<<blocks(nsrc), 256, 0, st>>>(d_sims, gsig, d_t, gc);
@@ -259,6 +306,12 @@ void launch_adj_p0(cudaStream_t st, const SimDev* d_sims, long long N, const Adj
 }
 void launch_adj_store_grad(cudaStream_t st, const double* gc, float* out, long long n) {
     k_adj_store_grad<<<blocks(n), 256, 0, st>>>(gc, out, n);
+}
+void launch_adj_rho_p0(cudaStream_t st, const SimDev* d_sims, long long N) {
+    k_adj_rho_p0<<<blocks(N), 256, 0, st>>>(d_sims);
+}
+void launch_adj_rho_final(cudaStream_t st, const SimDev* d_sims, long long N, float* out) {
+    k_adj_rho_final<<<blocks(N), 256, 0, st>>>(d_sims, out);
 }
 
 }  // namespace kw

@@ -23,16 +23,17 @@ enum AdjField {
     ADJ_SIG = 19,     // sum_a L_a / dx_a
     ADJ_GSIG = 20,    // G(sigma)
     ADJ_DDP = 21,     // d_a(t) = D-_a u_a(t) (points into the tape), 3
-    ADJ_SPARE = 24,   // 3 unused
+    ADJ_GP = 24,      // g_a = D+_a p(t-1), the velocity update's pressure gradient (density gradient), 3
     ADJ_PTP = 27,     // p(t)   (points into the tape)
     ADJ_SPRP = 28,    // S(t-1) (points into the tape, a checkpoint or a zero field)
     ADJ_DIVP = 29,    // div(t) (points into the tape; Stokes)
-    ADJ_COUNT = 30
+    ADJ_PPREV = 30,   // p(t-1) (points into the tape, a checkpoint or a zero field; density gradient)
+    ADJ_COUNT = 31
 };
 // entries that point into the tape instead of owning a field
 __host__ __device__ constexpr bool adj_is_view(int k) {
-    return k == ADJ_STP || k == ADJ_Q2 || (k >= ADJ_DDP && k < ADJ_DDP + 3) || (k >= ADJ_SPARE && k < ADJ_SPARE + 3) || k == ADJ_PTP ||
-           k == ADJ_SPRP || k == ADJ_DIVP;
+    return k == ADJ_STP || k == ADJ_Q2 || (k >= ADJ_DDP && k < ADJ_DDP + 3) || k == ADJ_PTP || k == ADJ_SPRP ||
+           k == ADJ_DIVP || k == ADJ_PPREV;
 }
 
 static_assert(ADJ_COUNT <= kAdjFields, "adjoint fields");
@@ -63,12 +64,17 @@ void launch_adj_begin(cudaStream_t st, SimDev* d_sims, int* d_t, const int* d_re
 void launch_adj_tape(cudaStream_t st, SimDev* d_sims, const int* d_t, const AdjTapeEntry* table, int stokes, long long N);
 // point the tape views of the work fields at table[t] (no step counter change)
 void launch_adj_views(cudaStream_t st, SimDev* d_sims, const AdjTapeEntry* table, int t);
-void launch_adj_eos(cudaStream_t st, const SimDev* d_sims, long long N, const AdjStepArgs& a, int* d_rev);
+void launch_adj_eos(cudaStream_t st, const SimDev* d_sims, long long N, const AdjStepArgs& a, int* d_rev, bool grho);
 void launch_adj_src(cudaStream_t st, const SimDev* d_sims, int nsrc, const float* gsig, const int* d_t, double* gc);
 void launch_adj_vel(cudaStream_t st, const SimDev* d_sims, long long N, const AdjStepArgs& a);
 void launch_adj_sum(cudaStream_t st, const SimDev* d_sims, long long N, const AdjStepArgs& a);
 void launch_adj_half_dtor(cudaStream_t st, const SimDev* d_sims, long long N, const AdjStepArgs& a);
 void launch_adj_p0(cudaStream_t st, const SimDev* d_sims, long long N, const AdjStepArgs& a, const float* p0s, float* gp);
 void launch_adj_store_grad(cudaStream_t st, const double* gc, float* out, long long n);
+// density gradient: the t = 0 override's u_a = dtor_a / 2 g_a (g_a = D+_a p0 in ADJ_GP):
+// dL/d dtor_a += lambda_u_a g_a / 2
+void launch_adj_rho_p0(cudaStream_t st, const SimDev* d_sims, long long N);
+// dL/drho0 = the direct terms + staggerDensity^T of dL/d rho_sg_a = -dL/d dtor_a dtor_a^2 / dt
+void launch_adj_rho_final(cudaStream_t st, const SimDev* d_sims, long long N, float* out);
 
 }  // namespace kw

@@ -132,6 +132,7 @@ enum Epilogue {
     EPI_ADJ_SUM,         // lambda_p = sum_a d_a; x1 = tau c2 lambda_p; x2 = eta c2 lambda_p
     EPI_ADJ_EOS,         // the reverse equation of state (kw_adjoint.cu k_adj_eos) with d = A1, A2, A2(S)
     EPI_DEN_SRC,         // EPI_DEN + rho_a += signal[t] psrc_q / d_a (precorrected pressure source active)
+    EPI_ADJ_EOS_RHO,     // EPI_ADJ_EOS + the direct terms of dL/drho0
 };
 
 // Source operator of one field variable (SourceOp, KSpaceFirstOrder.swift:129-175).
@@ -179,8 +180,9 @@ struct AdjTapeEntry {
     float* s;              // S(t) = sum_a rho_a
     float* sprev;          // S(t-1)
     float* div;            // Stokes div term
-    float* dd[kMaxComp];   // d_a(t) = D-_a u_a(t) (B/A)
+    float* dd[kMaxComp];   // d_a(t) = D-_a u_a(t) (B/A, or the density gradient)
     float* q2;             // A2(S(t)) (power law with dispersion)
+    float* pprev;          // p(t-1) (density gradient)
 };
 
 struct SimDev {
@@ -211,6 +213,8 @@ struct SimDev {
     float* adj[kAdjFields];     // adjoint work fields (kw_adjoint.cpp), unused by a forward run
     const AdjTapeEntry* tape;   // adjoint recompute: the tape epilogues store into tape[t] (else null)
     double* adj_gc;             // adjoint: dL/dc accumulated in FP64
+    double* adj_gr;             // adjoint: the direct terms of dL/drho0 in FP64 (null: not requested)
+    double* adj_gdtor[kMaxComp];   // adjoint: dL/d(dt / rho_sg_a) in FP64 (with adj_gr)
     int* adj_rev;               // adjoint: the reverse step counter
     float adj_y;                // adjoint: absorption power y
 

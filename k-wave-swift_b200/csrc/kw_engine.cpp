@@ -285,7 +285,8 @@ void Engine::issue_step(bool first) {
         co.gate = GATE_RECU;
         co.name = "colloc";
         issue_job(co, -1);
-        for (int a = 0; a < D; ++a) launch_sample(st(), d_sims_, d_t_, count(), max_pts_, 1, a);
+        if (!tune_mode_)
+            for (int a = 0; a < D; ++a) launch_sample(st(), d_sims_, d_t_, count(), max_pts_, 1, a);
     }
     timed("tick", 0, [&] { launch_tick(st(), d_t_); });
 }
@@ -999,6 +1000,7 @@ void Engine::create(const kw_sim_desc* descs, int n) {
     if (as) create_as_carrier();
     check(cudaStreamSynchronize(st()), "setup sync");
     reset();
+    autotune();
 }
 
 void Engine::reset() {

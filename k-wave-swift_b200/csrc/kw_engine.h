@@ -117,6 +117,7 @@ private:
     };
     template <class F>
     void timed(const std::string& name, double bytes, F&& f) {
+        if (tune_mode_) return;   // only the operator passes run (and are timed) in tune mode
         if (!prof_) { f(); return; }
         ProfRec r{name, bytes, nullptr, nullptr};
         cudaEventCreate(&r.a);
@@ -147,7 +148,8 @@ private:
     void build_plan(FFTPlanDev& pl, int n);
     void smooth_field(int s, float* field);
     const Map& map_rows(int lines_per_row, int ncomp, int sim_only, int sclass);
-    const Map& map_cols(int axis, int ncomp, int sim_only, bool op, int sclass);
+    // tw > 0: tiles of tw columns (the register operator pass of the chosen variant)
+    const Map& map_cols(int axis, int ncomp, int sim_only, bool op, int sclass, int tw = 0);
     const Map& map_elems(int sim_only);
     const Map& map_planes(int ncomp, int sim_only);
     void issue_job(const SpecJob& job, int sim_only);
@@ -186,6 +188,12 @@ private:
     // adjoint and the axisymmetric solver keep the per-step correction job
     bool precorrect_ok_ = true;
     void precorrect_psrc(int s);
+    // autotuner of the operator column pass (kw_tune.cpp)
+    bool tune_mode_ = false;
+    std::string colop_key(int n, int axis, const ColJob& cj, int ntiles) const;
+    ColopVariant colop_choice(int n, const std::string& key) const;
+    void tune_colop(int n, int axis, int ncomp_map, int sim_only, const ColJob& cj, const std::string& key);
+    void autotune();
     cudaStream_t st_override_ = nullptr;   // adjoint: the reverse sweep's own stream while it issues work
     // axisymmetric solver (kw_axisym.cpp): sims_[0] is the [nx][ny] simulation, car_ / d_car_ the
     // descriptor of its 4x radial expansion that the spectral jobs run on

@@ -67,8 +67,8 @@ const Engine::Map& Engine::map_rows(int lines_per_row, int ncomp, int sim_only, 
 
 // Column-pass tiles: col_lines(n) (col_lines_op(n) for an operator pass) contiguous columns, or
 // for the register-plan lengths colr_lines(n) (colop_lines(n)) columns of one plane.
-const Engine::Map& Engine::map_cols(int axis, int ncomp, int sim_only, bool op, int sclass) {
-    auto key = std::make_tuple(1 + axis + (op ? 2 : 0), 0, ncomp, sim_only, sclass);
+const Engine::Map& Engine::map_cols(int axis, int ncomp, int sim_only, bool op, int sclass, int tw_op) {
+    auto key = std::make_tuple(1 + axis + (op ? 2 : 0), tw_op, ncomp, sim_only, sclass);
     auto it = maps_.find(key);
     if (it != maps_.end()) return it->second;
     std::vector<BlockWork> v;
@@ -81,7 +81,7 @@ const Engine::Map& Engine::map_cols(int axis, int ncomp, int sim_only, bool op, 
         int tiles;
         const bool reg = op ? has_colop(sclass) : (has_colp(sclass) || (has_colop(sclass) && !(cola_policy() & 4)));
         if (sclass && reg) {   // register-plan kernels: columns of one plane
-            const int tw = op ? colop_lines(n) : colr_lines(n);
+            const int tw = op ? (tw_op > 0 ? tw_op : colop_lines(n)) : colr_lines(n);
             tiles = outer * ((inner + tw - 1) / tw);
         } else {
             const int tw = op ? col_lines_op(n) : col_lines(n);
@@ -240,8 +240,18 @@ void Engine::issue_job(const SpecJob& job, int sim_only) {
             const int cola = cola_policy();
             if (sc && op && has_colop(sc) && (cola & 1))
                 timed(std::string(label) + job.name, bytes, [&] { launch_cola(st(), d_sims_, d_t_, m.d, m.n, cj, sc); });
-            else if (sc && op && has_colop(sc))
-                timed(std::string(label) + job.name, bytes, [&] { launch_colop(st(), d_sims_, d_t_, m.d, m.n, cj, sc); });
+            else if (sc && op && has_colop(sc)) {
+                // the variant the autotuner chose for this pass (kw_tune.cpp), on its own tile map
+                const std::string key = colop_key(sc, axis, cj, m.n);
+                if (tune_mode_) {
+                    tune_colop(sc, axis, ncomp_map, sim_only, cj, key);
+                } else {
+                    const ColopVariant v = colop_choice(sc, key);
+                    const Map& mv = map_cols(axis, ncomp_map, sim_only, op, sc, colop_tile(sc, v.r1));
+                    timed(std::string(label) + job.name, bytes,
+                          [&] { launch_colop(st(), d_sims_, d_t_, mv.d, mv.n, cj, sc, v); });
+                }
+            }
             else if (sc && !op && has_colp(sc) && !(cola & 2))
                 timed(std::string(label) + job.name, bytes,
                       [&] { launch_colp(st(), d_sims_, d_t_, m.d, m.n, cj, sc, d_flag_ + 1); });

@@ -68,10 +68,18 @@ void launch_col(cudaStream_t st, const SimDev* d_sims, const int* d_t, const Blo
 void launch_row_c2r(cudaStream_t st, const SimDev* d_sims, const int* d_t, const BlockWork* map, int nmap,
                     const RowC2RJob& job, size_t smem, int size_class);
 // register-resident operator column pass for has_colop(n) lengths; one CTA per map entry,
-// whose tile indexes colop_lines(n) consecutive columns (the pass's outer extent is 1)
+// whose tile indexes colop_tile(n, v.r1) consecutive columns (the pass's outer extent is 1).
+// A variant fixes the values per thread (r1) and the launch bound in CTAs per SM (minb, 0: none);
+// colop_variants lists those of length n, the default first.
+struct ColopVariant {
+    int r1;
+    int minb;
+};
+__host__ __device__ constexpr int colop_tile(int n, int r1) { return reg_lines(n, r1); }
+int colop_variants(int n, ColopVariant* out, int max);
 void init_colop_attributes(int optin);
 void launch_colop(cudaStream_t st, const SimDev* d_sims, const int* d_t, const BlockWork* map, int nmap,
-                  const ColJob& job, int n);
+                  const ColJob& job, int n, ColopVariant v);
 // axisymmetric solver (kw_axisym.cu): radial mirror of an [nx][ny] field into the [nx][4 ny]
 // expansion (WSWA: p, ux; HAHS: uy; HSHA: uy / r with over_r), the trimmed updates, sources
 enum AsMirror { AS_WSWA = 0, AS_HAHS, AS_HSHA };

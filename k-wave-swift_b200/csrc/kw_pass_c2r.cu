@@ -139,7 +139,7 @@ __device__ __forceinline__ void epi_point(const SimDev& S, const RowC2RJob& job,
                 // precorrected additive pressure source (SimDev::psrc_q)
                 if (sgain != 0.f) r = r + (sgain * __ldg(S.psrc_q + i)) * S.ax[a].inv_d;
                 S.rho[a][i] = r;
-                if (te && S.nonlinear) te->dd[a][i] = d[a];   // the adjoint's recompute keeps d_a
+                if (te && (S.nonlinear || S.adj_gr)) te->dd[a][i] = d[a];   // the adjoint's recompute keeps d_a
                 rs = a == 0 ? r : rs + r;
                 dv = a == 0 ? d[a] : dv + d[a];
             }

@@ -15,14 +15,25 @@
 
 namespace kw {
 
-// three CTAs per SM (85 registers) up to 256 points; longer lines keep the compiler's choice
-template <int N>
-constexpr int colop_minb() { return N <= 256 ? 3 : 0; }
+// Variants (N, R1, MINB) of the operator pass: R1 values per thread (so N / R1 threads per line and
+// colop_tile(N, R1) lines per CTA) and a launch bound of MINB resident CTAs per SM (0: the
+// compiler's register choice). The first variant of each length is the default: three CTAs per SM
+// (85 registers) up to 256 points, the compiler's choice above. The autotuner (kw_tune.cpp) times
+// the variants of a length on the job it is about to run and keeps the fastest.
+#define KW_COLOP_VARIANTS(X)                                                                            \
+    X(16, 4, 3) X(32, 8, 3) X(24, 12, 3) X(48, 12, 3)                                                   \
+    X(64, 8, 3) X(64, 8, 4) X(64, 16, 3) X(64, 16, 2)                                                   \
+    X(128, 16, 3) X(128, 16, 2) X(128, 8, 3) X(128, 8, 4)                                               \
+    X(256, 16, 3) X(256, 16, 2) X(256, 8, 3) X(256, 8, 4)                                               \
+    X(512, 16, 0) X(512, 16, 2) X(512, 8, 2) X(512, 8, 3) X(512, 8, 4)                                  \
+    X(1024, 16, 0) X(1024, 16, 2) X(1024, 8, 2) X(1024, 8, 3)                                           \
+    X(96, 12, 3) X(96, 12, 2) X(96, 12, 4) X(192, 12, 3) X(192, 12, 2) X(192, 12, 4)                    \
+    X(384, 12, 0) X(384, 12, 2) X(384, 12, 3) X(768, 12, 0) X(768, 12, 2) X(768, 12, 3)
 
-template <int N>
-__global__ void __launch_bounds__(256, colop_minb<N>()) k_colop(const SimDev* __restrict__ sims, const int* __restrict__ d_t,
+template <int N, int R1V, int MINB>
+__global__ void __launch_bounds__(256, MINB) k_colop(const SimDev* __restrict__ sims, const int* __restrict__ d_t,
                                                const BlockWork* __restrict__ map, int nmap, ColJob job) {
-    using P = RegPlan<N, reg_r1(N)>;
+    using P = RegPlan<N, R1V>;
     using Lay = ColLayout<P, N>;
     constexpr int R1 = P::R1, T = P::T, TW = P::LINES;
     __shared__ float2 sh[Lay::SLOTS];
@@ -197,32 +208,50 @@ __global__ void __launch_bounds__(256, 2) k_colop_fanin(const SimDev* __restrict
 
 // dynamic shared memory: the parked product (several outputs, or the fan-in sum) and the radial
 // table slots
-template <int N>
-static size_t colop_park_bytes(const ColJob& job) {
+static size_t colop_park_bytes(const ColJob& job, int r1) {
     const bool park = job.fanin || (job.fanout && job.nout > 1);
     const bool table = !job.fanin && (job.op[0].radial != RT_NONE || job.op[1].radial != RT_NONE || job.op[2].radial != RT_NONE);
-    return (size_t)reg_r1(N) * 256 * ((park ? sizeof(float2) : 0) + (table ? sizeof(float) : 0));
+    return (size_t)r1 * 256 * ((park ? sizeof(float2) : 0) + (table ? sizeof(float) : 0));
 }
 
 void init_colop_attributes(int optin) {
-#define KW_SET(n) set_max_smem((const void*)k_colop<n>, optin); set_max_smem((const void*)k_colop_fanin<n>, optin);
+#define KW_SET(NN, RR, MB) set_max_smem((const void*)k_colop<NN, RR, MB>, optin);
+    KW_COLOP_VARIANTS(KW_SET)
+#undef KW_SET
+#define KW_SET(n) set_max_smem((const void*)k_colop_fanin<n>, optin);
     KW_COLOP_SIZES(KW_SET)
 #undef KW_SET
 }
 
+int colop_variants(int n, ColopVariant* out, int max) {
+    int k = 0;
+#define KW_ADD(NN, RR, MB) \
+    if (n == NN && k < max) out[k++] = ColopVariant{RR, MB};
+    KW_COLOP_VARIANTS(KW_ADD)
+#undef KW_ADD
+    return k;
+}
+
 void launch_colop(cudaStream_t st, const SimDev* d_sims, const int* d_t, const BlockWork* map, int nmap,
-                  const ColJob& job, int n) {
+                  const ColJob& job, int n, ColopVariant v) {
     if (nmap <= 0) return;
-    switch (n) {
-#define KW_CASE(n)                                                                                     \
-    case n:                                                                                            \
-        if (job.fanin) k_colop_fanin<n><<<nmap, 256, colop_park_bytes<n>(job), st>>>(d_sims, d_t, map, nmap, job); \
-        else k_colop<n><<<nmap, 256, colop_park_bytes<n>(job), st>>>(d_sims, d_t, map, nmap, job);                 \
-        break;
-        KW_COLOP_SIZES(KW_CASE)
+    if (job.fanin) {   // one variant (the adjoint's fan-in sum)
+        switch (n) {
+#define KW_CASE(n) \
+    case n: k_colop_fanin<n><<<nmap, 256, colop_park_bytes(job, reg_r1(n)), st>>>(d_sims, d_t, map, nmap, job); break;
+            KW_COLOP_SIZES(KW_CASE)
 #undef KW_CASE
-        default: break;
+            default: break;
+        }
+        return;
     }
+#define KW_CASE(NN, RR, MB)                                                                                 \
+    if (n == NN && v.r1 == RR && v.minb == MB) {                                                            \
+        k_colop<NN, RR, MB><<<nmap, 256, colop_park_bytes(job, RR), st>>>(d_sims, d_t, map, nmap, job);     \
+        return;                                                                                             \
+    }
+    KW_COLOP_VARIANTS(KW_CASE)
+#undef KW_CASE
 }
 
 }  // namespace kw

@@ -29,7 +29,7 @@ namespace kw {
 template <int M, int EPI, bool TAPE>
 constexpr int rowr_minb() {
     // left alone these take 129-152 registers at some lengths (one CTA per SM)
-    if (EPI == EPI_ADJ_EOS || EPI == EPI_ADD_RHO || TAPE || M >= 768) return 2;
+    if (EPI == EPI_ADJ_EOS || EPI == EPI_ADJ_EOS_RHO || EPI == EPI_ADD_RHO || TAPE || M >= 768) return 2;
     // the density update with the precorrected source reads one field more (spills at 85 registers)
     if (EPI == EPI_DEN_SRC) return 2;
     return M <= 128 ? 3 : 0;
@@ -94,7 +94,8 @@ __global__ void __launch_bounds__(256, rowr_minb<M, EPI, TAPE>()) k_rowr_c2r(con
     constexpr int R1 = P::R1, T = P::T, TW = P::LINES;
     // pairs whose inputs are loaded together (the density update reads the most fields)
     constexpr bool DEN = EPI == EPI_DEN || EPI == EPI_DEN_SRC;
-    constexpr int MB = (DEN || EPI == EPI_ADJ_EOS || R1 < 4) ? 2 : 4;
+    constexpr bool AEOS = EPI == EPI_ADJ_EOS || EPI == EPI_ADJ_EOS_RHO;
+    constexpr int MB = (DEN || AEOS || R1 < 4) ? 2 : 4;
     __shared__ float2 sh[Lay::SLOTS];
     extern __shared__ __align__(16) float2 parked[];   // coupled epilogues: [ncomp - 1][R1][256]
     if (blockIdx.x >= nmap) return;
@@ -273,7 +274,7 @@ __global__ void __launch_bounds__(256, rowr_minb<M, EPI, TAPE>()) k_rowr_c2r(con
                 if (S.eos_pointwise) st_state(S.p, e, p2);
                 if constexpr (TAPE) {   // the adjoint's recompute: d_a = D-_a u_a, and S, p, div when they are final here
                     const AdjTapeEntry& te = S.tape[*d_t];
-                    if (DEN && S.nonlinear) {
+                    if (DEN && (S.nonlinear || S.adj_gr)) {   // B/A, or the density gradient
 #pragma unroll
                         for (int a = 0; a < kMaxComp; ++a)
                             if (a < D) st_state(te.dd[a], e, dpair(a, m));
@@ -305,13 +306,20 @@ __global__ void __launch_bounds__(256, rowr_minb<M, EPI, TAPE>()) k_rowr_c2r(con
             for (int b = 0; b < MB; ++b) {
                 const float2 d = v[m0 + b];
                 float2 lo, wo;
+                const long long e = rbase + 2 * (t + T * (m0 + b));
+                if (S.adj_gr) {   // density gradient: dL/d dtor_a += -sg_a g_a mu_a, g_a = D+_a p(t-1)
+                    const float2 gp = ld_ro(S.adj[ADJ_GP + a], e);
+                    double2 gd = *reinterpret_cast<const double2*>(S.adj_gdtor[a] + e);
+                    gd.x -= (double)sg[b].x * gp.x * (uu[b].x - d.x);
+                    gd.y -= (double)sg[b].y * gp.y * (uu[b].y - d.y);
+                    *reinterpret_cast<double2*>(S.adj_gdtor[a] + e) = gd;
+                }
 #pragma unroll
                 for (int h = 0; h < 2; ++h) {
                     const float mu = half(uu[b], h) - (h ? d.y : d.x);
                     half(lo, h) = half(sg[b], h) * half(sg[b], h) * mu;
                     half(wo, h) = half(sg[b], h) * half(dr[b], h) * mu;
                 }
-                const long long e = rbase + 2 * (t + T * (m0 + b));
                 st_state(lu, e, lo);
                 st_state(w, e, wo);
             }
@@ -345,7 +353,7 @@ __global__ void __launch_bounds__(256, rowr_minb<M, EPI, TAPE>()) k_rowr_c2r(con
                         st_state(S.adj[ADJ_X2], e, make_float2(eta[b].x * c2[b].x * s2.x, eta[b].y * c2[b].y * s2.y));
                 }
             }
-        } else if constexpr (EPI == EPI_ADJ_EOS) {
+        } else if constexpr (AEOS) {
             // the reverse equation of state of kw_adjoint.cu (k_adj_eos), with the absorption
             // filters' outputs d = A1(tau c^2 lambda_p), A2(eta c^2 lambda_p), A2(S(t)) in hand
             const int tt = *d_t;
@@ -372,8 +380,10 @@ __global__ void __launch_bounds__(256, rowr_minb<M, EPI, TAPE>()) k_rowr_c2r(con
                 for (int a = 0; a < kMaxComp; ++a)
                     if (a < D) {
                         lr[a] = ld_state(S.adj[ADJ_LR + a], e);
-                        if (S.nonlinear) dd[a] = ld_ro(S.adj[ADJ_DDP + a], e);
+                        if (S.nonlinear || EPI == EPI_ADJ_EOS_RHO) dd[a] = ld_ro(S.adj[ADJ_DDP + a], e);
                     }
+                double2 grv = make_double2(0.0, 0.0);
+                if constexpr (EPI == EPI_ADJ_EOS_RHO) grv = *reinterpret_cast<const double2*>(S.adj_gr + e);
                 const float2 pmr = row_pair(S.ax[D - 1].pml, n);
                 const float2 a1 = dpair(0, m);
                 float2 a2 = make_float2(0.f, 0.f), q2 = a2;
@@ -416,8 +426,25 @@ __global__ void __launch_bounds__(256, rowr_minb<M, EPI, TAPE>()) k_rowr_c2r(con
                         half(lro[a], h) = pmv[a] * pmv[a] * lam[a] + lsprev;
                     }
                     half(sg2, h) = sig;
+                    if constexpr (EPI == EPI_ADJ_EOS_RHO) {
+                        // direct terms of dL/drho0: the absorption input rho0 div, B/A S^2 / (2 rho0),
+                        // and d(dt rho0 nl) / d rho0 = dt in each density update
+                        float sd = 0.f;
+                        double g = 0.0;
+#pragma unroll
+                        for (int a = 0; a < kMaxComp; ++a) {
+                            if (a >= D) break;
+                            const float dv = h ? dd[a].y : dd[a].x;
+                            sd += dv;
+                            g -= (double)pmv[a] * S.dt * dv * lam[a];
+                        }
+                        g += (double)ldiv * sd;
+                        if (S.nonlinear) g -= (double)lE * bo * s_ * s_ / (2.0 * (double)rr0 * rr0);
+                        if (h) grv.y += g; else grv.x += g;
+                    }
                 }
                 *reinterpret_cast<double2*>(S.adj_gc + e) = gcv;
+                if constexpr (EPI == EPI_ADJ_EOS_RHO) *reinterpret_cast<double2*>(S.adj_gr + e) = grv;
 #pragma unroll
                 for (int a = 0; a < kMaxComp; ++a)
                     if (a < D) { st_state(S.adj[ADJ_LR + a], e, lro[a]); st_state(S.adj[ADJ_W + a], e, wo[a]); }
@@ -485,6 +512,7 @@ void init_rowr_attributes(int optin) {
     set_rowr_attrs<EPI_EOS_ABS, true>(optin);
     set_rowr_attrs<EPI_ADJ_SUM>(optin);
     set_rowr_attrs<EPI_ADJ_EOS>(optin);
+    set_rowr_attrs<EPI_ADJ_EOS_RHO>(optin);
 }
 
 void launch_rowr_r2c(cudaStream_t st, const SimDev* d_sims, const int* d_t, const BlockWork* map, int nmap,
@@ -524,6 +552,7 @@ static void launch_c2r_m(cudaStream_t st, const SimDev* d_sims, const int* d_t, 
         case EPI_ADJ_VEL: k_rowr_c2r<M, EPI_ADJ_VEL><<<nmap, 256, smem, st>>>(d_sims, d_t, map, nmap, job); break;
         case EPI_ADJ_SUM: k_rowr_c2r<M, EPI_ADJ_SUM><<<nmap, 256, smem, st>>>(d_sims, d_t, map, nmap, job); break;
         case EPI_ADJ_EOS: k_rowr_c2r<M, EPI_ADJ_EOS><<<nmap, 256, smem, st>>>(d_sims, d_t, map, nmap, job); break;
+        case EPI_ADJ_EOS_RHO: k_rowr_c2r<M, EPI_ADJ_EOS_RHO><<<nmap, 256, smem, st>>>(d_sims, d_t, map, nmap, job); break;
         default: break;
     }
 }

@@ -123,6 +123,7 @@ class kw_adjoint_desc(C.Structure):
 
 
 KW_CHECKPOINT_SQRT, KW_CHECKPOINT_INTERVAL, KW_CHECKPOINT_BUDGET, KW_CHECKPOINT_STORE_ALL = 0, 1, 2, 3
+KW_CHECKPOINT_REVOLVE = 4
 
 # Every symbol include/kwave_cuda.h declares, with its ctypes signature.
 P = C.c_void_p

@@ -387,6 +387,7 @@ class AdjointOutput:
     misfit: float
     gradSoundSpeed: Optional[np.ndarray]
     gradP0: Optional[np.ndarray]
+    gradRho0: Optional[np.ndarray]
     forwardMs: float
     reverseMs: float
     checkpointInterval: int
@@ -396,17 +397,18 @@ class AdjointOutput:
 def kspaceFirstOrderAdjoint(grid: KWaveGrid, medium: KWaveMedium, source: KWaveSource, sensor: KWaveSensor,
                             data: np.ndarray, options: Optional[SimulationOptions] = None,
                             gradP0: bool = False, checkpointPolicy: int = abi.KW_CHECKPOINT_SQRT,
-                            checkpointInterval: int = 0, memoryBudget: float = 0.0) -> AdjointOutput:
+                            checkpointInterval: int = 0, memoryBudget: float = 0.0,
+                            gradRho0: bool = False) -> AdjointOutput:
     """Misfit 1/2 sum (p_sensor - data)^2 of the forward kspaceFirstOrder run and its gradients
-    with respect to the sound speed (and the initial pressure), by the discrete adjoint
-    (kw_adjoint_run). `data` has the layout of the p output, [n_sensor, nt]."""
+    with respect to the sound speed (and the initial pressure, and the density), by the discrete
+    adjoint (kw_adjoint_run). `data` has the layout of the p output, [n_sensor, nt]."""
     from .runtime import Context
 
     options = options or SimulationOptions()
     with Context.default() as ctx:
         r = ctx.adjoint(DescBuilder(grid, medium, source, sensor, options), data, True, gradP0,
-                        checkpointPolicy, checkpointInterval, memoryBudget)
-    return AdjointOutput(r["misfit"], r["grad_c0"], r["grad_p0"], r["forward_ms"], r["reverse_ms"],
+                        checkpointPolicy, checkpointInterval, memoryBudget, grad_rho0=gradRho0)
+    return AdjointOutput(r["misfit"], r["grad_c0"], r["grad_p0"], r["grad_rho0"], r["forward_ms"], r["reverse_ms"],
                          r["interval"], r["checkpoints"])
 
 

@@ -81,7 +81,8 @@ class Context:
         return Batch(self, builders)
 
     def adjoint(self, builder: DescBuilder, data: np.ndarray, grad_c0: bool = True, grad_p0: bool = False,
-                policy: int = abi.KW_CHECKPOINT_SQRT, interval: int = 0, memory_budget: float = 0.0) -> dict:
+                policy: int = abi.KW_CHECKPOINT_SQRT, interval: int = 0, memory_budget: float = 0.0,
+                grad_rho0: bool = False) -> dict:
         """kw_adjoint_run: misfit 1/2 sum (p_sensor - data)^2 and its gradients (see the header)."""
         d = np.ascontiguousarray(data, dtype=np.float32)
         shape = builder.shape
@@ -93,12 +94,15 @@ class Context:
         a.memory_budget = float(memory_budget)
         gc = np.zeros(shape, np.float32) if grad_c0 else None
         gp = np.zeros(shape, np.float32) if grad_p0 else None
+        gr = np.zeros(shape, np.float32) if grad_rho0 else None
+        if gr is not None:
+            a.grad_rho0 = gr.ctypes.data_as(C.POINTER(C.c_float))
         if gc is not None:
             a.grad_c0 = gc.ctypes.data_as(C.POINTER(C.c_float))
         if gp is not None:
             a.grad_p0 = gp.ctypes.data_as(C.POINTER(C.c_float))
         _check(self.lib, self.h, self.lib.kw_adjoint_run(self.h, C.byref(builder.desc), C.byref(a)))
-        return {"misfit": a.misfit, "grad_c0": gc, "grad_p0": gp, "forward_ms": a.forward_ms,
+        return {"misfit": a.misfit, "grad_c0": gc, "grad_p0": gp, "grad_rho0": gr, "forward_ms": a.forward_ms,
                 "reverse_ms": a.reverse_ms, "interval": a.interval, "checkpoints": a.checkpoints}
 
 

@@ -289,13 +289,13 @@ public enum CheckpointPolicy {
 }
 
 /// Gradients of the sensor-data misfit L = 1/2 sum (p_sensor - data)^2 of kspaceFirstOrder with
-/// respect to the sound speed and (with `source.p0`) the initial pressure, by the discrete
-/// adjoint of the time step (no counterpart in the reference). `data` has the p output's shape
-/// [nSensor, nt].
+/// respect to the sound speed, the density (`gradRho0`) and (with `source.p0`) the initial
+/// pressure, by the discrete adjoint of the time step (no counterpart in the reference). `data`
+/// has the p output's shape [nSensor, nt].
 public func kspaceFirstOrderAdjoint(grid: KWaveGrid, medium: KWaveMedium, source: KWaveSource,
                                     sensor: KWaveSensor, data: MLXArray, options: SimulationOptions = .init(),
-                                    gradP0: Bool = false, policy: CheckpointPolicy = .sqrtNt)
-    -> (misfit: Double, gradC0: MLXArray, gradP0: MLXArray?) {
+                                    gradP0: Bool = false, gradRho0: Bool = false, policy: CheckpointPolicy = .sqrtNt)
+    -> (misfit: Double, gradC0: MLXArray, gradP0: MLXArray?, gradRho0: MLXArray?) {
     let ctx = CUDAContext()
     let buffers = HostBuffers()
     var d = makeDescriptor(grid: grid, medium: medium, source: source, sensor: sensor, options: options,
@@ -312,17 +312,21 @@ public func kspaceFirstOrderAdjoint(grid: KWaveGrid, medium: KWaveMedium, source
     let observed = buffers.floats(data)
     var gc = [Float](repeating: 0, count: n)
     var gp = [Float](repeating: 0, count: gradP0 ? n : 0)
+    var gr = [Float](repeating: 0, count: gradRho0 ? n : 0)
     let status: Int32 = observed.withUnsafeBufferPointer { op in
         gc.withUnsafeMutableBufferPointer { gcp in
             gp.withUnsafeMutableBufferPointer { gpp in
-                a.data = op.baseAddress
-                a.grad_c0 = gcp.baseAddress
-                a.grad_p0 = gradP0 ? gpp.baseAddress : nil
-                return kw_adjoint_run(ctx.handle, &d, &a)
+                gr.withUnsafeMutableBufferPointer { grp in
+                    a.data = op.baseAddress
+                    a.grad_c0 = gcp.baseAddress
+                    a.grad_p0 = gradP0 ? gpp.baseAddress : nil
+                    a.grad_rho0 = gradRho0 ? grp.baseAddress : nil
+                    return kw_adjoint_run(ctx.handle, &d, &a)
+                }
             }
         }
     }
     ctx.check(status, "kw_adjoint_run")
     let shape = gridShape(grid)
-    return (a.misfit, MLXArray(gc, shape), gradP0 ? MLXArray(gp, shape) : nil)
+    return (a.misfit, MLXArray(gc, shape), gradP0 ? MLXArray(gp, shape) : nil, gradRho0 ? MLXArray(gr, shape) : nil)
 }

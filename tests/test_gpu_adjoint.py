@@ -1,8 +1,8 @@
 """Device discrete adjoint (kw_adjoint_run through the C ABI) against the FP64 oracle adjoint and
 FP64 central finite differences of the oracle's misfit.
 
-Tolerances (FP32 device arithmetic): misfit relative error <= 1e-3; gradient fields relative L2
-<= 2e-3 against the FP64 adjoint; directional derivatives within 1e-3 of the finite differences
+Tolerances (FP32 device arithmetic): misfit relative error <= 1e-3; gradient fields (c0, p0, rho0)
+relative L2 <= 2e-3 against the FP64 adjoint; directional derivatives within 1e-3 of the finite differences
 (2e-3 for the replica of the 512^2 configuration, whose 1 % speed error leaves a small misfit);
 the checkpoint policies agree to 1e-5.
 """
@@ -27,8 +27,9 @@ CASES = [
 ]
 
 
-def gpu_adjoint(shape, c, p0, data, kw, **opt):
-    return Context.default().adjoint(builder(shape, c, p0, **kw), data, grad_c0=True, grad_p0=p0 is not None, **opt)
+def gpu_adjoint(shape, c, p0, data, kw, grad_rho0=False, **opt):
+    return Context.default().adjoint(builder(shape, c, p0, **kw), data, grad_c0=True, grad_p0=p0 is not None,
+                                     grad_rho0=grad_rho0, **opt)
 
 
 @pytest.mark.parametrize("shape,kw", CASES)
@@ -172,3 +173,73 @@ def test_adjoint3d_configuration_replica():
     assert r["checkpoints"] > 0
     assert abs(r["misfit"] - L) <= 1e-3 * L
     assert rel_l2(r["grad_c0"], gc) < 2e-3, rel_l2(r["grad_c0"], gc)
+
+
+@pytest.mark.parametrize("shape,kw,fused_eos", [
+    (CASES[0][0], CASES[0][1], "0"), (CASES[1][0], CASES[1][1], "0"), (CASES[2][0], CASES[2][1], "0"),
+    (CASES[3][0], CASES[3][1], "0"), (CASES[4][0], CASES[4][1], "0"), (CASES[5][0], CASES[5][1], "0"),
+    ((40, 64), dict(absorb="powerlaw", nonlinear=True, cartesian=True, nt=50), "1"),
+    ((16, 20, 32), dict(absorb="powerlaw", nonlinear=False, nt=30), "1")])
+def test_device_density_gradient(shape, kw, fused_eos, monkeypatch):
+    # dL/drho0 (dt rho0 nl, dt / staggerDensity(rho0), rho0 div, B/A S^2 / (2 rho0)) against the FP64
+    # adjoint at 2e-3 relative L2 and FP64 central differences at 2e-3 (the density directional
+    # derivatives cancel more than the sound speed's, so the FP32 rounding of the device gradient
+    # shows at the 1e-3 level there); rows of 64 points take the register
+    # kernels with the reverse equation of state fused (forced here), the others the elementwise ones
+    monkeypatch.setenv("KW_ADJOINT_FUSED_EOS", fused_eos)
+    c, p0, data, kw = problem(shape, **kw)
+    L, gc, gp, gr = oracle.adjoint(builder(shape, c, p0, **kw), data, grad_rho0=True)
+    r = gpu_adjoint(shape, c, p0, data, kw, grad_rho0=True)
+    assert abs(r["misfit"] - L) <= 1e-3 * L
+    assert rel_l2(r["grad_c0"], gc) < 2e-3, rel_l2(r["grad_c0"], gc)
+    e_l2 = rel_l2(r["grad_rho0"], gr)
+    assert e_l2 < 2e-3, e_l2
+    rng = np.random.default_rng(4)
+    for _ in range(2):
+        v = rng.standard_normal(shape)
+        dL, dx = fd_misfit_diff(shape, c, p0, data, v, 0.1, "rho", kw)
+        e_fd = abs(dL - np.sum(r["grad_rho0"] * dx)) / abs(dL)
+        e_64 = abs(np.sum((r["grad_rho0"] - gr) * v)) / abs(np.sum(gr * v))   # against the FP64 adjoint
+        print(f"\n{shape} {kw}: rel L2 {e_l2:.2e}, directional vs FD {e_fd:.2e}, vs FP64 adjoint {e_64:.2e}")
+        assert e_fd <= 2e-3, (e_fd, e_64)
+
+
+def test_density_gradient_checkpoint_policies_agree():
+    # p(t-1) of a segment's first step comes from its checkpoint, of the others from the tape;
+    # the overlapped and sequential reverse sweeps agree too
+    shape = (40, 36)
+    c, p0, data, kw = problem(shape, absorb="powerlaw", nonlinear=True, nt=45)
+    runs = [gpu_adjoint(shape, c, p0, data, kw, grad_rho0=True, policy=abi.KW_CHECKPOINT_STORE_ALL),
+            gpu_adjoint(shape, c, p0, data, kw, grad_rho0=True, policy=abi.KW_CHECKPOINT_SQRT),
+            gpu_adjoint(shape, c, p0, data, kw, grad_rho0=True, policy=abi.KW_CHECKPOINT_INTERVAL, interval=6)]
+    for r in runs[1:]:
+        assert r["checkpoints"] > 2
+        assert rel_l2(r["grad_rho0"], runs[0]["grad_rho0"]) < 1e-5
+        assert rel_l2(r["grad_c0"], runs[0]["grad_c0"]) < 1e-5
+
+
+@pytest.mark.parametrize("snapshots", [1, 3, 6])
+def test_revolve_matches_store_all(snapshots):
+    # the binomial (revolve) schedule with 1, 3 and 6 state snapshots (one tape slot) against
+    # keeping every state: the 48^3 power-law + B/A problem, gradients of c0, p0 and rho0
+    shape = (48, 48, 48)
+    c, p0, data, kw = problem(shape, absorb="powerlaw", nonlinear=True, cartesian=True, nt=40)
+    ref = gpu_adjoint(shape, c, p0, data, kw, grad_rho0=True, policy=abi.KW_CHECKPOINT_STORE_ALL)
+    r = gpu_adjoint(shape, c, p0, data, kw, grad_rho0=True, policy=abi.KW_CHECKPOINT_REVOLVE, interval=snapshots)
+    assert r["checkpoints"] == snapshots and r["interval"] == 0
+    assert abs(r["misfit"] - ref["misfit"]) <= 1e-6 * ref["misfit"]
+    for g in ("grad_c0", "grad_p0", "grad_rho0"):
+        assert rel_l2(r[g], ref[g]) < 1e-5, (g, rel_l2(r[g], ref[g]))
+
+
+def test_budget_falls_back_to_revolve():
+    # a memory budget below every uniform interval's needs (checkpoints + tape slots) but above a
+    # few snapshots takes the binomial schedule
+    shape = (40, 36)
+    c, p0, data, kw = problem(shape, absorb="powerlaw", nonlinear=True, nt=45)
+    fb = 40 * 36 * 4
+    ref = gpu_adjoint(shape, c, p0, data, kw, policy=abi.KW_CHECKPOINT_STORE_ALL)
+    r = gpu_adjoint(shape, c, p0, data, kw, policy=abi.KW_CHECKPOINT_BUDGET, memory_budget=60.0 * fb)
+    assert r["interval"] == 0 and r["checkpoints"] == 7   # (60 - 5 tape - 2) // 7 fields per snapshot
+    assert rel_l2(r["grad_c0"], ref["grad_c0"]) < 1e-5
+    assert rel_l2(r["grad_p0"], ref["grad_p0"]) < 1e-5

@@ -222,7 +222,10 @@ def test_plane_pass_shapes(shape, plane, monkeypatch):
     compare(out, ref)
 
 
-def test_batch_equals_individual_runs():
+def test_batch_equals_individual_runs(monkeypatch):
+    # bit for bit with fixed kernel variants (the autotuner may pick another radix split for the
+    # batch's larger launches, whose results then differ in the last bits)
+    monkeypatch.setenv("KW_AUTOTUNE", "0")
     rng = np.random.default_rng(3)
     builders = []
     for n in (48, 64, 40):
@@ -247,9 +250,10 @@ def test_batch_equals_individual_runs():
         batch.close()
 
 
-def test_batch_with_and_without_directivity():
+def test_batch_with_and_without_directivity(monkeypatch):
     # the per-angle filter jobs gate themselves per simulation: a batch mixing a directivity
     # sensor, a plain sensor and a second angle set gives each simulation's own run
+    monkeypatch.setenv("KW_AUTOTUNE", "0")
     builders = [builder_from_case(load_golden(n)[0]) for n in ("2d_directivity_pressure", "2d_ivp",
                                                                "2d_directivity_gradient")]
     singles = [run_gpu(b) for b in builders]
