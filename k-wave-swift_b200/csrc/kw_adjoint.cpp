@@ -420,7 +420,7 @@ void Engine::adjoint(const kw_sim_desc& din, kw_adjoint_desc& a) {
             issue_job(gj, -1);
         }
         if (fused) {
-            job(ADJ_W, ADJ_E, D, deriv(AO_DPOS), EPI_ADJ_VEL, 0, "adj_vel");
+            job(ADJ_W, ADJ_E, D, deriv(AO_DPOS), grho ? EPI_ADJ_VEL_RHO : EPI_ADJ_VEL, 0, "adj_vel");
             // lambda_p = sum_a D-_a w_a: the operator pass sums the components' spectra, so one
             // inverse transform serves all of them
             job(ADJ_W, ADJ_E, D, deriv(AO_DNEG), EPI_ADJ_SUM, 1, "adj_sum", fanin ? 1 : 0);

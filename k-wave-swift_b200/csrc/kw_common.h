@@ -133,6 +133,7 @@ enum Epilogue {
     EPI_ADJ_EOS,         // the reverse equation of state (kw_adjoint.cu k_adj_eos) with d = A1, A2, A2(S)
     EPI_DEN_SRC,         // EPI_DEN + rho_a += signal[t] psrc_q / d_a (precorrected pressure source active)
     EPI_ADJ_EOS_RHO,     // EPI_ADJ_EOS + the direct terms of dL/drho0
+    EPI_ADJ_VEL_RHO,     // EPI_ADJ_VEL + dL/d(dt / rho_sg_a) += -sg_a g_a mu (density gradient)
 };
 
 // Source operator of one field variable (SourceOp, KSpaceFirstOrder.swift:129-175).

@@ -162,6 +162,13 @@ void Engine::issue_step(bool first) {
     }
     const int D = dim_;
     const int sp1 = D == 1 ? 0 : 1;   // first output spectrum
+    // row fusion (kw_jobs.cpp): the velocity C2R transforms the new u_a into the density job's
+    // spectra unless a velocity source changes u in between; the density C2R transforms
+    // rho0 div u and rho_sum into the absorption job's spectra unless a pressure source job or a
+    // Dirichlet source changes them in between (and not while the adjoint tape is recorded)
+    const bool fuse = D >= 2 && fuse_rows();
+    const bool fuse_vel = fuse && !any_u_direct_ && !any_u_add_;
+    const bool fuse_den = fuse && any_abs_ && !tape_mode_ && !any_p_direct_ && !any_p_add_;
 
     // velocity update: u_a = pml_sg (pml_sg u_a - dt/rho_sg Re F^-1(ddPos_a kappa F(p)))
     SpecJob vel;
@@ -173,6 +180,7 @@ void Engine::issue_step(bool first) {
     vel.spec_in = 0;
     vel.spec_out = sp1;
     vel.epi = EPI_VEL;
+    vel.fwd_spec = fuse_vel ? sp1 : -1;   // the density job's input spectra
     vel.name = "vel";
     issue_job(vel, -1);
 
@@ -204,6 +212,8 @@ void Engine::issue_step(bool first) {
     den.epi = psrc_live() ? EPI_DEN_SRC : EPI_DEN;
     den.tape = tape_mode_ ? 1 : 0;
     den.coupled = 1;
+    den.r2c_done = fuse_vel ? 1 : 0;
+    den.fwd_spec = fuse_den ? 0 : -1;   // the absorption job's input spectra
     den.name = "den";
     issue_job(den, -1);
 
@@ -239,6 +249,7 @@ void Engine::issue_step(bool first) {
         ab.tape = tape_mode_ ? 1 : 0;
         ab.coupled = 1;
         ab.gate = GATE_ABS;
+        ab.r2c_done = fuse_den ? 1 : 0;
         ab.name = "abs";
         issue_job(ab, -1);
     }
@@ -249,6 +260,7 @@ void Engine::issue_step(bool first) {
         launch_init_p0(st(), d_sims_, d_t_, m.d, m.n, d_p0s_);
         SpecJob vi = vel;
         vi.epi = EPI_VEL_INIT;
+        vi.fwd_spec = -1;
         vi.gate = GATE_P0;
         vi.name = "vel0";
         issue_job(vi, -1);
@@ -512,7 +524,7 @@ void Engine::setup_sim(int s, const kw_sim_desc& d) {
 
     // ---- medium; smoothing on the device (KSFO:367-373) ----
     const bool c0map = d.sound_speed.len > 1, rho0map = d.density.len > 1;
-    std::vector<double> c0(c0map ? N : 1), rho0(rho0map ? N : 1);
+    std::vector<double> c0(c0map ? N : 1), rho0(rho0map && d.smooth_rho0 ? N : 1);
     auto smooth_to_host = [&](const float* src, std::vector<double>& dst) {
         float* f = (float*)dalloc(fb);
         check(cudaMemcpyAsync(f, src, fb, cudaMemcpyHostToDevice, st()), "upload");
@@ -579,14 +591,16 @@ void Engine::setup_sim(int s, const kw_sim_desc& d) {
         v.radial[RT_WINDOW] = upload(tab);
         build_tensor_maps(h, v);   // the smoothing jobs below run the TMA-fed column pass
     }
+    // the (smoothed) maps stay on the device: the medium-derived fields are computed there in FP64
+    // (kw_setup.cu); the host keeps c0 for c_ref and the source scales
     float* d_c0 = nullptr;
     float* d_rho0 = nullptr;
     if (d.smooth_c0 && c0map) d_c0 = smooth_to_host(d.sound_speed.data, c0);
     else parallel_for((long long)c0.size(), [&](long long i) { c0[i] = d.sound_speed.data[i]; });
+    if (c0map && !d_c0) d_c0 = upload_floats(d.sound_speed.data, N);
     if (d.smooth_rho0 && rho0map) d_rho0 = smooth_to_host(d.density.data, rho0);
-    else parallel_for((long long)rho0.size(), [&](long long i) { rho0[i] = d.density.data[i]; });
-    (void)d_c0;
-    (void)d_rho0;
+    else if (rho0map) d_rho0 = upload_floats(d.density.data, N);
+    else rho0[0] = d.density.data[0];
     if (d.p0) {
         float* f = (float*)dalloc(fb);
         check(cudaMemcpyAsync(f, d.p0, fb, cudaMemcpyHostToDevice, st()), "upload p0");
@@ -598,11 +612,19 @@ void Engine::setup_sim(int s, const kw_sim_desc& d) {
         v.has_p0 = 1;
     }
     auto c0_at = [&](long long i) { return c0map ? c0[i] : c0[0]; };
-    auto rho0_at = [&](long long i) { return rho0map ? rho0[i] : rho0[0]; };
 
     // referenceSoundSpeed (KSFO:786-788), or the caller's fixed value
     double cref = c0[0];
-    if (c0map) for (double x : c0) cref = std::max(cref, x);
+    if (c0map) {
+        const long long nchunk = 64, per = (N + nchunk - 1) / nchunk;
+        std::vector<double> part(nchunk, c0[0]);
+        parallel_for(nchunk, [&](long long ch) {
+            double m = c0[0];
+            for (long long i = ch * per; i < std::min(N, (ch + 1) * per); ++i) m = std::max(m, c0[i]);
+            part[ch] = m;
+        });
+        for (double x : part) cref = std::max(cref, x);
+    }
     if (!std::isnan(d.c_ref)) cref = d.c_ref;
     h.cref = cref;
     const double dt = d.dt;
@@ -632,29 +654,30 @@ void Engine::setup_sim(int s, const kw_sim_desc& d) {
     }
 
     // ---- medium-derived quantities ----
-    auto field_or_scalar = [&](bool map, auto f) {
-        FieldOrScalar r{nullptr, 0.f};
-        if (!map) { r.s = (float)f(0); return r; }
-        std::vector<float> tmp(N);
-        parallel_for(N, [&](long long i) { tmp[i] = (float)f(i); });
-        r.ptr = upload(tmp);
-        return r;
-    };
-    v.c2 = field_or_scalar(c0map, [&](long long i) { return c0_at(i) * c0_at(i); });
+    // maps computed on the device in FP64 (kw_setup.cu), scalars here
+    if (c0map) {
+        float* c2 = (float*)dalloc(fb);
+        launch_setup_c2(st(), d_c0, c2, N);
+        v.c2 = FieldOrScalar{c2, 0.f};
+    } else {
+        v.c2 = FieldOrScalar{nullptr, (float)(c0[0] * c0[0])};
+    }
     v.dt = (float)dt;
-    v.rho0 = field_or_scalar(rho0map, [&](long long i) { return rho0_at(i); });
+    v.rho0 = rho0map ? FieldOrScalar{d_rho0, 0.f} : FieldOrScalar{nullptr, (float)rho0[0]};
     for (int a = 0; a < h.dim; ++a) {
         // staggerDensity (KSFO:799-806): mean of neighbours, last index replicated
         const int L = a + 3 - h.dim;
         const long long stride = L == 2 ? 1 : (L == 1 ? h.C : (long long)h.B * h.C);
         const int n = h.n_ref[a];
-        v.dtor[a] = field_or_scalar(rho0map, [&](long long i) {
-            if (!rho0map) return dt / rho0[0];
-            const long long ia = (i / stride) % n;
-            const double sg = ia < n - 1 ? 0.5 * (rho0[i] + rho0[i + stride]) : rho0[i];
-            return dt / sg;
-        });
+        if (rho0map) {
+            float* q = (float*)dalloc(fb);
+            launch_setup_dtor(st(), d_rho0, q, N, stride, n, dt);
+            v.dtor[a] = FieldOrScalar{q, 0.f};
+        } else {
+            v.dtor[a] = FieldOrScalar{nullptr, (float)(dt / rho0[0])};
+        }
     }
+    check(cudaGetLastError(), "setup kernels");
 
     // absorption (KSFO:851-882)
     v.absorb = 0;
@@ -666,16 +689,22 @@ void Engine::setup_sim(int s, const kw_sim_desc& d) {
         const double np1 = db2neper(1.0, y);
         auto anp = [&](long long i) { return (double)d.alpha_coeff.data[amap ? i : 0] * np1; };
         const bool stokes = d.alpha_mode == KW_ABSORPTION_STOKES || std::fabs(y - 2.0) < 1e-10;
-        if (stokes) {
-            v.absorb = 1;
-            v.tau = field_or_scalar(amap || c0map, [&](long long i) { return -2.0 * anp(i) * c0_at(i); });
+        v.absorb = stokes ? 1 : (d.alpha_mode == KW_ABSORPTION_NO_DISPERSION ? 2 : 3);
+        const double tn = std::tan(M_PI * y / 2.0);
+        if (amap || c0map) {   // on the device in FP64 (kw_setup.cu)
+            const float* d_alpha = amap ? upload_floats(d.alpha_coeff.data, N) : nullptr;
+            float* tau = (float*)dalloc(fb);
+            float* eta = v.absorb == 3 ? (float*)dalloc(fb) : nullptr;
+            launch_setup_absorb(st(), c0map ? d_c0 : nullptr, c0[0], d_alpha, (double)d.alpha_coeff.data[0], np1, y,
+                                stokes ? 1 : 0, tn, tau, eta, N);
+            check(cudaGetLastError(), "setup absorption");
+            v.tau = FieldOrScalar{tau, 0.f};
+            if (eta) v.eta = FieldOrScalar{eta, 0.f};
+        } else if (stokes) {
+            v.tau = FieldOrScalar{nullptr, (float)(-2.0 * anp(0) * c0[0])};
         } else {
-            v.absorb = d.alpha_mode == KW_ABSORPTION_NO_DISPERSION ? 2 : 3;
-            v.tau = field_or_scalar(amap || c0map, [&](long long i) { return -2.0 * anp(i) * std::pow(c0_at(i), y - 1.0); });
-            if (v.absorb == 3) {
-                const double tn = std::tan(M_PI * y / 2.0);
-                v.eta = field_or_scalar(amap || c0map, [&](long long i) { return 2.0 * anp(i) * std::pow(c0_at(i), y) * tn; });
-            }
+            v.tau = FieldOrScalar{nullptr, (float)(-2.0 * anp(0) * std::pow(c0[0], y - 1.0))};
+            if (v.absorb == 3) v.eta = FieldOrScalar{nullptr, (float)(2.0 * anp(0) * std::pow(c0[0], y) * tn)};
         }
         v.div_term = (float*)dalloc(fb);
     }
@@ -688,7 +717,7 @@ void Engine::setup_sim(int s, const kw_sim_desc& d) {
         for (size_t i = 0; i < d.b_on_a.len; ++i) mx = std::max(mx, (double)std::fabs(d.b_on_a.data[i]));
         if (mx != 0.0) {
             v.nonlinear = 1;
-            v.bona = field_or_scalar(bmap, [&](long long i) { return (double)d.b_on_a.data[bmap ? i : 0]; });
+            v.bona = bmap ? FieldOrScalar{upload_floats(d.b_on_a.data, N), 0.f} : FieldOrScalar{nullptr, d.b_on_a.data[0]};
         }
     }
 
@@ -774,32 +803,22 @@ void Engine::setup_sim(int s, const kw_sim_desc& d) {
             std::vector<double>& dst = L == 0 ? kA : (L == 1 ? kB : kC);
             dst = kv[a];
         }
-        const size_t Ns = (size_t)h.Ns;
-        std::vector<float> kap(Ns, 0.f), skap, nu1, nu2;
-        if (need_skappa) skap.assign(Ns, 0.f);
-        if (v.absorb >= 2) { nu1.assign(Ns, 0.f); if (v.absorb == 3) nu2.assign(Ns, 0.f); }
-        const double half = cref * dt / 2.0;
-        const int absorb = v.absorb;
-        parallel_for((long long)h.A * h.B * h.Ch, [&](long long q) {
-            const int kc = (int)(q % h.Ch);
-            const long long r = q / h.Ch;
-            const int ib = (int)(r % h.B), ia = (int)(r / h.B);
-            const size_t i = ((size_t)ia * h.B + ib) * h.Cp + kc;
-            const double k = std::sqrt(kA[ia] * kA[ia] + kB[ib] * kB[ib] + kC[kc] * kC[kc]);
-            const double arg = k * half;
-            kap[i] = (float)(arg == 0.0 ? 1.0 : std::sin(arg) / arg);
-            if (need_skappa) skap[i] = (float)std::cos(arg);
-            if (absorb >= 2) {
-                nu1[i] = (float)(k == 0.0 ? 0.0 : std::pow(k, y - 2.0));
-                if (absorb == 3) nu2[i] = (float)(k == 0.0 ? 0.0 : std::pow(k, y - 1.0));
-            }
-        });
-        v.radial[RT_KAPPA] = upload(kap);
-        if (need_skappa) v.radial[RT_SKAPPA] = upload(skap);
-        if (v.absorb >= 2) {
-            v.radial[RT_NU1] = upload(nu1);
-            if (v.absorb == 3) v.radial[RT_NU2] = upload(nu2);
-        }
+        // computed on the device in FP64 from the wavenumber vectors (kw_setup.cu); the padding
+        // bins keep dalloc's zeros
+        const size_t tb = (size_t)h.Ns * sizeof(float);
+        float* kap = (float*)dalloc(tb);
+        float* skap = need_skappa ? (float*)dalloc(tb) : nullptr;
+        float* nu1 = v.absorb >= 2 ? (float*)dalloc(tb) : nullptr;
+        float* nu2 = v.absorb == 3 ? (float*)dalloc(tb) : nullptr;
+        const double* dkA = upload(kA);
+        const double* dkB = upload(kB);
+        const double* dkC = upload(kC);
+        launch_setup_radial(st(), dkA, dkB, dkC, h.A, h.B, h.Ch, h.Cp, cref * dt / 2.0, y, kap, skap, nu1, nu2);
+        check(cudaGetLastError(), "setup radial tables");
+        v.radial[RT_KAPPA] = kap;
+        v.radial[RT_SKAPPA] = skap;
+        v.radial[RT_NU1] = nu1;
+        v.radial[RT_NU2] = nu2;
     }
 
     // ---- sensor (REC:8-97) ----

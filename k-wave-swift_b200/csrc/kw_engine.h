@@ -108,6 +108,8 @@ private:
         int comp_mask = 7;        // which components take part (per-comp jobs)
         int fanin = 0;            // the operator pass sums the nin inputs into output 0 (register column kernel)
         int tape = 0;             // the epilogue also stores the adjoint tape of the step
+        int fwd_spec = -1;        // >= 0: the C2R also writes the next job's input spectra (row fusion)
+        int r2c_done = 0;         // the previous job's C2R wrote this job's input spectra (register rows)
         const char* name = "job";
     };
     struct ProfRec {
@@ -139,6 +141,12 @@ private:
         check(cudaMemcpyAsync(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, st()), "upload");
         return p;
     }
+    // device copy of n host floats
+    float* upload_floats(const float* src, long long n) {
+        float* p = (float*)dalloc((size_t)n * sizeof(float));
+        check(cudaMemcpyAsync(p, src, (size_t)n * sizeof(float), cudaMemcpyHostToDevice, st()), "upload");
+        return p;
+    }
     void check(cudaError_t e, const char* what);
     cudaStream_t st() const { return st_override_ ? st_override_ : ctx_->stream; }
 
@@ -153,6 +161,7 @@ private:
     const Map& map_elems(int sim_only);
     const Map& map_planes(int ncomp, int sim_only);
     void issue_job(const SpecJob& job, int sim_only);
+    bool fuse_rows() const;   // row fusion of consecutive jobs allowed (not with the plane pass; KW_FUSE_ROWS=0 off)
     void issue_step(bool first);
     int capture_graph();   // returns the variant captured / in use for the current step
     void finalize_outputs();
@@ -191,8 +200,9 @@ private:
     // autotuner of the operator column pass (kw_tune.cpp)
     bool tune_mode_ = false;
     std::string colop_key(int n, int axis, const ColJob& cj, int ntiles) const;
-    ColopVariant colop_choice(int n, const std::string& key) const;
-    void tune_colop(int n, int axis, int ncomp_map, int sim_only, const ColJob& cj, const std::string& key);
+    ColopVariant colop_choice(int n, const std::string& key, bool tma_ok) const;
+    void tune_colop(int n, int axis, int ncomp_map, int sim_only, const ColJob& cj, const std::string& key,
+                    bool tma_ok);
     void autotune();
     cudaStream_t st_override_ = nullptr;   // adjoint: the reverse sweep's own stream while it issues work
     // axisymmetric solver (kw_axisym.cpp): sims_[0] is the [nx][ny] simulation, car_ / d_car_ the

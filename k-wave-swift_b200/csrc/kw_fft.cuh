@@ -5,8 +5,9 @@
 // input r by exp(-+2 pi i r k / (Ns R)) with k = j mod Ns, does a length-R DFT in registers and
 // writes y[(j - k) R + k + r Ns] (the self-sorting Stockham order; no bit reversal). Stages
 // ping-pong between two shared-memory buffers. Twiddles are precomputed in FP64 on the host and
-// rounded to FP32 (kw_plan.cpp). Butterflies of radix 2, 3, 4, 5, 8 and 16 are unrolled in
-// registers; any other prime radix runs through a direct O(R^2) DFT with FP64-derived roots.
+// rounded to FP32 (Engine::build_plan in kw_engine.cpp). Butterflies of radix 2, 3, 4, 5, 8, 12
+// and 16 are unrolled in registers; any other prime radix runs through a direct O(R^2) DFT with
+// FP64-derived roots.
 #pragma once
 
 #include "kw_common.h"

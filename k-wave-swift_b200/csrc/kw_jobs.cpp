@@ -33,6 +33,14 @@ static bool plane_policy() {
     if (const char* e = std::getenv("KW_PLANE")) return e[0] == '1';
     return false;
 }
+// Row fusion: the register C2R of a job also runs the forward R2C of its epilogue's output into
+// the next job's input spectra (velocity -> density, density -> power-law absorption), so the
+// next job skips its R2C and the field is not read back. KW_FUSE_ROWS=0 turns it off.
+bool Engine::fuse_rows() const {
+    if (plane_policy()) return false;
+    const char* e = std::getenv("KW_FUSE_ROWS");
+    return !(e && e[0] == '0');
+}
 static int col_class(const SimHost& h, int axis) {
     const int n = axis == 0 ? h.A : h.B;
     return has_fixed_kernel(n) ? n : 0;
@@ -181,6 +189,7 @@ void Engine::issue_job(const SpecJob& job, int sim_only) {
     // ---- forward row pass (R2C) ----
     for (int sc : classes(row_class)) {
         if (plane) break;
+        if (job.r2c_done && rowr_class(sc) && dim_ >= 2) continue;   // written by the previous job's C2R
         auto in_class = [&](const SimHost& h) { return row_class(h) == sc; };
         long long te = 0;
         for (int s = 0; s < count(); ++s)
@@ -243,13 +252,17 @@ void Engine::issue_job(const SpecJob& job, int sim_only) {
             else if (sc && op && has_colop(sc)) {
                 // the variant the autotuner chose for this pass (kw_tune.cpp), on its own tile map
                 const std::string key = colop_key(sc, axis, cj, m.n);
+                // the TMA-fed kernel needs every simulation of the launch to have the A-axis maps
+                bool tma_ok = dim_ == 3 && axis == 0 && !job.fanin && colop_tma_length(sc);
+                for (int s = 0; tma_ok && s < count(); ++s)
+                    if (in_launch(s) && in_class(sims_[s])) tma_ok = colp_enabled(sims_[s], 0) && sims_[s].dev.tmaps;
                 if (tune_mode_) {
-                    tune_colop(sc, axis, ncomp_map, sim_only, cj, key);
+                    tune_colop(sc, axis, ncomp_map, sim_only, cj, key, tma_ok);
                 } else {
-                    const ColopVariant v = colop_choice(sc, key);
+                    const ColopVariant v = colop_choice(sc, key, tma_ok);
                     const Map& mv = map_cols(axis, ncomp_map, sim_only, op, sc, colop_tile(sc, v.r1));
                     timed(std::string(label) + job.name, bytes,
-                          [&] { launch_colop(st(), d_sims_, d_t_, mv.d, mv.n, cj, sc, v); });
+                          [&] { launch_colop(st(), d_sims_, d_t_, mv.d, mv.n, cj, sc, v, d_flag_ + 1); });
                 }
             }
             else if (sc && !op && has_colp(sc) && !(cola & 2))
@@ -306,12 +319,19 @@ void Engine::issue_job(const SpecJob& job, int sim_only) {
         cj.tape = job.tape;
         cj.tile_elems = te;
         const bool reg = rowr_class(sc);
+        cj.fwd = job.fwd_spec >= 0 && reg && dim_ >= 2;
+        cj.fwd_spec = job.fwd_spec;
         const Map& m = map_rows(reg ? -2 : ncta, job.coupled ? 1 : job.nout, sim_only, sc);
         const double bytes = sum_sims(in_class, [&](const SimHost& h) {
             int no = job.coupled ? (open_comps(h, 1) ? job.nout : 0) : open_comps(h, job.nout);
             if (job.epi == EPI_EOS_ABS && no) no = h.dev.absorb == 3 ? 2 : 1;
             if (no == 0) return 0.0;
-            return no * spec_bytes(h) + (double)h.N * epi_bytes(h, job.epi, job.coupled ? 1 : no);
+            double b = no * spec_bytes(h) + (double)h.N * epi_bytes(h, job.epi, job.coupled ? 1 : no);
+            if (cj.fwd) {   // the fused R2C's spectra; the density epilogue then keeps rho0 div u on chip
+                if (job.epi == EPI_VEL) b += no * spec_bytes(h);
+                else if (h.dev.absorb >= 2) b += (h.dev.absorb == 3 ? 2 : 1) * spec_bytes(h) - (double)h.N * 4;
+            }
+            return b;
         });
         const size_t smem = (size_t)(has_fixed_kernel(sc) ? 2 : 3) * te * sizeof(float2) + (size_t)aux_floats * sizeof(float);
         if (reg)

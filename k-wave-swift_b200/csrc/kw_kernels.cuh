@@ -51,6 +51,8 @@ struct RowC2RJob {
     int generic;           // some simulation needs the runtime-plan (ping-pong) path
     long long tile_elems;
     int tape;              // the density / source / absorption epilogues also fill the adjoint tape
+    int fwd;               // register row kernels: also run the forward R2C of the epilogue's output
+    int fwd_spec;          // ... into spec[fwd_spec + o] (velocity: o = component; density: 0 = rho0 div u, 1 = rho_sum)
 };
 
 // Host entry points (kw_passes.cu, kw_small.cu). The pass launchers take the tile map and its
@@ -76,10 +78,15 @@ struct ColopVariant {
     int minb;
 };
 __host__ __device__ constexpr int colop_tile(int n, int r1) { return reg_lines(n, r1); }
+// minb of the TMA-fed, warp-specialised variant (kw_pass_colop.cu): 3D operator passes along A of
+// the lengths colop_tma_length(n) whose simulations have the A-axis tensor maps (r1 = 16)
+constexpr int kColopTma = -1;
+constexpr int kColopPf = -2;   // persistent, next tile prefetched into registers
+bool colop_tma_length(int n);
 int colop_variants(int n, ColopVariant* out, int max);
 void init_colop_attributes(int optin);
 void launch_colop(cudaStream_t st, const SimDev* d_sims, const int* d_t, const BlockWork* map, int nmap,
-                  const ColJob& job, int n, ColopVariant v);
+                  const ColJob& job, int n, ColopVariant v, int* err = nullptr);
 // axisymmetric solver (kw_axisym.cu): radial mirror of an [nx][ny] field into the [nx][4 ny]
 // expansion (WSWA: p, ux; HAHS: uy; HSHA: uy / r with over_r), the trimmed updates, sources
 enum AsMirror { AS_WSWA = 0, AS_HAHS, AS_HSHA };
@@ -129,6 +136,14 @@ void launch_sample(cudaStream_t st, const SimDev* d_sims, const int* d_t, int ns
 void launch_tick(cudaStream_t st, int* d_t);
 void launch_scatter(cudaStream_t st, float* dst, const int* idx, const float* val, int n);
 void launch_check_finite(cudaStream_t st, const SimDev* d_sims, const int* d_t, const BlockWork* map, int nblocks);
+
+// once-per-simulation setup on the device in FP64 (kw_setup.cu)
+void launch_setup_c2(cudaStream_t st, const float* c0, float* c2, long long n);
+void launch_setup_dtor(cudaStream_t st, const float* rho0, float* out, long long n, long long stride, int len, double dt);
+void launch_setup_absorb(cudaStream_t st, const float* c0_map, double c0_s, const float* alpha_map, double alpha_s,
+                         double np1, double y, int stokes, double tn, float* tau, float* eta, long long n);
+void launch_setup_radial(cudaStream_t st, const double* kA, const double* kB, const double* kC, int A, int B, int Ch,
+                         int Cp, double half, double y, float* kap, float* skap, float* nu1, float* nu2);
 
 // setup helpers on one field (single simulation)
 void launch_absmax(cudaStream_t st, const float* x, long long n, unsigned int* d_out_bits);

@@ -10,6 +10,7 @@
 // its own slots) so that only one line's worth of registers is live. Many small CTAs per SM keep
 // enough loads in flight. The fan-in variant sums H_c X_c over several inputs into one output
 // with one inverse.
+#include "kw_async.cuh"
 #include "kw_fft_reg.cuh"
 #include "kw_pass_common.cuh"
 
@@ -30,53 +31,24 @@ namespace kw {
     X(96, 12, 3) X(96, 12, 2) X(96, 12, 4) X(192, 12, 3) X(192, 12, 2) X(192, 12, 4)                    \
     X(384, 12, 0) X(384, 12, 2) X(384, 12, 3) X(768, 12, 0) X(768, 12, 2) X(768, 12, 3)
 
-template <int N, int R1V, int MINB>
-__global__ void __launch_bounds__(256, MINB) k_colop(const SimDev* __restrict__ sims, const int* __restrict__ d_t,
-                                               const BlockWork* __restrict__ map, int nmap, ColJob job) {
-    using P = RegPlan<N, R1V>;
-    using Lay = ColLayout<P, N>;
-    constexpr int R1 = P::R1, T = P::T, TW = P::LINES;
-    __shared__ float2 sh[Lay::SLOTS];
-    extern __shared__ __align__(16) float2 parked[];   // [R1][256] when the job has several outputs
-    if (blockIdx.x >= nmap) return;
-    const BlockWork bw = map[blockIdx.x];
-    const SimDev& S = sims[bw.sim];
-    if (!gate_open(S, job.gate, bw.comp, *d_t)) return;
-
-    // the pass's lines are the columns of one plane (the layout axis before it has length 1)
-    const bool axisA = job.layout_axis == 0;
-    const int inner = axisA ? S.B * S.Cp : S.Cp;
-    const int l = threadIdx.x % TW;
-    const int t = threadIdx.x / TW;
-    const int c = bw.tile * TW + l;
-    const bool col_ok = c < inner;
-    const long long base = col_ok ? c : 0;
+// The operator work of one tile after its spectrum is in registers (v[m] = X(row t + T m) of line
+// l, not yet transformed): forward transform, x radial table (this thread's slots `tsl`, filled by
+// cp.async) x 1/N, inverse transform(s), outputs stored. `sh` is the exchange buffer of the
+// transforms, `parked` this thread's slots for the product when the job has several outputs.
+template <int N, class P, class Lay, class Sync>
+__device__ __forceinline__ void colop_body(const SimDev& S, const ColJob& job, int comp, float2 (&v)[P::R1], float2* sh,
+                                           float2* parked, const float* tsl, int t, int l, int c, bool col_ok,
+                                           long long base, int inner, bool axisA, int rad) {
+    constexpr int R1 = P::R1, T = P::T;
     const float2* __restrict__ twn = axisA ? S.plan_a.twn : S.plan_b.twn;
-    const int comp_in = job.fanout ? 0 : bw.comp;
-    const float2* in = S.spec[job.spec_in + comp_in] + base;
-    // the radial table of this thread's bins is copied into its own shared-memory slots while the
-    // spectrum loads and the forward transform run (behind the parked product, if any)
-    const int rad = (comp_in == 0 ? job.op[0] : (comp_in == 1 ? job.op[1] : job.op[2])).radial;
-    float* tsl = reinterpret_cast<float*>(parked + (job.fanout && job.nout > 1 ? R1 * 256 : 0)) + threadIdx.x;
-    if (rad != RT_NONE && col_ok) {
-        const float* tab = S.radial[rad] + base;
-#pragma unroll
-        for (int r = 0; r < R1; ++r) cp_async4(tsl + r * 256, tab + (long long)(t + T * r) * inner);
-    }
-    cp_commit();
-
-    float2 v[R1];
-#pragma unroll
-    for (int r = 0; r < R1; ++r) v[r] = col_ok ? in[(long long)(t + T * r) * inner] : make_float2(0.f, 0.f);
-
-    FftReg<N, P, false, Lay>::run(v, sh, t, l, twn);          // v[m] = X(row t + T m)
+    FftReg<N, P, false, Lay, Sync>::run(v, sh, t, l, twn);          // v[m] = X(row t + T m)
     int kb = 0, kc = c;
     if (axisA) { kb = c / S.Cp; kc = c - kb * S.Cp; }
     const bool bin_ok = col_ok && kc < S.Ch;
     const int pass_ref_axis = (axisA ? 0 : 1) - (3 - S.dim);
     const int nouts = job.fanout ? job.nout : 1;
     auto op_of = [&](int oc) { return oc == 0 ? job.op[0] : (oc == 1 ? job.op[1] : job.op[2]); };
-    auto out_comp = [&](int oo) { return job.fanout ? oo : bw.comp; };
+    auto out_comp = [&](int oo) { return job.fanout ? oo : comp; };
     auto factor_vec = [&](const OpSpec& op) -> const float2* {
         if (op.axis_op == AO_NONE) return nullptr;
         const AxisDev& ax = S.ax[op.axis];
@@ -99,12 +71,13 @@ __global__ void __launch_bounds__(256, MINB) k_colop(const SimDev* __restrict__ 
     bool shared = false;
     for (int oo = 0; oo < nouts; ++oo) shared |= !along(op_of(out_comp(oo)));
     const bool park = nouts > 1;
+    const int me = threadIdx.x;   // consumer thread index (the 256 threads of the tile)
     if (park) {
 #pragma unroll
-        for (int m = 0; m < R1; ++m) parked[m * 256 + threadIdx.x] = v[m];
+        for (int m = 0; m < R1; ++m) parked[m * 256 + me] = v[m];
     }
     if (shared) {
-        FftReg<N, P, true, Lay>::run(v, sh, t, l, twn);
+        FftReg<N, P, true, Lay, Sync>::run(v, sh, t, l, twn);
         for (int oo = 0; oo < nouts; ++oo) {
             const int oc = out_comp(oo);
             const OpSpec op = op_of(oc);
@@ -126,11 +99,11 @@ __global__ void __launch_bounds__(256, MINB) k_colop(const SimDev* __restrict__ 
         const float2* fv = factor_vec(op);
         if (park) {
 #pragma unroll
-            for (int m = 0; m < R1; ++m) v[m] = parked[m * 256 + threadIdx.x];
+            for (int m = 0; m < R1; ++m) v[m] = parked[m * 256 + me];
         }
 #pragma unroll
         for (int m = 0; m < R1; ++m) v[m] = cmul(v[m], __ldg(fv + t + T * m));
-        FftReg<N, P, true, Lay>::run(v, sh, t, l, twn);
+        FftReg<N, P, true, Lay, Sync>::run(v, sh, t, l, twn);
         float2* out = S.spec[job.spec_out + oc] + base;
         if (bin_ok) {
 #pragma unroll
@@ -139,6 +112,212 @@ __global__ void __launch_bounds__(256, MINB) k_colop(const SimDev* __restrict__ 
     }
 }
 
+// the radial table of this thread's bins into its own shared-memory slots (cp.async), overlapping
+// the forward transform
+template <int R1, int T>
+__device__ __forceinline__ void colop_table(const SimDev& S, int rad, bool col_ok, long long base, int inner, int t,
+                                            float* tsl) {
+    if (rad != RT_NONE && col_ok) {
+        const float* tab = S.radial[rad] + base;
+#pragma unroll
+        for (int r = 0; r < R1; ++r) cp_async4(tsl + r * 256, tab + (long long)(t + T * r) * inner);
+    }
+    cp_commit();
+}
+
+template <int N, int R1V, int MINB>
+__global__ void __launch_bounds__(256, MINB) k_colop(const SimDev* __restrict__ sims, const int* __restrict__ d_t,
+                                               const BlockWork* __restrict__ map, int nmap, ColJob job) {
+    using P = RegPlan<N, R1V>;
+    using Lay = ColLayout<P, N>;
+    constexpr int R1 = P::R1, T = P::T, TW = P::LINES;
+    __shared__ float2 sh[Lay::SLOTS];
+    extern __shared__ __align__(16) float2 parked[];   // [R1][256] when the job has several outputs
+    if (blockIdx.x >= nmap) return;
+    const BlockWork bw = map[blockIdx.x];
+    const SimDev& S = sims[bw.sim];
+    if (!gate_open(S, job.gate, bw.comp, *d_t)) return;
+
+    // the pass's lines are the columns of one plane (the layout axis before it has length 1)
+    const bool axisA = job.layout_axis == 0;
+    const int inner = axisA ? S.B * S.Cp : S.Cp;
+    const int l = threadIdx.x % TW;
+    const int t = threadIdx.x / TW;
+    const int c = bw.tile * TW + l;
+    const bool col_ok = c < inner;
+    const long long base = col_ok ? c : 0;
+    const int comp_in = job.fanout ? 0 : bw.comp;
+    const float2* in = S.spec[job.spec_in + comp_in] + base;
+    const int rad = (comp_in == 0 ? job.op[0] : (comp_in == 1 ? job.op[1] : job.op[2])).radial;
+    float* tsl = reinterpret_cast<float*>(parked + (job.fanout && job.nout > 1 ? R1 * 256 : 0)) + threadIdx.x;
+    colop_table<R1, T>(S, rad, col_ok, base, inner, t, tsl);
+    float2 v[R1];
+#pragma unroll
+    for (int r = 0; r < R1; ++r) v[r] = col_ok ? in[(long long)(t + T * r) * inner] : make_float2(0.f, 0.f);
+    colop_body<N, P, Lay, BlockSync>(S, job, bw.comp, v, sh, parked, tsl, t, l, c, col_ok, base, inner, axisA, rad);
+}
+
+// Persistent variant with the next tile's spectrum loaded into registers while this tile is
+// transformed: each CTA walks the tile map with stride gridDim.x; the loads of tile i + 1 are issued
+// before the transforms of tile i and are waited on only when tile i + 1 starts, so every SM keeps
+// loads in flight through the compute phase (two CTAs per SM: the prefetch takes R1 more float2
+// registers a thread).
+template <int N, int R1V>
+__global__ void __launch_bounds__(256, 2) k_colop_pf(const SimDev* __restrict__ sims, const int* __restrict__ d_t,
+                                                     const BlockWork* __restrict__ map, int nmap, ColJob job) {
+    using P = RegPlan<N, R1V>;
+    using Lay = ColLayout<P, N>;
+    constexpr int R1 = P::R1, T = P::T, TW = P::LINES;
+    __shared__ float2 sh[Lay::SLOTS];
+    extern __shared__ __align__(16) float2 parked[];   // [R1][256] when the job has several outputs
+    const int tstep = *d_t;
+    const bool axisA = job.layout_axis == 0;
+    const int l = threadIdx.x % TW;
+    const int t = threadIdx.x / TW;
+    float* tsl = reinterpret_cast<float*>(parked + (job.fanout && job.nout > 1 ? R1 * 256 : 0)) + threadIdx.x;
+    // the next tile of this CTA whose gate is open (nmap when none is left)
+    auto next_open = [&](int idx) {
+        for (; idx < nmap; idx += gridDim.x) {
+            const BlockWork bw = map[idx];
+            if (gate_open(sims[bw.sim], job.gate, bw.comp, tstep)) break;
+        }
+        return idx;
+    };
+    auto load = [&](int idx, float2 (&dst)[R1]) {
+        const BlockWork bw = map[idx];
+        const SimDev& S = sims[bw.sim];
+        const int inner = axisA ? S.B * S.Cp : S.Cp;
+        const int c = bw.tile * TW + l;
+        const bool col_ok = c < inner;
+        const float2* in = S.spec[job.spec_in + (job.fanout ? 0 : bw.comp)] + (col_ok ? c : 0);
+#pragma unroll
+        for (int r = 0; r < R1; ++r) dst[r] = col_ok ? in[(long long)(t + T * r) * inner] : make_float2(0.f, 0.f);
+    };
+    int idx = next_open(blockIdx.x);
+    float2 nx[R1];
+    if (idx < nmap) load(idx, nx);
+    while (idx < nmap) {
+        float2 v[R1];
+#pragma unroll
+        for (int r = 0; r < R1; ++r) v[r] = nx[r];
+        const int cur = idx;
+        idx = next_open(idx + gridDim.x);
+        if (idx < nmap) load(idx, nx);   // in flight during the transforms below
+        const BlockWork bw = map[cur];
+        const SimDev& S = sims[bw.sim];
+        const int inner = axisA ? S.B * S.Cp : S.Cp;
+        const int c = bw.tile * TW + l;
+        const bool col_ok = c < inner;
+        const long long base = col_ok ? c : 0;
+        const int comp_in = job.fanout ? 0 : bw.comp;
+        const int rad = (comp_in == 0 ? job.op[0] : (comp_in == 1 ? job.op[1] : job.op[2])).radial;
+        colop_table<R1, T>(S, rad, col_ok, base, inner, t, tsl);
+        colop_body<N, P, Lay, BlockSync>(S, job, bw.comp, v, sh, parked, tsl, t, l, c, col_ok, base, inner, axisA, rad);
+    }
+}
+
+// Dense column layout (no padding) for LINES >= 16: a half warp (16 lanes) touches one row of
+// 16 consecutive values in every access of the transform, so rows need no padding to avoid bank
+// conflicts; the TMA tile itself ([row][LINES] float2) is in this layout.
+template <class P, int N>
+struct ColLayoutDense {
+    static constexpr int SLOTS = N * P::LINES;
+    __device__ __forceinline__ static int at(int j, int l) { return j * P::LINES + l; }
+};
+
+// TMA-fed, warp-specialised operator pass along layout axis A (3D; the column lengths of the
+// in-place TMA pass, R1 = 16): a persistent CTA of 8 consumer warps and one producer warp. The
+// producer loads each tile (colr_lines(N) columns by the N rows) with one tensor copy into a ring
+// of `ns` stages; the consumers take their values, run the forward transform, operator and
+// inverse(s) with the stage itself as the exchange buffer, store the outputs and only then release
+// the stage, so up to ns - 1 further tiles are in flight meanwhile. Bounded waits as in kw_pass_colp.cu.
+template <int N>
+__global__ void __launch_bounds__(288, 2) k_colop_tma(const SimDev* __restrict__ sims, const int* __restrict__ d_t,
+                                                      const BlockWork* __restrict__ map, int nmap, ColJob job, int ns,
+                                                      int* __restrict__ err) {
+    using P = RegPlan<N, 16>;
+    using Lay = ColLayoutDense<P, N>;
+    constexpr int R1 = P::R1, T = P::T, TW = P::LINES;
+    constexpr int STAGE = N * TW * 8;
+    static_assert(TW >= 16, "dense layout needs 16 lines");
+    extern __shared__ __align__(128) unsigned char smem[];
+    const bool park_on = job.fanout && job.nout > 1;
+    float2* parked = reinterpret_cast<float2*>(smem + ns * STAGE);
+    float* tslots = reinterpret_cast<float*>(smem + ns * STAGE + (park_on ? R1 * 256 * 8 : 0));
+    uint64_t* full = reinterpret_cast<uint64_t*>(reinterpret_cast<unsigned char*>(tslots) + R1 * 256 * 4);
+    uint64_t* empty = full + ns;
+    __shared__ volatile int abort;   // set by the consumers when one of their waits ran out
+    if (threadIdx.x == 0) {
+        abort = 0;
+        for (int s2 = 0; s2 < ns; ++s2) {
+            mbar_init(full + s2, 1);
+            mbar_init(empty + s2, 8);
+        }
+        fence_barrier_init();
+    }
+    __syncthreads();
+    const int tstep = *d_t;
+
+    if (threadIdx.x >= 256) {
+        // ---------------- producer ----------------
+        if (threadIdx.x != 256) return;
+        int k = 0;
+        for (int idx = blockIdx.x; idx < nmap; idx += gridDim.x) {
+            const BlockWork bw = map[idx];
+            const SimDev& S = sims[bw.sim];
+            if (!gate_open(S, job.gate, bw.comp, tstep)) continue;
+            const int s = k % ns;
+            if (k >= ns && !mbar_wait_or_abort(empty + s, ((k / ns) & 1) ^ 1, err, KE_TIMEOUT_EMPTY, &abort)) break;
+            const int comp_in = job.fanout ? 0 : bw.comp;
+            mbar_arrive_expect_tx(full + s, STAGE);
+            tma_load_2d(smem + s * STAGE, S.tmaps + tmap_spec(job.spec_in + comp_in, 0), bw.tile * TW, 0, full + s);
+            ++k;
+        }
+        // every issued copy must have landed before this CTA's shared memory is released
+        for (int j = k > ns ? k - ns : 0; j < k; ++j) mbar_wait(full + j % ns, (j / ns) & 1, err, KE_TIMEOUT_DRAIN);
+        return;
+    }
+
+    // ---------------- consumers ----------------
+    const int l = threadIdx.x % TW;
+    const int t = threadIdx.x / TW;
+    const int lane = threadIdx.x & 31;
+    float* tsl = tslots + threadIdx.x;
+    int k = 0;
+    for (int idx = blockIdx.x; idx < nmap; idx += gridDim.x) {
+        const BlockWork bw = map[idx];
+        const SimDev& S = sims[bw.sim];
+        if (!gate_open(S, job.gate, bw.comp, tstep)) continue;
+        const int s = k % ns;
+        const int inner = S.B * S.Cp;
+        const int c = bw.tile * TW + l;
+        const bool col_ok = c < inner;
+        const long long base = col_ok ? c : 0;
+        const int comp_in = job.fanout ? 0 : bw.comp;
+        const int rad = (comp_in == 0 ? job.op[0] : (comp_in == 1 ? job.op[1] : job.op[2])).radial;
+        colop_table<R1, T>(S, rad, col_ok, base, inner, t, tsl);   // overlaps the wait and the transform
+        const bool ok = mbar_wait(full + s, (k / ns) & 1, err, KE_TIMEOUT_FULL, S.wait_cycles);
+        int all_ok;
+        asm volatile("{\n\t.reg .pred p, q;\n\tsetp.ne.u32 p, %1, 0;\n\tbar.red.and.pred q, 1, 256, p;\n\tselp.u32 %0, 1, 0, q;\n\t}"
+                     : "=r"(all_ok) : "r"((unsigned)ok) : "memory");
+        if (!all_ok) {
+            cp_wait<0>();
+            if (threadIdx.x == 0) abort = 1;
+            return;
+        }
+        float2* stage = reinterpret_cast<float2*>(smem + s * STAGE);
+        float2 v[R1];
+#pragma unroll
+        for (int r = 0; r < R1; ++r) v[r] = stage[(t + T * r) * TW + l];
+        ConsumerSync::sync();   // every value is read before the transform reuses the stage
+        colop_body<N, P, Lay, ConsumerSync>(S, job, bw.comp, v, stage, parked, tsl, t, l, c, col_ok, base, inner, true,
+                                            rad);
+        ConsumerSync::sync();   // the last exchange through the stage is done
+        __syncwarp();
+        if (lane == 0) mbar_arrive(empty + s);
+        ++k;
+    }
+}
 
 // fan-in operator pass: sum_c H_c X_c over job.fanin inputs with one inverse transform (the
 // adjoint's lambda_p = sum_a D-_a w_a); the running sum is kept in this thread's shared-memory slots
@@ -214,9 +393,15 @@ static size_t colop_park_bytes(const ColJob& job, int r1) {
     return (size_t)r1 * 256 * ((park ? sizeof(float2) : 0) + (table ? sizeof(float) : 0));
 }
 
+// (N, R1) of the persistent prefetching variant (minb = kColopPf)
+#define KW_COLOP_PF(X) X(128, 16) X(256, 16) X(256, 8) X(512, 16) X(512, 8) X(192, 12) X(384, 12)
+
 void init_colop_attributes(int optin) {
 #define KW_SET(NN, RR, MB) set_max_smem((const void*)k_colop<NN, RR, MB>, optin);
     KW_COLOP_VARIANTS(KW_SET)
+#undef KW_SET
+#define KW_SET(NN, RR) set_max_smem((const void*)k_colop_pf<NN, RR>, optin);
+    KW_COLOP_PF(KW_SET)
 #undef KW_SET
 #define KW_SET(n) set_max_smem((const void*)k_colop_fanin<n>, optin);
     KW_COLOP_SIZES(KW_SET)
@@ -229,12 +414,89 @@ int colop_variants(int n, ColopVariant* out, int max) {
     if (n == NN && k < max) out[k++] = ColopVariant{RR, MB};
     KW_COLOP_VARIANTS(KW_ADD)
 #undef KW_ADD
+#define KW_ADD(NN, RR) \
+    if (n == NN && k < max) out[k++] = ColopVariant{RR, kColopPf};
+    KW_COLOP_PF(KW_ADD)
+#undef KW_ADD
     return k;
 }
 
+template <int N, int R1>
+static void launch_colop_pf(cudaStream_t st, const SimDev* d_sims, const int* d_t, const BlockWork* map, int nmap,
+                            const ColJob& job) {
+    static int sms = 0;
+    if (!sms) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    }
+    const size_t smem = colop_park_bytes(job, R1);
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void*)k_colop_pf<N, R1>, 256, smem) != cudaSuccess ||
+        per_sm < 1) {
+        cudaGetLastError();
+        per_sm = 1;
+    }
+    const int grid = nmap < per_sm * sms ? nmap : per_sm * sms;
+    k_colop_pf<N, R1><<<grid, 256, smem, st>>>(d_sims, d_t, map, nmap, job);
+}
+
+// shared memory of the TMA-fed operator pass: `ns` stages, the parked product (several outputs),
+// the radial table slots, the mbarriers; ns as large as two CTAs per SM allow (at most 4)
+template <int N>
+static void colop_tma_layout(const ColJob& job, int* ns, size_t* bytes) {
+    constexpr size_t STAGE = (size_t)N * reg_lines(N, 16) * 8;
+    const size_t fixed = (job.fanout && job.nout > 1 ? 16 * 256 * 8 : 0) + 16 * 256 * 4;
+    const size_t budget = 113 * 1024 - 128;
+    int k = (int)((budget - fixed) / (STAGE + 16));
+    k = k < 2 ? 2 : (k > 4 ? 4 : k);
+    *ns = k;
+    *bytes = (size_t)k * STAGE + fixed + 16 * (size_t)k;
+}
+
+template <int N>
+static void launch_colop_tma(cudaStream_t st, const SimDev* d_sims, const int* d_t, const BlockWork* map, int nmap,
+                             const ColJob& job, int* err) {
+    int ns;
+    size_t smem;
+    colop_tma_layout<N>(job, &ns, &smem);
+    static int sms = 0;
+    if (!sms) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    }
+    cudaFuncSetAttribute((const void*)k_colop_tma<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void*)k_colop_tma<N>, 288, smem) != cudaSuccess ||
+        per_sm < 1) {
+        cudaGetLastError();
+        per_sm = 1;
+    }
+    const int grid = nmap < per_sm * sms ? nmap : per_sm * sms;
+    k_colop_tma<N><<<grid, 288, smem, st>>>(d_sims, d_t, map, nmap, job, ns, err);
+}
+
+bool colop_tma_length(int n) { return n == 128 || n == 256; }
+
 void launch_colop(cudaStream_t st, const SimDev* d_sims, const int* d_t, const BlockWork* map, int nmap,
-                  const ColJob& job, int n, ColopVariant v) {
+                  const ColJob& job, int n, ColopVariant v, int* err) {
     if (nmap <= 0) return;
+    if (v.minb == kColopTma && !job.fanin) {
+        if (n == 256) launch_colop_tma<256>(st, d_sims, d_t, map, nmap, job, err);
+        else if (n == 128) launch_colop_tma<128>(st, d_sims, d_t, map, nmap, job, err);
+        return;
+    }
+    if (v.minb == kColopPf && !job.fanin) {
+#define KW_CASE(NN, RR)                                                      \
+    if (n == NN && v.r1 == RR) {                                             \
+        launch_colop_pf<NN, RR>(st, d_sims, d_t, map, nmap, job);            \
+        return;                                                              \
+    }
+        KW_COLOP_PF(KW_CASE)
+#undef KW_CASE
+        return;
+    }
     if (job.fanin) {   // one variant (the adjoint's fan-in sum)
         switch (n) {
 #define KW_CASE(n) \

@@ -9,7 +9,9 @@
 // tile map, and the fastest is kept for that key. The spectra the passes overwrite are scratch
 // between jobs, so timing them before the first step changes no result.
 //
-// Keys: "colop/<length>/<layout axis>/<outputs>/<fan-out>/<log2 tiles>". Choices are cached in
+// Keys: "colop/<length>/<layout axis>/<outputs>/<fan-out>/<log2 tiles>". Where the launch allows
+// it (3D, along A, lengths 128 and 256, tensor maps present) the TMA-fed warp-specialised kernel is
+// a further candidate (minb = kColopTma). Choices are cached in
 // memory for the process and in a JSON file per GPU model: $KW_TUNE_CACHE if set, else
 // $HOME/.cache/kwave_b200/tune_<gpu>.json. KW_AUTOTUNE=0 turns tuning off (every pass takes its
 // default variant); KW_COLOP_VARIANT=r1,minb forces that variant wherever the length has it.
@@ -135,13 +137,22 @@ bool autotune_enabled() {
     return !(e && e[0] == '0');
 }
 
-bool forced_variant(int n, ColopVariant* v) {
+// the variants of length n for this launch: the register ones, and the TMA-fed one where the
+// launch can take it (KW_COLOP_TMA=0 leaves it out)
+int candidates(int n, bool tma_ok, ColopVariant* out) {
+    int nc = colop_variants(n, out, 15);
+    const char* e = std::getenv("KW_COLOP_TMA");
+    if (tma_ok && colop_tma_length(n) && !(e && e[0] == '0')) out[nc++] = ColopVariant{16, kColopTma};
+    return nc;
+}
+
+bool forced_variant(int n, bool tma_ok, ColopVariant* v) {
     const char* e = std::getenv("KW_COLOP_VARIANT");
     if (!e) return false;
     ColopVariant f{};
     if (std::sscanf(e, "%d,%d", &f.r1, &f.minb) != 2) return false;
     ColopVariant cands[16];
-    const int nc = colop_variants(n, cands, 16);
+    const int nc = candidates(n, tma_ok, cands);
     for (int k = 0; k < nc; ++k)
         if (cands[k].r1 == f.r1 && cands[k].minb == f.minb) {
             *v = f;
@@ -160,21 +171,25 @@ std::string Engine::colop_key(int n, int axis, const ColJob& cj, int ntiles) con
            std::to_string(cj.fanout) + "/" + std::to_string(lg);
 }
 
-ColopVariant Engine::colop_choice(int n, const std::string& key) const {
+ColopVariant Engine::colop_choice(int n, const std::string& key, bool tma_ok) const {
     ColopVariant cands[16];
-    colop_variants(n, cands, 16);
+    const int nc = candidates(n, tma_ok, cands);
     ColopVariant v = cands[0];
-    if (forced_variant(n, &v)) return v;
-    if (autotune_enabled()) TuneCache::get().find(key, &v);
+    if (forced_variant(n, tma_ok, &v)) return v;
+    ColopVariant c;
+    if (autotune_enabled() && TuneCache::get().find(key, &c))
+        for (int k = 0; k < nc; ++k)
+            if (cands[k].r1 == c.r1 && cands[k].minb == c.minb) v = c;   // only a choice valid here
     return v;
 }
 
 // Time every variant of the operator pass on its own tile map and keep the fastest (tune mode).
-void Engine::tune_colop(int n, int axis, int ncomp_map, int sim_only, const ColJob& cj, const std::string& key) {
+void Engine::tune_colop(int n, int axis, int ncomp_map, int sim_only, const ColJob& cj, const std::string& key,
+                        bool tma_ok) {
     ColopVariant cur;
     if (!autotune_enabled() || TuneCache::get().find(key, &cur)) return;
     ColopVariant cands[16];
-    const int nc = colop_variants(n, cands, 16);
+    const int nc = candidates(n, tma_ok, cands);
     if (nc <= 1) {
         TuneCache::get().put(key, cands[0], 0.0);
         return;
@@ -186,9 +201,9 @@ void Engine::tune_colop(int n, int axis, int ncomp_map, int sim_only, const ColJ
     double best_us = 1e300;
     for (int k = 0; k < nc; ++k) {
         const Map& m = map_cols(axis, ncomp_map, sim_only, true, n, colop_tile(n, cands[k].r1));
-        launch_colop(st(), d_sims_, d_t_, m.d, m.n, cj, n, cands[k]);   // warm-up
+        launch_colop(st(), d_sims_, d_t_, m.d, m.n, cj, n, cands[k], d_flag_ + 1);   // warm-up
         check(cudaEventRecord(a, st()), "event");
-        for (int r = 0; r < 3; ++r) launch_colop(st(), d_sims_, d_t_, m.d, m.n, cj, n, cands[k]);
+        for (int r = 0; r < 3; ++r) launch_colop(st(), d_sims_, d_t_, m.d, m.n, cj, n, cands[k], d_flag_ + 1);
         check(cudaEventRecord(b, st()), "event");
         check(cudaEventSynchronize(b), "tune sync");
         check(cudaGetLastError(), "tune launch");

@@ -21,8 +21,11 @@ pytestmark = pytest.mark.gpu
 
 # (shape, operator-axis length): 3D passes run along A, 2D along B
 SHAPES = [((256, 24, 32), 256), ((128, 24, 32), 128), ((192, 16, 24), 192), ((512, 64), 512)]
-VARIANTS = {16: [], 256: [(16, 3), (16, 2), (8, 3), (8, 4)], 128: [(16, 3), (16, 2), (8, 3), (8, 4)],
-            192: [(12, 3), (12, 2), (12, 4)], 512: [(16, 0), (16, 2), (8, 2), (8, 3), (8, 4)]}
+# (r1, minb); minb -1 is the TMA-fed warp-specialised kernel (3D passes along A of 128 and 256),
+# minb -2 the persistent kernel that prefetches the next tile into registers
+VARIANTS = {16: [], 256: [(16, 3), (16, 2), (8, 3), (8, 4), (16, -2), (8, -2), (16, -1)],
+            128: [(16, 3), (16, 2), (8, 3), (8, 4), (16, -2), (16, -1)],
+            192: [(12, 3), (12, 2), (12, 4), (12, -2)], 512: [(16, 0), (16, 2), (8, 2), (8, 3), (8, 4), (16, -2), (8, -2)]}
 
 
 def _run(b):
