@@ -26,6 +26,9 @@ simulation). The metric is grid-point-steps per second over the whole job.
 With --gpus N > 1 every rank runs an independent replica (no collective on the data path):
 "scaling": "weak", value = all ranks' grid-point-steps / max-over-ranks time. Without torchrun's
 environment, --gpus N > 1 relaunches this script under torch.distributed.run with N local ranks.
+--profile-step runs one step of the workload after W warm-up steps with every kernel launched on
+          its own inside the NVTX range "step" and prints its per-launch profile (the command the
+          ncu summaries under profiles/ are taken with).
 """
 from __future__ import annotations
 
@@ -445,6 +448,25 @@ def run_adjoint(args) -> None:
     rep.close()
 
 
+def run_profile_step(args) -> None:
+    """One time step of the workload after W warm-up steps, every kernel launched on its own inside
+    the NVTX range "step" (for ncu --nvtx --nvtx-include "step/"); prints the per-launch CUDA-event
+    profile as one JSON line. Not a bench line: nothing here is timed as a metric."""
+    import torch
+    rep, ctx, stream, gpu_id = _gpu_setup()
+    b = workload(args.workload)
+    sim = ctx.create_sim(b)
+    sim.step(max(args.warmup, 1))
+    torch.cuda.synchronize()
+    torch.cuda.nvtx.range_push("step")
+    prof = sim.profile_step(1)
+    torch.cuda.synchronize()
+    torch.cuda.nvtx.range_pop()
+    sim.close()
+    print(json.dumps({"workload": args.workload, "after_steps": max(args.warmup, 1),
+                      "launches": [[k["name"], round(k["ms"], 4), k["bytes"]] for k in prof]}))
+
+
 def run_ours(args) -> None:
     import torch
     rep, ctx, stream, gpu_id = _gpu_setup()
@@ -592,6 +614,8 @@ def main() -> None:
     ap.add_argument("--cpu-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extras", action="store_true", help="skip the batched/plain and gradient/forward ratios")
+    ap.add_argument("--profile-step", action="store_true",
+                    help="one step of the forward workload, each kernel launched alone in the NVTX range 'step' (for ncu)")
     ap.add_argument("--adjoint-nt", type=int, default=0,
                     help="adjoint workloads: time steps (default: the configuration's; shorter runs for profiling)")
     args = ap.parse_args()
@@ -602,7 +626,9 @@ def main() -> None:
         sys.exit(_relaunch_under_torchrun(args))
     if world and world != args.gpus:
         sys.exit(f"--gpus {args.gpus} but WORLD_SIZE={world}")
-    if args.impl == "reference":
+    if args.profile_step:
+        run_profile_step(args)
+    elif args.impl == "reference":
         run_reference(args)
     elif args.workload == BATCH:
         run_batch(args)

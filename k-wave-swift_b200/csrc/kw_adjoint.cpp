@@ -369,8 +369,13 @@ void Engine::adjoint(const kw_sim_desc& din, kw_adjoint_desc& a) {
     A.gc = gc;
     A.y = y;
 
-    auto job_in = [&](int in_field, int out, int nin, auto opf, int epi, int coupled, const char* name, int fanin = 0) {
+    // fwd_spec / r2c_done: row fusion (the adjoint velocity C2R transforms the new w_a into the
+    // summing job's input spectra, kw_jobs.cpp)
+    auto job_in = [&](int in_field, int out, int nin, auto opf, int epi, int coupled, const char* name, int fanin = 0,
+                      int fwd_spec = -1, int r2c_done = 0) {
         SpecJob j;
+        j.fwd_spec = fwd_spec;
+        j.r2c_done = r2c_done;
         j.in_field = in_field;
         j.nin = nin;
         j.nout = fanin ? 1 : nin;
@@ -384,9 +389,11 @@ void Engine::adjoint(const kw_sim_desc& din, kw_adjoint_desc& a) {
         j.name = name;
         issue_job(j, -1);
     };
-    auto job = [&](int in, int out, int nin, auto opf, int epi, int coupled, const char* name, int fanin = 0) {
-        job_in(FS_ADJ + in, out, nin, opf, epi, coupled, name, fanin);
+    auto job = [&](int in, int out, int nin, auto opf, int epi, int coupled, const char* name, int fanin = 0,
+                   int fwd_spec = -1, int r2c_done = 0) {
+        job_in(FS_ADJ + in, out, nin, opf, epi, coupled, name, fanin, fwd_spec, r2c_done);
     };
+    const bool fuse_w = D >= 2 && fuse_rows();
     // absorption filters: x1 with |k|^(y-2); x2 with |k|^(y-1) (A2(S(t)) comes from the tape)
     auto absorption_op = [](int c) { return OpSpec{AO_NONE, 0, (int8_t)(c == 0 ? RT_NU1 : RT_NU2), (int8_t)c}; };
     auto radial = [](int r) { return [r](int c) { return OpSpec{AO_NONE, 0, (int8_t)r, (int8_t)c}; }; };
@@ -420,10 +427,10 @@ void Engine::adjoint(const kw_sim_desc& din, kw_adjoint_desc& a) {
             issue_job(gj, -1);
         }
         if (fused) {
-            job(ADJ_W, ADJ_E, D, deriv(AO_DPOS), grho ? EPI_ADJ_VEL_RHO : EPI_ADJ_VEL, 0, "adj_vel");
+            job(ADJ_W, ADJ_E, D, deriv(AO_DPOS), grho ? EPI_ADJ_VEL_RHO : EPI_ADJ_VEL, 0, "adj_vel", 0, fuse_w ? 0 : -1);
             // lambda_p = sum_a D-_a w_a: the operator pass sums the components' spectra, so one
             // inverse transform serves all of them
-            job(ADJ_W, ADJ_E, D, deriv(AO_DNEG), EPI_ADJ_SUM, 1, "adj_sum", fanin ? 1 : 0);
+            job(ADJ_W, ADJ_E, D, deriv(AO_DNEG), EPI_ADJ_SUM, 1, "adj_sum", fanin ? 1 : 0, -1, fuse_w ? 1 : 0);
         } else {
             job(ADJ_W, ADJ_E, D, deriv(AO_DPOS), EPI_STORE, 0, "adj_dpos");
             launch_adj_vel(st(), d_sims_, N, A);

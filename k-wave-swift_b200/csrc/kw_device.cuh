@@ -7,6 +7,35 @@
 namespace kw {
 
 // ------------------------------------------------------------------------------------------
+// Programmatic dependent launch of the step's kernels. A kernel started by launch_pdl may be
+// scheduled while its predecessor grid drains: its first instruction waits until every
+// prerequisite grid has completed and its memory is visible (griddepcontrol.wait), and then
+// lets its own successor be scheduled (griddepcontrol.launch_dependents). Every kernel that
+// launch_pdl starts calls pdl_enter() before anything else, so each one still runs after the
+// whole of the previous one; for a launch without the attribute both are no-ops.
+// ------------------------------------------------------------------------------------------
+__device__ __forceinline__ void pdl_enter() {
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+bool pdl_enabled();   // KW_PDL=1 (kw_small.cu); off by default: plain stream order
+template <typename... KArgs, typename... Args>
+inline void launch_pdl(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t st,
+                       Args... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = pdl_enabled() ? 1 : 0;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    cudaLaunchKernelEx(&cfg, kernel, args...);
+}
+
+// ------------------------------------------------------------------------------------------
 // helpers
 // ------------------------------------------------------------------------------------------
 __device__ __forceinline__ void load_sim(SimDev& dst, const SimDev* __restrict__ src) {

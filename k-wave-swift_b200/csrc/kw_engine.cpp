@@ -9,7 +9,9 @@
 #include "kw_host.h"
 
 #include <algorithm>
+#include <chrono>
 #include <cmath>
+#include <cstdio>
 #include <cstring>
 #include <limits>
 
@@ -39,15 +41,97 @@ void* Engine::dalloc(size_t bytes) {
         check(cudaMemsetAsync(arena_ + off, 0, bytes, st()), "memset");
         return arena_ + off;
     }
-    void* p = nullptr;
-    cudaError_t e = cudaMalloc(&p, bytes);
-    if (e != cudaSuccess) {
-        cudaGetLastError();
-        throw err(KW_ERR_OOM, "device allocation of " + std::to_string(bytes) + " bytes failed: " + cudaGetErrorString(e));
+    const size_t rounded = Context::round_block(bytes);
+    void* p = ctx_->cache_take(rounded);
+    if (!p) {
+        cudaError_t e = cudaMalloc(&p, rounded);
+        if (e != cudaSuccess) {   // blocks kept for later creates may be what is missing
+            cudaGetLastError();
+            ctx_->cache_release();
+            e = cudaMalloc(&p, rounded);
+        }
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            throw err(KW_ERR_OOM, "device allocation of " + std::to_string(bytes) + " bytes failed: " + cudaGetErrorString(e));
+        }
     }
-    allocs_.push_back(p);
+    allocs_.emplace_back(p, rounded);
     check(cudaMemsetAsync(p, 0, bytes, st()), "memset");
     return p;
+}
+
+void* Context::cache_take(size_t rounded) {
+    std::lock_guard<std::mutex> lock(cache_mu);
+    auto it = cache.find(rounded);
+    if (it == cache.end()) return nullptr;
+    void* p = it->second;
+    cache.erase(it);
+    cached_bytes -= rounded;
+    return p;
+}
+
+void Context::cache_put(void* p, size_t rounded) {
+    std::lock_guard<std::mutex> lock(cache_mu);
+    cache.emplace(rounded, p);
+    cached_bytes += rounded;
+}
+
+void Context::cache_release() {
+    std::lock_guard<std::mutex> lock(cache_mu);
+    for (auto& kv : cache) cudaFree(kv.second);
+    cache.clear();
+    cached_bytes = 0;
+}
+
+Context::~Context() {
+    cache_release();
+    for (int b = 0; b < 2; ++b) {
+        if (stage_ev[b]) {
+            cudaEventSynchronize(stage_ev[b]);
+            cudaEventDestroy(stage_ev[b]);
+        }
+        if (stage[b]) cudaFreeHost(stage[b]);
+    }
+}
+
+void Engine::upload_host(void* dst, const void* src, size_t bytes) {
+    constexpr size_t kSub = 1u << 20;   // one host thread copies 1 MiB pieces of a chunk
+    Context& c = *ctx_;
+    std::unique_lock<std::mutex> lock(c.stage_mu);
+    if (bytes >= 2 * kSub && !c.stage[0]) {
+        bool ok = true;
+        for (int b = 0; b < 2 && ok; ++b)
+            ok = cudaHostAlloc(&c.stage[b], Context::kStageBytes, cudaHostAllocDefault) == cudaSuccess &&
+                 cudaEventCreateWithFlags(&c.stage_ev[b], cudaEventDisableTiming) == cudaSuccess;
+        if (!ok) {   // no pinned memory: plain copies from then on
+            cudaGetLastError();
+            for (int b = 0; b < 2; ++b) {
+                if (c.stage[b]) cudaFreeHost(c.stage[b]);
+                if (c.stage_ev[b]) cudaEventDestroy(c.stage_ev[b]);
+                c.stage[b] = nullptr;
+                c.stage_ev[b] = nullptr;
+            }
+        }
+    }
+    if (bytes < 2 * kSub || !c.stage[0] || !c.stage[1]) {
+        lock.unlock();
+        check(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, st()), "upload");
+        return;
+    }
+    const char* s = static_cast<const char*>(src);
+    char* d = static_cast<char*>(dst);
+    for (size_t off = 0, k = 0; off < bytes; off += Context::kStageBytes, ++k) {
+        const int b = (int)(k & 1);
+        check(cudaEventSynchronize(c.stage_ev[b]), "stage wait");   // the buffer's previous copy is done
+        const size_t len = std::min(Context::kStageBytes, bytes - off);
+        char* buf = static_cast<char*>(c.stage[b]);
+        parallel_for((long long)((len + kSub - 1) / kSub), [&](long long q) {
+            const size_t lo = (size_t)q * kSub, n = std::min(kSub, len - lo);
+            std::memcpy(buf + lo, s + off + lo, n);
+        }, 2);
+        check(cudaMemcpyAsync(d + off, buf, len, cudaMemcpyHostToDevice, st()), "upload");
+        check(cudaEventRecord(c.stage_ev[b], st()), "stage event");
+    }
 }
 
 Engine::~Engine() {
@@ -58,7 +142,10 @@ Engine::~Engine() {
         if (graph_[v]) cudaGraphDestroy(graph_[v]);
     }
     cudaStreamSynchronize(ctx_->stream);
-    for (void* p : allocs_) cudaFree(p);
+    if (cudaGetLastError() == cudaSuccess && !arena_)
+        for (auto& a : allocs_) ctx_->cache_put(a.first, a.second);   // kept for the next create
+    else
+        for (auto& a : allocs_) cudaFree(a.first);
 }
 
 // ------------------------------------------------------------------------------------------
@@ -297,7 +384,7 @@ void Engine::issue_step(bool first) {
         co.gate = GATE_RECU;
         co.name = "colloc";
         issue_job(co, -1);
-        if (!tune_mode_)
+        if (!tune_mode_ && !dry_)
             for (int a = 0; a < D; ++a) launch_sample(st(), d_sims_, d_t_, count(), max_pts_, 1, a);
     }
     timed("tick", 0, [&] { launch_tick(st(), d_t_); });
@@ -404,6 +491,19 @@ int Engine::capture_graph() {
     if (graph_exec_[var] && graph_stream_[var] == st()) return var;
     if (graph_exec_[var]) { cudaGraphExecDestroy(graph_exec_[var]); graph_exec_[var] = nullptr; }
     if (graph_[var]) { cudaGraphDestroy(graph_[var]); graph_[var] = nullptr; }
+    // a dry pass first: it creates every tile map this step variant needs (device allocations are
+    // not allowed inside the capture) and launches nothing. The axisymmetric step launches its own
+    // kernels directly and has one job structure, whose maps its first (uncaptured) step created.
+    if (!as_mode_) {
+        dry_ = true;
+        try {
+            issue_step(false);
+        } catch (...) {
+            dry_ = false;
+            throw;
+        }
+        dry_ = false;
+    }
     check(cudaStreamBeginCapture(st(), cudaStreamCaptureModeThreadLocal), "begin capture");
     try {
         issue_step(false);
@@ -489,6 +589,7 @@ void Engine::setup_sim(int s, const kw_sim_desc& d) {
     v.inv_n = (float)(1.0 / (double)N);
     for (int L = 0; L < 3; ++L) v.axis_of_layout[L] = L + h.dim - 3;
 
+    trace_phase("validate");
     // FFT plans
     const bool odd = (h.C & 1) != 0;
     build_plan(v.plan_row, odd ? h.C : h.C / 2);
@@ -507,6 +608,7 @@ void Engine::setup_sim(int s, const kw_sim_desc& d) {
     h.M = odd ? h.C : h.C / 2;
     max_M_ = std::max(max_M_, h.M);
 
+    trace_phase("plans");
     // device fields
     const size_t fb = (size_t)N * sizeof(float);
     const int nspec = h.dim + 1;
@@ -522,12 +624,17 @@ void Engine::setup_sim(int s, const kw_sim_desc& d) {
     v.wait_cycles = wait_cycles_;
     v.test_stall = test_stall_;
 
+    trace_phase("alloc fields");
     // ---- medium; smoothing on the device (KSFO:367-373) ----
     const bool c0map = d.sound_speed.len > 1, rho0map = d.density.len > 1;
-    std::vector<double> c0(c0map ? N : 1), rho0(rho0map && d.smooth_rho0 ? N : 1);
+    // FP64 host copies only of smoothed maps (their values come back from the device); an
+    // unsmoothed map is read from the caller's buffer where the host needs single values
+    const bool c0_host = c0map && d.smooth_c0;
+    std::vector<double> c0(c0_host ? N : 1), rho0(rho0map && d.smooth_rho0 ? N : 1);
+    c0[0] = d.sound_speed.data[0];
     auto smooth_to_host = [&](const float* src, std::vector<double>& dst) {
         float* f = (float*)dalloc(fb);
-        check(cudaMemcpyAsync(f, src, fb, cudaMemcpyHostToDevice, st()), "upload");
+        upload_host(f, src, fb);
         // the smoothing job needs the device descriptor (plans, buffers, window)
         check(cudaMemcpyAsync(d_sims_ + s, &v, sizeof(SimDev), cudaMemcpyHostToDevice, st()), "upload sim");
         smooth_field(s, f);
@@ -595,15 +702,14 @@ void Engine::setup_sim(int s, const kw_sim_desc& d) {
     // (kw_setup.cu); the host keeps c0 for c_ref and the source scales
     float* d_c0 = nullptr;
     float* d_rho0 = nullptr;
-    if (d.smooth_c0 && c0map) d_c0 = smooth_to_host(d.sound_speed.data, c0);
-    else parallel_for((long long)c0.size(), [&](long long i) { c0[i] = d.sound_speed.data[i]; });
-    if (c0map && !d_c0) d_c0 = upload_floats(d.sound_speed.data, N);
+    if (c0_host) d_c0 = smooth_to_host(d.sound_speed.data, c0);
+    else if (c0map) d_c0 = upload_floats(d.sound_speed.data, N);
     if (d.smooth_rho0 && rho0map) d_rho0 = smooth_to_host(d.density.data, rho0);
     else if (rho0map) d_rho0 = upload_floats(d.density.data, N);
     else rho0[0] = d.density.data[0];
     if (d.p0) {
         float* f = (float*)dalloc(fb);
-        check(cudaMemcpyAsync(f, d.p0, fb, cudaMemcpyHostToDevice, st()), "upload p0");
+        upload_host(f, d.p0, fb);
         if (d.smooth_p0) {
             check(cudaMemcpyAsync(d_sims_ + s, &v, sizeof(SimDev), cudaMemcpyHostToDevice, st()), "upload sim");
             smooth_field(s, f);
@@ -611,11 +717,19 @@ void Engine::setup_sim(int s, const kw_sim_desc& d) {
         h.p0s = f;
         v.has_p0 = 1;
     }
-    auto c0_at = [&](long long i) { return c0map ? c0[i] : c0[0]; };
+    auto c0_at = [&](long long i) -> double { return c0_host ? c0[i] : (c0map ? (double)d.sound_speed.data[i] : c0[0]); };
 
+    trace_phase("medium upload");
     // referenceSoundSpeed (KSFO:786-788), or the caller's fixed value
     double cref = c0[0];
-    if (c0map) {
+    if (c0map && !c0_host) {   // the largest value of the map, on the device (exact: a max)
+        check(cudaMemsetAsync(d_red_ + 2, 0, sizeof(unsigned int), st()), "memset");
+        launch_setup_max(st(), d_c0, N, d_red_ + 2);
+        unsigned int bits = 0;
+        check(cudaMemcpyAsync(&bits, d_red_ + 2, sizeof bits, cudaMemcpyDeviceToHost, st()), "c_ref");
+        check(cudaStreamSynchronize(st()), "c_ref");
+        cref = std::max(cref, (double)setup_max_decode(bits));
+    } else if (c0map) {
         const long long nchunk = 64, per = (N + nchunk - 1) / nchunk;
         std::vector<double> part(nchunk, c0[0]);
         parallel_for(nchunk, [&](long long ch) {
@@ -629,6 +743,7 @@ void Engine::setup_sim(int s, const kw_sim_desc& d) {
     h.cref = cref;
     const double dt = d.dt;
 
+    trace_phase("c_ref");
     // ---- per-axis operators, PML (KSFO:376-397, 764-769) ----
     std::vector<std::vector<double>> kv(h.dim);
     for (int a = 0; a < h.dim; ++a) {
@@ -653,6 +768,7 @@ void Engine::setup_sim(int s, const kw_sim_desc& d) {
         ax.inv_d = (float)(1.0 / dd);
     }
 
+    trace_phase("axis tables");
     // ---- medium-derived quantities ----
     // maps computed on the device in FP64 (kw_setup.cu), scalars here
     if (c0map) {
@@ -721,6 +837,7 @@ void Engine::setup_sim(int s, const kw_sim_desc& d) {
         }
     }
 
+    trace_phase("medium fields");
     // ---- sources (KSFO:404-423, 129-201) ----
     const double nd = (double)h.dim;
     bool need_skappa = false;
@@ -795,6 +912,7 @@ void Engine::setup_sim(int s, const kw_sim_desc& d) {
         }
     }
 
+    trace_phase("sources");
     // ---- radial tables over the half spectrum (FP64 -> FP32) ----
     {
         std::vector<double> kA(h.A, 0.0), kB(h.B, 0.0), kC(h.C, 0.0);
@@ -821,6 +939,7 @@ void Engine::setup_sim(int s, const kw_sim_desc& d) {
         v.radial[RT_NU2] = nu2;
     }
 
+    trace_phase("radial tables");
     // ---- sensor (REC:8-97) ----
     const unsigned rec = d.record;
     h.record_p = (rec & (KW_RECORD_P | KW_RECORD_P_MAX | KW_RECORD_P_MIN | KW_RECORD_P_RMS | KW_RECORD_I_AVG)) != 0;
@@ -944,8 +1063,10 @@ void Engine::setup_sim(int s, const kw_sim_desc& d) {
     }
     if (v.absorb >= 2) any_abs_ = true;
     if (v.has_p0) any_p0_ = true;
+    trace_phase("sensor");
     build_tensor_maps(h, v);
     check(cudaMemcpyAsync(d_sims_ + s, &v, sizeof(SimDev), cudaMemcpyHostToDevice, st()), "upload sim");
+    trace_phase("tensor maps");
 }
 
 // The k-space corrected additive source of a single-row signal (SourceOp.apply .additive,
@@ -970,6 +1091,16 @@ void Engine::precorrect_psrc(int s) {
     issue_job(q, s);
     v.psrc_q = v.src_buf[0];
     check(cudaMemcpyAsync(d_sims_ + s, &v, sizeof(SimDev), cudaMemcpyHostToDevice, st()), "upload sim");
+}
+
+// KW_TRACE_SETUP=1: wall time since the previous mark, per phase of create, on stderr (the
+// stream is synchronised first, so device work is counted where it was issued)
+void Engine::trace_phase(const char* what) {
+    if (!trace_) return;
+    check(cudaStreamSynchronize(st()), "trace sync");
+    const auto now = std::chrono::steady_clock::now();
+    std::fprintf(stderr, "kw setup: %-16s %8.2f ms\n", what, std::chrono::duration<double, std::milli>(now - trace_last_).count());
+    trace_last_ = now;
 }
 
 void Engine::create(const kw_sim_desc* descs, int n) {
@@ -1009,9 +1140,15 @@ void Engine::create(const kw_sim_desc* descs, int n) {
     d_t_ = (int*)dalloc(sizeof(int));
     d_flag_ = (int*)dalloc(2 * sizeof(int));   // [0] non-finite pressure, [1] device-side wait timeout
     d_red_ = (unsigned int*)dalloc(4 * sizeof(unsigned int));
+    const char* trace_env = std::getenv("KW_TRACE_SETUP");
+    trace_ = trace_env && trace_env[0] == '1';
+    trace_last_ = std::chrono::steady_clock::now();
+    auto phase = [&](const char* what) { trace_phase(what); };
     for (int i = 0; i < n; ++i) setup_sim(i, descs[i]);
+    phase("setup_sim");
     for (int i = 0; i < n; ++i)
         if (sims_[i].psrc_precorrect) precorrect_psrc(i);
+    phase("precorrect");
     std::vector<const float*> p0s(n);
     for (int i = 0; i < n; ++i) p0s[i] = sims_[i].p0s;
     d_p0s_ = (const float**)dalloc(sizeof(float*) * n);
@@ -1019,7 +1156,9 @@ void Engine::create(const kw_sim_desc* descs, int n) {
     if (as) create_as_carrier();
     check(cudaStreamSynchronize(st()), "setup sync");
     reset();
+    phase("reset");
     autotune();
+    phase("autotune");
 }
 
 void Engine::reset() {

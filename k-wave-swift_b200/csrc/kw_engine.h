@@ -1,8 +1,10 @@
 // kw_engine.h — host engine: setup (FP64 precompute), step sequencing, recording, outputs.
 #pragma once
 
+#include <chrono>
 #include <map>
 #include <memory>
+#include <mutex>
 #include <string>
 #include <tuple>
 #include <vector>
@@ -20,6 +22,28 @@ struct Context {
     cudaStream_t stream = nullptr;
     std::string err;
     int fail(int code, const std::string& msg) { err = msg; return code; }
+
+    // Device blocks of destroyed simulations, kept for the next create on this context (keyed by
+    // their rounded size; a create of the same problem finds every block it needs). A failed
+    // cudaMalloc releases the cache and tries once more. kw_context_destroy frees it.
+    std::mutex cache_mu;
+    std::multimap<size_t, void*> cache;
+    size_t cached_bytes = 0;
+    static size_t round_block(size_t bytes) {
+        return bytes >= (1u << 20) ? (bytes + (2u << 20) - 1) & ~(size_t)((2u << 20) - 1) : (bytes + 511) & ~(size_t)511;
+    }
+    void* cache_take(size_t rounded);
+    void cache_put(void* p, size_t rounded);
+    void cache_release();
+
+    // Two pinned staging buffers for host -> device uploads of large inputs: the host copy of one
+    // chunk (on several threads) overlaps the DMA of the previous one
+    static constexpr size_t kStageBytes = 8u << 20;
+    std::mutex stage_mu;
+    void* stage[2] = {nullptr, nullptr};
+    cudaEvent_t stage_ev[2] = {nullptr, nullptr};
+
+    ~Context();
 };
 
 // A status-carrying error used inside the engine; converted to kw_status at the ABI.
@@ -119,7 +143,7 @@ private:
     };
     template <class F>
     void timed(const std::string& name, double bytes, F&& f) {
-        if (tune_mode_) return;   // only the operator passes run (and are timed) in tune mode
+        if (tune_mode_ || dry_) return;   // only the operator passes run (and are timed) in tune mode
         if (!prof_) { f(); return; }
         ProfRec r{name, bytes, nullptr, nullptr};
         cudaEventCreate(&r.a);
@@ -144,9 +168,12 @@ private:
     // device copy of n host floats
     float* upload_floats(const float* src, long long n) {
         float* p = (float*)dalloc((size_t)n * sizeof(float));
-        check(cudaMemcpyAsync(p, src, (size_t)n * sizeof(float), cudaMemcpyHostToDevice, st()), "upload");
+        upload_host(p, src, (size_t)n * sizeof(float));
         return p;
     }
+    // host -> device copy of a caller's (pageable) buffer, staged through the context's pinned
+    // buffers when it is large
+    void upload_host(void* dst, const void* src, size_t bytes);
     void check(cudaError_t e, const char* what);
     cudaStream_t st() const { return st_override_ ? st_override_ : ctx_->stream; }
 
@@ -168,7 +195,7 @@ private:
 
     Context* ctx_;
     std::vector<SimHost> sims_;
-    std::vector<void*> allocs_;
+    std::vector<std::pair<void*, size_t>> allocs_;   // device blocks and their rounded sizes
     SimDev* d_sims_ = nullptr;
     int* d_t_ = nullptr;
     int* d_flag_ = nullptr;
@@ -199,6 +226,10 @@ private:
     void precorrect_psrc(int s);
     // autotuner of the operator column pass (kw_tune.cpp)
     bool tune_mode_ = false;
+    bool dry_ = false;
+    bool trace_ = false;   // KW_TRACE_SETUP=1
+    std::chrono::steady_clock::time_point trace_last_;
+    void trace_phase(const char* what);   // issue_step creates the tile maps but launches nothing (before a graph capture)
     std::string colop_key(int n, int axis, const ColJob& cj, int ntiles) const;
     ColopVariant colop_choice(int n, const std::string& key, bool tma_ok) const;
     void tune_colop(int n, int axis, int ncomp_map, int sim_only, const ColJob& cj, const std::string& key,

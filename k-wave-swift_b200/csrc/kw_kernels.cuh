@@ -144,6 +144,10 @@ void launch_setup_absorb(cudaStream_t st, const float* c0_map, double c0_s, cons
                          double np1, double y, int stokes, double tn, float* tau, float* eta, long long n);
 void launch_setup_radial(cudaStream_t st, const double* kA, const double* kB, const double* kC, int A, int B, int Ch,
                          int Cp, double half, double y, float* kap, float* skap, float* nu1, float* nu2);
+// largest value of x as order-preserving bits (atomicMax into *d_bits, zeroed by the caller) and
+// its decoding
+void launch_setup_max(cudaStream_t st, const float* x, long long n, unsigned int* d_bits);
+float setup_max_decode(unsigned int bits);
 
 // setup helpers on one field (single simulation)
 void launch_absmax(cudaStream_t st, const float* x, long long n, unsigned int* d_out_bits);

@@ -22,6 +22,7 @@ namespace kw {
 template <int N, int MODE>
 __global__ void __launch_bounds__(256, 2) k_cola(const SimDev* __restrict__ sims, const int* __restrict__ d_t,
                                                  const BlockWork* __restrict__ map, int nmap, ColJob job) {
+    pdl_enter();
     using P = RegPlan<N, reg_r1(N)>;
     using Lay = ColLayout<P, N>;
     constexpr int R1 = P::R1, T = P::T, TW = P::LINES;
@@ -239,7 +240,7 @@ static void cola_launch(cudaStream_t st, const SimDev* d_sims, const int* d_t, c
     static int grid_cap = 0;
     if (!grid_cap) grid_cap = persistent_grid((const void*)k_cola<N, MODE>, cola_land_bytes<N>(), 1 << 30);
     const int grid = nmap < grid_cap ? nmap : grid_cap;
-    k_cola<N, MODE><<<grid, 256, cola_land_bytes<N>(), st>>>(d_sims, d_t, map, nmap, job);
+    launch_pdl(k_cola<N, MODE>, grid, 256, cola_land_bytes<N>(), st, d_sims, d_t, map, nmap, job);
 }
 
 void launch_cola(cudaStream_t st, const SimDev* d_sims, const int* d_t, const BlockWork* map, int nmap,

@@ -128,6 +128,7 @@ __device__ __forceinline__ void colop_table(const SimDev& S, int rad, bool col_o
 template <int N, int R1V, int MINB>
 __global__ void __launch_bounds__(256, MINB) k_colop(const SimDev* __restrict__ sims, const int* __restrict__ d_t,
                                                const BlockWork* __restrict__ map, int nmap, ColJob job) {
+    pdl_enter();
     using P = RegPlan<N, R1V>;
     using Lay = ColLayout<P, N>;
     constexpr int R1 = P::R1, T = P::T, TW = P::LINES;
@@ -165,6 +166,7 @@ __global__ void __launch_bounds__(256, MINB) k_colop(const SimDev* __restrict__ 
 template <int N, int R1V>
 __global__ void __launch_bounds__(256, 2) k_colop_pf(const SimDev* __restrict__ sims, const int* __restrict__ d_t,
                                                      const BlockWork* __restrict__ map, int nmap, ColJob job) {
+    pdl_enter();
     using P = RegPlan<N, R1V>;
     using Lay = ColLayout<P, N>;
     constexpr int R1 = P::R1, T = P::T, TW = P::LINES;
@@ -235,6 +237,7 @@ template <int N>
 __global__ void __launch_bounds__(288, 2) k_colop_tma(const SimDev* __restrict__ sims, const int* __restrict__ d_t,
                                                       const BlockWork* __restrict__ map, int nmap, ColJob job, int ns,
                                                       int* __restrict__ err) {
+    pdl_enter();
     using P = RegPlan<N, 16>;
     using Lay = ColLayoutDense<P, N>;
     constexpr int R1 = P::R1, T = P::T, TW = P::LINES;
@@ -324,6 +327,7 @@ __global__ void __launch_bounds__(288, 2) k_colop_tma(const SimDev* __restrict__
 template <int N>
 __global__ void __launch_bounds__(256, 2) k_colop_fanin(const SimDev* __restrict__ sims, const int* __restrict__ d_t,
                                                         const BlockWork* __restrict__ map, int nmap, ColJob job) {
+    pdl_enter();
     using P = RegPlan<N, reg_r1(N)>;
     using Lay = ColLayout<P, N>;
     constexpr int R1 = P::R1, T = P::T, TW = P::LINES;
@@ -438,7 +442,7 @@ static void launch_colop_pf(cudaStream_t st, const SimDev* d_sims, const int* d_
         per_sm = 1;
     }
     const int grid = nmap < per_sm * sms ? nmap : per_sm * sms;
-    k_colop_pf<N, R1><<<grid, 256, smem, st>>>(d_sims, d_t, map, nmap, job);
+    launch_pdl(k_colop_pf<N, R1>, grid, 256, smem, st, d_sims, d_t, map, nmap, job);
 }
 
 // shared memory of the TMA-fed operator pass: `ns` stages, the parked product (several outputs),
@@ -474,7 +478,7 @@ static void launch_colop_tma(cudaStream_t st, const SimDev* d_sims, const int* d
         per_sm = 1;
     }
     const int grid = nmap < per_sm * sms ? nmap : per_sm * sms;
-    k_colop_tma<N><<<grid, 288, smem, st>>>(d_sims, d_t, map, nmap, job, ns, err);
+    launch_pdl(k_colop_tma<N>, grid, 288, smem, st, d_sims, d_t, map, nmap, job, ns, err);
 }
 
 bool colop_tma_length(int n) { return n == 128 || n == 256; }
@@ -500,7 +504,7 @@ void launch_colop(cudaStream_t st, const SimDev* d_sims, const int* d_t, const B
     if (job.fanin) {   // one variant (the adjoint's fan-in sum)
         switch (n) {
 #define KW_CASE(n) \
-    case n: k_colop_fanin<n><<<nmap, 256, colop_park_bytes(job, reg_r1(n)), st>>>(d_sims, d_t, map, nmap, job); break;
+    case n: launch_pdl(k_colop_fanin<n>, nmap, 256, colop_park_bytes(job, reg_r1(n)), st, d_sims, d_t, map, nmap, job); break;
             KW_COLOP_SIZES(KW_CASE)
 #undef KW_CASE
             default: break;
@@ -509,7 +513,7 @@ void launch_colop(cudaStream_t st, const SimDev* d_sims, const int* d_t, const B
     }
 #define KW_CASE(NN, RR, MB)                                                                                 \
     if (n == NN && v.r1 == RR && v.minb == MB) {                                                            \
-        k_colop<NN, RR, MB><<<nmap, 256, colop_park_bytes(job, RR), st>>>(d_sims, d_t, map, nmap, job);     \
+        launch_pdl(k_colop<NN, RR, MB>, nmap, 256, colop_park_bytes(job, RR), st, d_sims, d_t, map, nmap, job);     \
         return;                                                                                             \
     }
     KW_COLOP_VARIANTS(KW_CASE)

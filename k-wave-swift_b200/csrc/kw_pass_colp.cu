@@ -39,6 +39,7 @@ template <int N, bool INV>
 __global__ void __launch_bounds__(288, ColpCfg<N>::MINB) k_colp(const SimDev* __restrict__ sims, const int* __restrict__ d_t,
                                                                 const BlockWork* __restrict__ map, int nmap, ColJob job,
                                                                 int* __restrict__ err) {
+    pdl_enter();
     using Cfg = ColpCfg<N>;
     using P = typename Cfg::P;
     using Lay = ColLayout<P, N>;
@@ -170,7 +171,7 @@ static void launch_one(cudaStream_t st, const SimDev* d_sims, const int* d_t, co
         grid_cap = sms * (per_sm > 0 ? per_sm : 1);
     }
     const int grid = nmap < grid_cap ? nmap : grid_cap;
-    k_colp<N, INV><<<grid, 288, Cfg::SMEM, st>>>(d_sims, d_t, map, nmap, job, err);
+    launch_pdl(k_colp<N, INV>, grid, 288, Cfg::SMEM, st, d_sims, d_t, map, nmap, job, err);
 }
 
 template <bool INV>

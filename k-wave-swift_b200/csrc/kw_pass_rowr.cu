@@ -75,6 +75,7 @@ __device__ __forceinline__ void rowr_forward(float2 (&v)[P::R1], float2* sh, int
 template <int M>
 __global__ void __launch_bounds__(256) k_rowr_r2c(const SimDev* __restrict__ sims, const int* __restrict__ d_t,
                                                   const BlockWork* __restrict__ map, int nmap, RowR2CJob job) {
+    pdl_enter();
     using P = RegPlan<M, reg_r1(M)>;
     using Lay = RowLayout<P, M>;
     constexpr int R1 = P::R1, T = P::T, TW = P::LINES;
@@ -125,6 +126,7 @@ __device__ __forceinline__ float2 ld_ro(const float* p, long long e) { return __
 template <int M, int EPI, bool TAPE = false, int VAR = 0, bool FWD = false>
 __global__ void __launch_bounds__(256, rowr_minb<M, EPI, TAPE, VAR>()) k_rowr_c2r(const SimDev* __restrict__ sims, const int* __restrict__ d_t,
                                                   const BlockWork* __restrict__ map, int nmap, RowC2RJob job) {
+    pdl_enter();
     using P = RegPlan<M, c2r_r1(M)>;
     using Lay = RowLayout<P, M>;
     constexpr int R1 = P::R1, T = P::T, TW = P::LINES;
@@ -171,14 +173,15 @@ __global__ void __launch_bounds__(256, rowr_minb<M, EPI, TAPE, VAR>()) k_rowr_c2
     // slot 0); the number of transforms is uniform over the CTA (one simulation per CTA)
     auto forward_tail = [&]() {
         if constexpr (FWD) {
-            static_assert(EPI == EPI_VEL || EPI == EPI_DEN || EPI == EPI_DEN_SRC, "row fusion");
-            const int nf = EPI == EPI_VEL ? 1 : (S.absorb == 3 ? 2 : (S.absorb == 2 ? 1 : 0));
+            constexpr bool PER_COMP = EPI == EPI_VEL || EPI == EPI_ADJ_VEL || EPI == EPI_ADJ_VEL_RHO;
+            static_assert(PER_COMP || EPI == EPI_DEN || EPI == EPI_DEN_SRC, "row fusion");
+            const int nf = PER_COMP ? 1 : (S.absorb == 3 ? 2 : (S.absorb == 2 ? 1 : 0));
             for (int f = 0; f < nf; ++f) {
                 if (f == 1) {
 #pragma unroll
                     for (int m = 0; m < R1; ++m) v[m] = parked[m * 256 + threadIdx.x];
                 }
-                const int o = EPI == EPI_VEL ? comp0 : f;
+                const int o = PER_COMP ? comp0 : f;
                 rowr_forward<M, P, Lay>(v, sh, t, l, S.plan_row.twn, tw, S.spec[job.fwd_spec + o] + (long long)row * S.Cp, ok);
             }
         }
@@ -384,6 +387,7 @@ __global__ void __launch_bounds__(256, rowr_minb<M, EPI, TAPE, VAR>()) k_rowr_c2
                     }
                     st_state(lu, e, lo);
                     st_state(w, e, wo);
+                    if constexpr (FWD) v[m0 + b] = wo;
                 }
             } else if constexpr (EPI == EPI_ADJ_SUM) {
                 // lambda_p = sum_a d_a and the next reverse step's absorption inputs (the medium of the
@@ -518,7 +522,7 @@ __global__ void __launch_bounds__(256, rowr_minb<M, EPI, TAPE, VAR>()) k_rowr_c2
 #pragma unroll
                 for (int b = 0; b < MB; ++b) {
                     const long long e = rbase + 2 * (t + T * (m0 + b));
-                    rs[b] = ld_state(S.rho_sum, e);
+                    rs[b] = ld_ro(S.rho_sum, e);   // read-only here: may be issued ahead of the stores
                     c2[b] = ld_medium(S.c2, e);
                     tau[b] = ld_medium(S.tau, e);
                     if (S.absorb == 3) eta[b] = ld_medium(S.eta, e);
@@ -597,11 +601,11 @@ template <int M, int EPI, bool FWD = false>
 static void launch_var(int var, const SimDev* d_sims, const int* d_t, const BlockWork* map, int nmap, const RowC2RJob& job,
                        size_t smem, cudaStream_t st) {
     if constexpr (M == 128) {
-        if (var == 1) { k_rowr_c2r<M, EPI, false, 1, FWD><<<nmap, 256, smem, st>>>(d_sims, d_t, map, nmap, job); return; }
-        if (var == 2) { k_rowr_c2r<M, EPI, false, 2, FWD><<<nmap, 256, smem, st>>>(d_sims, d_t, map, nmap, job); return; }
-        if (var == 3) { k_rowr_c2r<M, EPI, false, 3, FWD><<<nmap, 256, smem, st>>>(d_sims, d_t, map, nmap, job); return; }
+        if (var == 1) { launch_pdl(k_rowr_c2r<M, EPI, false, 1, FWD>, nmap, 256, smem, st, d_sims, d_t, map, nmap, job); return; }
+        if (var == 2) { launch_pdl(k_rowr_c2r<M, EPI, false, 2, FWD>, nmap, 256, smem, st, d_sims, d_t, map, nmap, job); return; }
+        if (var == 3) { launch_pdl(k_rowr_c2r<M, EPI, false, 3, FWD>, nmap, 256, smem, st, d_sims, d_t, map, nmap, job); return; }
     }
-    k_rowr_c2r<M, EPI, false, 0, FWD><<<nmap, 256, smem, st>>>(d_sims, d_t, map, nmap, job);
+    launch_pdl(k_rowr_c2r<M, EPI, false, 0, FWD>, nmap, 256, smem, st, d_sims, d_t, map, nmap, job);
 }
 
 void init_rowr_attributes(int optin) {
@@ -620,7 +624,7 @@ void launch_rowr_r2c(cudaStream_t st, const SimDev* d_sims, const int* d_t, cons
     if (nmap <= 0) return;
     switch (M) {
 #define KW_CASE(m) \
-    case m: k_rowr_r2c<m><<<nmap, 256, 0, st>>>(d_sims, d_t, map, nmap, job); break;
+    case m: launch_pdl(k_rowr_r2c<m>, nmap, 256, 0, st, d_sims, d_t, map, nmap, job); break;
         KW_REG_ROW_SIZES(KW_CASE)
 #undef KW_CASE
         default: break;
@@ -632,15 +636,15 @@ static void launch_c2r_m(cudaStream_t st, const SimDev* d_sims, const int* d_t, 
                          const RowC2RJob& job) {
     const size_t smem = rowr_park_bytes<M>(job.ncomp);
     switch (job.epi) {
-        case EPI_STORE: k_rowr_c2r<M, EPI_STORE><<<nmap, 256, smem, st>>>(d_sims, d_t, map, nmap, job); break;
+        case EPI_STORE: launch_pdl(k_rowr_c2r<M, EPI_STORE>, nmap, 256, smem, st, d_sims, d_t, map, nmap, job); break;
         case EPI_VEL:
-            if (job.fwd) k_rowr_c2r<M, EPI_VEL, false, 0, true><<<nmap, 256, smem, st>>>(d_sims, d_t, map, nmap, job);
-            else k_rowr_c2r<M, EPI_VEL><<<nmap, 256, smem, st>>>(d_sims, d_t, map, nmap, job);
+            if (job.fwd) launch_pdl(k_rowr_c2r<M, EPI_VEL, false, 0, true>, nmap, 256, smem, st, d_sims, d_t, map, nmap, job);
+            else launch_pdl(k_rowr_c2r<M, EPI_VEL>, nmap, 256, smem, st, d_sims, d_t, map, nmap, job);
             break;
-        case EPI_VEL_INIT: k_rowr_c2r<M, EPI_VEL_INIT><<<nmap, 256, smem, st>>>(d_sims, d_t, map, nmap, job); break;
-        case EPI_ADD_U: k_rowr_c2r<M, EPI_ADD_U><<<nmap, 256, smem, st>>>(d_sims, d_t, map, nmap, job); break;
+        case EPI_VEL_INIT: launch_pdl(k_rowr_c2r<M, EPI_VEL_INIT>, nmap, 256, smem, st, d_sims, d_t, map, nmap, job); break;
+        case EPI_ADD_U: launch_pdl(k_rowr_c2r<M, EPI_ADD_U>, nmap, 256, smem, st, d_sims, d_t, map, nmap, job); break;
         case EPI_DEN:
-            if (job.tape) k_rowr_c2r<M, EPI_DEN, true><<<nmap, 256, smem, st>>>(d_sims, d_t, map, nmap, job);
+            if (job.tape) launch_pdl(k_rowr_c2r<M, EPI_DEN, true>, nmap, 256, smem, st, d_sims, d_t, map, nmap, job);
             else if (job.fwd) launch_var<M, EPI_DEN, true>(c2r_var(EPI_DEN), d_sims, d_t, map, nmap, job, smem, st);
             else launch_var<M, EPI_DEN>(c2r_var(EPI_DEN), d_sims, d_t, map, nmap, job, smem, st);
             break;
@@ -649,18 +653,24 @@ static void launch_c2r_m(cudaStream_t st, const SimDev* d_sims, const int* d_t, 
             else launch_var<M, EPI_DEN_SRC>(c2r_var(EPI_DEN_SRC), d_sims, d_t, map, nmap, job, smem, st);
             break;
         case EPI_ADD_RHO:
-            if (job.tape) k_rowr_c2r<M, EPI_ADD_RHO, true><<<nmap, 256, smem, st>>>(d_sims, d_t, map, nmap, job);
-            else k_rowr_c2r<M, EPI_ADD_RHO><<<nmap, 256, smem, st>>>(d_sims, d_t, map, nmap, job);
+            if (job.tape) launch_pdl(k_rowr_c2r<M, EPI_ADD_RHO, true>, nmap, 256, smem, st, d_sims, d_t, map, nmap, job);
+            else launch_pdl(k_rowr_c2r<M, EPI_ADD_RHO>, nmap, 256, smem, st, d_sims, d_t, map, nmap, job);
             break;
         case EPI_EOS_ABS:
-            if (job.tape) k_rowr_c2r<M, EPI_EOS_ABS, true><<<nmap, 256, smem, st>>>(d_sims, d_t, map, nmap, job);
+            if (job.tape) launch_pdl(k_rowr_c2r<M, EPI_EOS_ABS, true>, nmap, 256, smem, st, d_sims, d_t, map, nmap, job);
             else launch_var<M, EPI_EOS_ABS>(c2r_var(EPI_EOS_ABS), d_sims, d_t, map, nmap, job, smem, st);
             break;
-        case EPI_ADJ_VEL: k_rowr_c2r<M, EPI_ADJ_VEL><<<nmap, 256, smem, st>>>(d_sims, d_t, map, nmap, job); break;
-        case EPI_ADJ_VEL_RHO: k_rowr_c2r<M, EPI_ADJ_VEL_RHO><<<nmap, 256, smem, st>>>(d_sims, d_t, map, nmap, job); break;
-        case EPI_ADJ_SUM: k_rowr_c2r<M, EPI_ADJ_SUM><<<nmap, 256, smem, st>>>(d_sims, d_t, map, nmap, job); break;
-        case EPI_ADJ_EOS: k_rowr_c2r<M, EPI_ADJ_EOS><<<nmap, 256, smem, st>>>(d_sims, d_t, map, nmap, job); break;
-        case EPI_ADJ_EOS_RHO: k_rowr_c2r<M, EPI_ADJ_EOS_RHO><<<nmap, 256, smem, st>>>(d_sims, d_t, map, nmap, job); break;
+        case EPI_ADJ_VEL:
+            if (job.fwd) launch_pdl(k_rowr_c2r<M, EPI_ADJ_VEL, false, 0, true>, nmap, 256, smem, st, d_sims, d_t, map, nmap, job);
+            else launch_pdl(k_rowr_c2r<M, EPI_ADJ_VEL>, nmap, 256, smem, st, d_sims, d_t, map, nmap, job);
+            break;
+        case EPI_ADJ_VEL_RHO:
+            if (job.fwd) launch_pdl(k_rowr_c2r<M, EPI_ADJ_VEL_RHO, false, 0, true>, nmap, 256, smem, st, d_sims, d_t, map, nmap, job);
+            else launch_pdl(k_rowr_c2r<M, EPI_ADJ_VEL_RHO>, nmap, 256, smem, st, d_sims, d_t, map, nmap, job);
+            break;
+        case EPI_ADJ_SUM: launch_pdl(k_rowr_c2r<M, EPI_ADJ_SUM>, nmap, 256, smem, st, d_sims, d_t, map, nmap, job); break;
+        case EPI_ADJ_EOS: launch_pdl(k_rowr_c2r<M, EPI_ADJ_EOS>, nmap, 256, smem, st, d_sims, d_t, map, nmap, job); break;
+        case EPI_ADJ_EOS_RHO: launch_pdl(k_rowr_c2r<M, EPI_ADJ_EOS_RHO>, nmap, 256, smem, st, d_sims, d_t, map, nmap, job); break;
         default: break;
     }
 }

@@ -11,6 +11,9 @@
 //                                                                 (KSpaceFirstOrder.swift:376-378, 812-826)
 #include "kw_kernels.cuh"
 
+#include <algorithm>
+#include <cstring>
+
 namespace kw {
 
 __global__ void k_setup_c2(const float* __restrict__ c0, float* __restrict__ c2, long long n) {
@@ -68,7 +71,31 @@ __global__ void k_setup_radial(const double* __restrict__ kA, const double* __re
     if (nu2) nu2[i] = (float)(k == 0.0 ? 0.0 : pow(k, y - 1.0));
 }
 
+// max of x (NaNs ignored, as std::max(m, x) with m first ignores them) as order-preserving bits:
+// a float's bits with the sign bit flipped (non-negative) or all bits flipped (negative) compare
+// as unsigned integers in the order of the values, so one atomicMax per warp gives the maximum
+__global__ void k_setup_max(const float* __restrict__ x, long long n, unsigned int* out) {
+    float m = -INFINITY;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        m = fmaxf(m, x[i]);
+    for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+    const unsigned b = __float_as_uint(m);
+    if ((threadIdx.x & 31) == 0) atomicMax(out, (b & 0x80000000u) ? ~b : (b | 0x80000000u));
+}
+
 static unsigned blocks(long long n) { return (unsigned)((n + 255) / 256); }
+
+void launch_setup_max(cudaStream_t st, const float* x, long long n, unsigned int* d_bits) {
+    const long long b = std::min<long long>((n + 255) / 256, 148 * 8);
+    k_setup_max<<<(unsigned)(b < 1 ? 1 : b), 256, 0, st>>>(x, n, d_bits);
+}
+
+float setup_max_decode(unsigned int bits) {
+    const unsigned b = (bits & 0x80000000u) ? (bits & 0x7fffffffu) : ~bits;
+    float f;
+    std::memcpy(&f, &b, sizeof f);
+    return f;
+}
 
 void launch_setup_c2(cudaStream_t st, const float* c0, float* c2, long long n) {
     k_setup_c2<<<blocks(n), 256, 0, st>>>(c0, c2, n);

@@ -3,6 +3,7 @@
 #include "kw_device.cuh"
 
 #include <algorithm>
+#include <cstdlib>
 
 namespace kw {
 
@@ -100,6 +101,7 @@ void launch_scatter(cudaStream_t st, float* dst, const int* idx, const float* va
 // sensor sampling + recording (Recording.swift:37-45, 129-168). which = 0: p, 1: velocity
 // component `comp` (collocated field in tmp[comp]).
 __global__ void k_sample(const SimDev* __restrict__ sims, const int* __restrict__ d_t, int which, int comp) {
+    pdl_enter();
     const SimDev& S = sims[blockIdx.y];
     const int t = *d_t;
     if (t >= S.nt) return;
@@ -146,7 +148,10 @@ __global__ void k_sample(const SimDev* __restrict__ sims, const int* __restrict_
     }
 }
 
-__global__ void k_tick(int* d_t) { *d_t += 1; }
+__global__ void k_tick(int* d_t) {
+    pdl_enter();
+    *d_t += 1;
+}
 
 __global__ void k_check_finite(const SimDev* __restrict__ sims, const int* __restrict__ d_t,
                                const BlockWork* __restrict__ map) {
@@ -241,10 +246,20 @@ void launch_sample(cudaStream_t st, const SimDev* d_sims, const int* d_t, int ns
                    int comp) {
     if (max_pts <= 0) return;
     dim3 g((max_pts + 255) / 256, nsims);
-    k_sample<<<g, 256, 0, st>>>(d_sims, d_t, which, comp);
+    launch_pdl(k_sample, g, 256, 0, st, d_sims, d_t, which, comp);
 }
 
-void launch_tick(cudaStream_t st, int* d_t) { k_tick<<<1, 1, 0, st>>>(d_t); }
+void launch_tick(cudaStream_t st, int* d_t) { launch_pdl(k_tick, 1, 1, 0, st, d_t); }
+
+// Opt-in (KW_PDL=1): on a B200 the 256^3 step, captured as a CUDA graph, took 1.67 ms with the
+// attribute on every pass kernel against 1.46 ms without it (the per-launch times did not change).
+bool pdl_enabled() {
+    static const bool on = [] {
+        const char* e = std::getenv("KW_PDL");
+        return e && e[0] == '1';
+    }();
+    return on;
+}
 
 void launch_check_finite(cudaStream_t st, const SimDev* d_sims, const int* d_t, const BlockWork* map, int nblocks) {
     if (nblocks <= 0) return;

@@ -6,9 +6,10 @@ Each absorption mode (power law with and without dispersion: two and one fused t
 and lossless: velocity fusion only) is run on grids whose row count leaves the last C2R tile
 partly empty (rows past the end take part in the transforms' barriers only) and on a 128-point row
 length (the benchmark's instantiation), against the FP64 oracle (relative L2 <= 1e-4 on the p
-series and pFinal) and against the same run with fusion off (KW_FUSE_ROWS=0; the fused R2C uses
+series and pFinal) and against the same run with fusion off (the default; the fused R2C uses
 the C2R's radix split, so results agree to 1e-5 rather than bit for bit). A batch that mixes
-an absorbing and a lossless simulation runs each one as it runs alone, bit for bit.
+an absorbing and a lossless simulation runs each one as it runs alone. Fusion is opt-in
+(KW_FUSE_ROWS=1); the adjoint's fused reverse step is checked against the FP64 adjoint.
 """
 import numpy as np
 import pytest
@@ -67,6 +68,7 @@ def _run(b):
 @pytest.mark.parametrize("shape,pml", SHAPES, ids=lambda v: str(v))
 def test_fused_rows_match_oracle_and_unfused(shape, pml, mode, monkeypatch):
     monkeypatch.setenv("KW_AUTOTUNE", "0")
+    monkeypatch.setenv("KW_FUSE_ROWS", "1")
     b = _case(shape, pml, mode)
     fused = _run(b)
     ref, _ = oracle.run(b)
@@ -83,6 +85,7 @@ def test_batch_mixing_absorbing_and_lossless(monkeypatch):
     # lossless member's density update runs in the fused kernel instead of the plain one (the same
     # expressions, compiled in another kernel), so it is held to 1e-6
     monkeypatch.setenv("KW_AUTOTUNE", "0")
+    monkeypatch.setenv("KW_FUSE_ROWS", "1")
     builders = [_case((100, 128), 6, AbsorptionMode.powerLaw, seed=1), _case((100, 128), 6, AbsorptionMode.noAbsorption, seed=2),
                 _case((100, 128), 6, AbsorptionMode.noDispersion, seed=3)]
     singles = [_run(b) for b in builders]
@@ -98,3 +101,17 @@ def test_batch_mixing_absorbing_and_lossless(monkeypatch):
                 assert np.array_equal(p, singles[i]["p"]) and np.array_equal(pf, singles[i]["pFinal"]), i
     finally:
         batch.close()
+
+
+@pytest.mark.parametrize("shape,kw", [((36, 32), dict(absorb="nodispersion", nonlinear=True, cartesian=False, nt=40, no_p0=True)),
+                                      ((16, 20, 32), dict(absorb="powerlaw", nonlinear=True, cartesian=True, nt=30))])
+def test_fused_adjoint_matches_fp64_adjoint(shape, kw, monkeypatch):
+    # the forward fusions and the adjoint velocity C2R writing the summing job's spectra; 2D 36 x 32
+    # puts rows inside and past the end of the grid into one warp of the last C2R tile
+    from adjoint_cases import builder, problem
+    monkeypatch.setenv("KW_FUSE_ROWS", "1")
+    c, p0, data, kw = problem(shape, **kw)
+    L, gc, gp = oracle.adjoint(builder(shape, c, p0, **kw), data)
+    r = Context.default().adjoint(builder(shape, c, p0, **kw), data, grad_c0=True, grad_p0=p0 is not None)
+    assert abs(r["misfit"] - L) <= 1e-3 * L, (r["misfit"], L)
+    assert rel_l2(r["grad_c0"], gc) < 2e-3, rel_l2(r["grad_c0"], gc)
