@@ -370,7 +370,12 @@ void Engine::issue_step(bool first) {
             dj.name = "dir";
             issue_job(dj, -1);
         }
-    if (any_recp_) timed("sample_p", 0, [&] { launch_sample(st(), d_sims_, d_t_, count(), max_pts_, 0, 0); });
+    // the pressure sample, when it is the step's last launch, also advances the step counter
+    const bool tick_in_sample = any_recp_ && !any_recu_ && max_pts_ > 0;
+    if (any_recp_)
+        timed("sample_p", 0, [&] {
+            launch_sample(st(), d_sims_, d_t_, count(), max_pts_, 0, 0, tick_in_sample ? d_tickc_ : nullptr);
+        });
     if (any_recu_) {
         SpecJob co;
         co.in_field = FS_U;
@@ -387,7 +392,7 @@ void Engine::issue_step(bool first) {
         if (!tune_mode_ && !dry_)
             for (int a = 0; a < D; ++a) launch_sample(st(), d_sims_, d_t_, count(), max_pts_, 1, a);
     }
-    timed("tick", 0, [&] { launch_tick(st(), d_t_); });
+    if (!tick_in_sample) timed("tick", 0, [&] { launch_tick(st(), d_t_); });
 }
 
 bool Engine::host_gate(const SimHost& h, int gate, int comp) const {
@@ -1139,6 +1144,7 @@ void Engine::create(const kw_sim_desc* descs, int n) {
     d_sims_ = (SimDev*)dalloc(sizeof(SimDev) * n);
     d_t_ = (int*)dalloc(sizeof(int));
     d_flag_ = (int*)dalloc(2 * sizeof(int));   // [0] non-finite pressure, [1] device-side wait timeout
+    d_tickc_ = (unsigned int*)dalloc(sizeof(unsigned int));   // CTAs of the step's last sample that have read t
     d_red_ = (unsigned int*)dalloc(4 * sizeof(unsigned int));
     const char* trace_env = std::getenv("KW_TRACE_SETUP");
     trace_ = trace_env && trace_env[0] == '1';
@@ -1176,6 +1182,7 @@ void Engine::reset() {
             if (v.src_buf[a] && v.src_buf[a] != v.psrc_q) check(cudaMemsetAsync(v.src_buf[a], 0, fb, st()), "reset");
     }
     check(cudaMemsetAsync(d_t_, 0, sizeof(int), st()), "reset");
+    check(cudaMemsetAsync(d_tickc_, 0, sizeof(unsigned int), st()), "reset");
     check(cudaMemsetAsync(d_flag_, 0, 2 * sizeof(int), st()), "reset");
     t_ = 0;
     finalized_t_ = -1;

@@ -198,6 +198,7 @@ private:
     std::vector<std::pair<void*, size_t>> allocs_;   // device blocks and their rounded sizes
     SimDev* d_sims_ = nullptr;
     int* d_t_ = nullptr;
+    unsigned int* d_tickc_ = nullptr;   // see launch_sample
     int* d_flag_ = nullptr;
     const float** d_p0s_ = nullptr;
     unsigned int* d_red_ = nullptr;

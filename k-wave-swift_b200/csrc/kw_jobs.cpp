@@ -44,6 +44,11 @@ bool Engine::fuse_rows() const {
     const char* e = std::getenv("KW_FUSE_ROWS");
     return e && e[0] == '1';
 }
+// bulk L2 prefetch of the C2R epilogue's field rows (k_rowr_c2r); KW_C2R_PREFETCH=0 turns it off
+static bool c2r_prefetch() {
+    const char* e = std::getenv("KW_C2R_PREFETCH");
+    return !(e && e[0] == '0');
+}
 static int col_class(const SimHost& h, int axis) {
     const int n = axis == 0 ? h.A : h.B;
     return has_fixed_kernel(n) ? n : 0;
@@ -322,6 +327,7 @@ void Engine::issue_job(const SpecJob& job, int sim_only) {
         cj.tape = job.tape;
         cj.tile_elems = te;
         const bool reg = rowr_class(sc);
+        cj.prefetch = c2r_prefetch() ? 1 : 0;
         cj.fwd = job.fwd_spec >= 0 && reg && dim_ >= 2;
         cj.fwd_spec = job.fwd_spec;
         const Map& m = map_rows(reg ? -2 : ncta, job.coupled ? 1 : job.nout, sim_only, sc);

@@ -51,6 +51,7 @@ struct RowC2RJob {
     int generic;           // some simulation needs the runtime-plan (ping-pong) path
     long long tile_elems;
     int tape;              // the density / source / absorption epilogues also fill the adjoint tape
+    int prefetch;          // register row kernels: bulk-prefetch the CTA's rows of the epilogue's fields into L2
     int fwd;               // register row kernels: also run the forward R2C of the epilogue's output
     int fwd_spec;          // ... into spec[fwd_spec + o] (velocity: o = component; density: 0 = rho0 div u, 1 = rho_sum)
 };
@@ -131,8 +132,10 @@ void launch_init_p0(cudaStream_t st, const SimDev* d_sims, const int* d_t, const
                     const float* const* d_p0s);
 void launch_src_u(cudaStream_t st, const SimDev* d_sims, const int* d_t, int nsims, int max_src, int scatter_only);
 void launch_src_p(cudaStream_t st, const SimDev* d_sims, const int* d_t, int nsims, int max_src, int scatter_only);
-void launch_sample(cudaStream_t st, const SimDev* d_sims, const int* d_t, int nsims, int max_pts, int which,
-                   int comp);
+// tick_count (a zeroed device counter): the launch also advances the step counter *d_t once every
+// CTA has read it, for a sample that is the last launch of the step
+void launch_sample(cudaStream_t st, const SimDev* d_sims, int* d_t, int nsims, int max_pts, int which, int comp,
+                   unsigned int* tick_count = nullptr);
 void launch_tick(cudaStream_t st, int* d_t);
 void launch_scatter(cudaStream_t st, float* dst, const int* idx, const float* val, int n);
 void launch_check_finite(cudaStream_t st, const SimDev* d_sims, const int* d_t, const BlockWork* map, int nblocks);

@@ -147,6 +147,32 @@ __global__ void __launch_bounds__(256, rowr_minb<M, EPI, TAPE, VAR>()) k_rowr_c2
     const int comp0 = job.ncomp == 1 ? bw.comp : 0;
     const int ncomp = (EPI == EPI_EOS_ABS && S.absorb != 3) ? 1 : job.ncomp;
     const float2* __restrict__ tw = S.row_tw;
+    // The epilogue's field rows of this CTA are contiguous (TW rows of 2M floats): one thread asks
+    // for each of them to be brought into L2 now (cp.async.bulk.prefetch), so the epilogue's loads
+    // after the inverse transforms find them there. No registers or shared memory are involved.
+    if (job.prefetch && threadIdx.x == 0) {
+        const long long r0 = (long long)bw.tile * TW;
+        const long long nrows = min((long long)TW, (long long)S.A * S.B - r0);
+        const unsigned bytes = (unsigned)(nrows * 2 * M * sizeof(float));
+        auto pf = [&](const float* f) {
+            if (f) asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(f + r0 * 2 * M), "r"(bytes) : "memory");
+        };
+        if constexpr (EPI == EPI_VEL) {
+            pf(S.u[comp0]);
+            pf(S.dtor[comp0].ptr);
+        } else if constexpr (EPI == EPI_DEN || EPI == EPI_DEN_SRC) {
+            for (int a = 0; a < S.dim; ++a) pf(S.rho[a]);
+            pf(S.rho0.ptr);
+            if (EPI == EPI_DEN_SRC && psrc_gain(S, *d_t) != 0.f) pf(S.psrc_q);
+            if (S.eos_pointwise) { pf(S.c2.ptr); if (S.absorb == 1) pf(S.tau.ptr); if (S.nonlinear) pf(S.bona.ptr); }
+        } else if constexpr (EPI == EPI_EOS_ABS) {
+            pf(S.rho_sum);
+            pf(S.c2.ptr);
+            pf(S.tau.ptr);
+            if (S.absorb == 3) pf(S.eta.ptr);
+            if (S.nonlinear) { pf(S.bona.ptr); pf(S.rho0.ptr); }
+        }
+    }
 
     // Z'[k] = (X[k] + conj X[M-k]) + i exp(+2 pi i k / C) (X[k] - conj X[M-k]), X[0] and X[M] real
     float2 v[R1];

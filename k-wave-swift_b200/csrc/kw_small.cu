@@ -100,10 +100,8 @@ void launch_scatter(cudaStream_t st, float* dst, const int* idx, const float* va
 
 // sensor sampling + recording (Recording.swift:37-45, 129-168). which = 0: p, 1: velocity
 // component `comp` (collocated field in tmp[comp]).
-__global__ void k_sample(const SimDev* __restrict__ sims, const int* __restrict__ d_t, int which, int comp) {
-    pdl_enter();
+__device__ __forceinline__ void sample_one(const SimDev* __restrict__ sims, int t, int which, int comp) {
     const SimDev& S = sims[blockIdx.y];
-    const int t = *d_t;
     if (t >= S.nt) return;
     const SensorDev& sn = S.sensor;
     if (sn.kind == 0) return;
@@ -144,6 +142,24 @@ __global__ void k_sample(const SimDev* __restrict__ sims, const int* __restrict_
             const float tt = s + y;
             sn.u_ssc[comp][q] = (tt - s) - y;
             sn.u_ss[comp][q] = tt;
+        }
+    }
+}
+
+// tick_count != null: this launch is the last of the step and also advances the step counter,
+// once every CTA has read it (the last CTA to finish writes t + 1 and rearms the count)
+__global__ void k_sample(const SimDev* __restrict__ sims, int* d_t, int which, int comp, unsigned int* tick_count) {
+    pdl_enter();
+    const int t = *d_t;
+    sample_one(sims, t, which, comp);
+    if (tick_count) {
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            __threadfence();
+            if (atomicAdd(tick_count, 1u) == gridDim.x * gridDim.y - 1) {
+                *tick_count = 0;
+                *d_t = t + 1;
+            }
         }
     }
 }
@@ -242,11 +258,11 @@ void launch_src_p(cudaStream_t st, const SimDev* d_sims, const int* d_t, int nsi
     k_src_p<<<g, 256, 0, st>>>(d_sims, d_t, scatter_only);
 }
 
-void launch_sample(cudaStream_t st, const SimDev* d_sims, const int* d_t, int nsims, int max_pts, int which,
-                   int comp) {
+void launch_sample(cudaStream_t st, const SimDev* d_sims, int* d_t, int nsims, int max_pts, int which, int comp,
+                   unsigned int* tick_count) {
     if (max_pts <= 0) return;
     dim3 g((max_pts + 255) / 256, nsims);
-    launch_pdl(k_sample, g, 256, 0, st, d_sims, d_t, which, comp);
+    launch_pdl(k_sample, g, 256, 0, st, d_sims, d_t, which, comp, tick_count);
 }
 
 void launch_tick(cudaStream_t st, int* d_t) { launch_pdl(k_tick, 1, 1, 0, st, d_t); }
