@@ -157,6 +157,15 @@ __global__ void __launch_bounds__(256, rowr_minb<M, EPI, TAPE, VAR>()) k_rowr_c2
         auto pf = [&](const float* f) {
             if (f) asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(f + r0 * 2 * M), "r"(bytes) : "memory");
         };
+        auto pf64 = [&](const double* f) {   // FP64 accumulators
+            if (f) asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(f + r0 * 2 * M), "r"(2 * bytes) : "memory");
+        };
+        // the coupled components after the first are transformed after it: their spectrum rows too
+        for (int cc = 1; cc < ncomp; ++cc) {
+            const float2* X0 = S.spec[job.spec_in + comp0 + cc] + r0 * S.Cp;
+            asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(X0), "r"((unsigned)(nrows * S.Cp * sizeof(float2)))
+                         : "memory");
+        }
         if constexpr (EPI == EPI_VEL) {
             pf(S.u[comp0]);
             pf(S.dtor[comp0].ptr);
@@ -171,6 +180,23 @@ __global__ void __launch_bounds__(256, rowr_minb<M, EPI, TAPE, VAR>()) k_rowr_c2
             pf(S.tau.ptr);
             if (S.absorb == 3) pf(S.eta.ptr);
             if (S.nonlinear) { pf(S.bona.ptr); pf(S.rho0.ptr); }
+        } else if constexpr (EPI == EPI_ADJ_VEL || EPI == EPI_ADJ_VEL_RHO) {
+            pf(S.adj[ADJ_LU + comp0]);
+            pf(S.dtor[comp0].ptr);
+            if (EPI == EPI_ADJ_VEL_RHO) { pf(S.adj[ADJ_GP + comp0]); pf64(S.adj_gdtor[comp0]); }
+        } else if constexpr (EPI == EPI_ADJ_SUM) {
+            if (S.absorb >= 2) { pf(S.c2.ptr); pf(S.tau.ptr); if (S.absorb == 3) pf(S.eta.ptr); }
+        } else if constexpr (AEOS) {
+            pf(S.adj[ADJ_LP]); pf(S.adj[ADJ_PTP]); pf(S.adj[ADJ_STP]);
+            pf(S.c2.ptr); pf(S.rho0.ptr); pf(S.tau.ptr);
+            if (S.absorb == 3) { pf(S.eta.ptr); pf(S.adj[ADJ_Q2]); }
+            if (S.nonlinear) { pf(S.bona.ptr); pf(S.adj[ADJ_SPRP]); }
+            for (int a = 0; a < S.dim; ++a) {
+                pf(S.adj[ADJ_LR + a]);
+                if (S.nonlinear || EPI == EPI_ADJ_EOS_RHO) pf(S.adj[ADJ_DDP + a]);
+            }
+            pf64(S.adj_gc);
+            if (EPI == EPI_ADJ_EOS_RHO) pf64(S.adj_gr);
         }
     }
 
