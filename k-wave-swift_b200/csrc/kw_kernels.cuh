@@ -82,7 +82,7 @@ __host__ __device__ constexpr int colop_tile(int n, int r1) { return reg_lines(n
 // minb of the TMA-fed, warp-specialised variant (kw_pass_colop.cu): 3D operator passes along A of
 // the lengths colop_tma_length(n) whose simulations have the A-axis tensor maps (r1 = 16)
 constexpr int kColopTma = -1;
-constexpr int kColopPf = -2;   // persistent, next tile prefetched into registers
+constexpr int kColopPf = -10;   // persistent L2-prefetching variants: minb = kColopPf - CTAs per SM
 bool colop_tma_length(int n);
 int colop_variants(int n, ColopVariant* out, int max);
 void init_colop_attributes(int optin);

@@ -158,14 +158,16 @@ __global__ void __launch_bounds__(256, MINB) k_colop(const SimDev* __restrict__ 
     colop_body<N, P, Lay, BlockSync>(S, job, bw.comp, v, sh, parked, tsl, t, l, c, col_ok, base, inner, axisA, rad);
 }
 
-// Persistent variant with the next tile's spectrum loaded into registers while this tile is
-// transformed: each CTA walks the tile map with stride gridDim.x; the loads of tile i + 1 are issued
-// before the transforms of tile i and are waited on only when tile i + 1 starts, so every SM keeps
-// loads in flight through the compute phase (two CTAs per SM: the prefetch takes R1 more float2
-// registers a thread).
-template <int N, int R1V>
-__global__ void __launch_bounds__(256, 2) k_colop_pf(const SimDev* __restrict__ sims, const int* __restrict__ d_t,
-                                                     const BlockWork* __restrict__ map, int nmap, ColJob job) {
+// Persistent variant: each CTA walks the tile map with stride gridDim.x, and before transforming
+// tile i it asks for tile i + 1's rows of the spectrum and of its radial table to be brought into
+// L2 (cp.async.bulk.prefetch, one per row segment and thread; no registers or shared memory), so
+// the loads of the next tile find them there. The tile's own work is k_colop's.
+__device__ __forceinline__ void prefetch_l2(const void* p, unsigned bytes) {
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
+}
+template <int N, int R1V, int MINB>
+__global__ void __launch_bounds__(256, MINB) k_colop_pf(const SimDev* __restrict__ sims, const int* __restrict__ d_t,
+                                                        const BlockWork* __restrict__ map, int nmap, ColJob job) {
     pdl_enter();
     using P = RegPlan<N, R1V>;
     using Lay = ColLayout<P, N>;
@@ -185,26 +187,28 @@ __global__ void __launch_bounds__(256, 2) k_colop_pf(const SimDev* __restrict__ 
         }
         return idx;
     };
-    auto load = [&](int idx, float2 (&dst)[R1]) {
+    // tile idx's N row segments (TW columns, the last tile possibly fewer: a multiple of 4, so every
+    // segment is a multiple of 16 bytes and starts 16-byte aligned)
+    auto prefetch = [&](int idx) {
         const BlockWork bw = map[idx];
         const SimDev& S = sims[bw.sim];
         const int inner = axisA ? S.B * S.Cp : S.Cp;
-        const int c = bw.tile * TW + l;
-        const bool col_ok = c < inner;
-        const float2* in = S.spec[job.spec_in + (job.fanout ? 0 : bw.comp)] + (col_ok ? c : 0);
-#pragma unroll
-        for (int r = 0; r < R1; ++r) dst[r] = col_ok ? in[(long long)(t + T * r) * inner] : make_float2(0.f, 0.f);
+        const int c0 = bw.tile * TW;
+        const int w = min(TW, inner - c0);
+        const int comp_in = job.fanout ? 0 : bw.comp;
+        const float2* in = S.spec[job.spec_in + comp_in] + c0;
+        const int rad = (comp_in == 0 ? job.op[0] : (comp_in == 1 ? job.op[1] : job.op[2])).radial;
+        const float* tab = rad != RT_NONE ? S.radial[rad] + c0 : nullptr;
+        for (int r = threadIdx.x; r < N; r += blockDim.x) {
+            prefetch_l2(in + (long long)r * inner, (unsigned)w * 8u);
+            if (tab) prefetch_l2(tab + (long long)r * inner, (unsigned)w * 4u);
+        }
     };
     int idx = next_open(blockIdx.x);
-    float2 nx[R1];
-    if (idx < nmap) load(idx, nx);
     while (idx < nmap) {
-        float2 v[R1];
-#pragma unroll
-        for (int r = 0; r < R1; ++r) v[r] = nx[r];
         const int cur = idx;
         idx = next_open(idx + gridDim.x);
-        if (idx < nmap) load(idx, nx);   // in flight during the transforms below
+        if (idx < nmap) prefetch(idx);   // comes into L2 during the transforms below
         const BlockWork bw = map[cur];
         const SimDev& S = sims[bw.sim];
         const int inner = axisA ? S.B * S.Cp : S.Cp;
@@ -212,8 +216,12 @@ __global__ void __launch_bounds__(256, 2) k_colop_pf(const SimDev* __restrict__ 
         const bool col_ok = c < inner;
         const long long base = col_ok ? c : 0;
         const int comp_in = job.fanout ? 0 : bw.comp;
+        const float2* in = S.spec[job.spec_in + comp_in] + base;
         const int rad = (comp_in == 0 ? job.op[0] : (comp_in == 1 ? job.op[1] : job.op[2])).radial;
         colop_table<R1, T>(S, rad, col_ok, base, inner, t, tsl);
+        float2 v[R1];
+#pragma unroll
+        for (int r = 0; r < R1; ++r) v[r] = col_ok ? in[(long long)(t + T * r) * inner] : make_float2(0.f, 0.f);
         colop_body<N, P, Lay, BlockSync>(S, job, bw.comp, v, sh, parked, tsl, t, l, c, col_ok, base, inner, axisA, rad);
     }
 }
@@ -397,14 +405,14 @@ static size_t colop_park_bytes(const ColJob& job, int r1) {
     return (size_t)r1 * 256 * ((park ? sizeof(float2) : 0) + (table ? sizeof(float) : 0));
 }
 
-// (N, R1) of the persistent prefetching variant (minb = kColopPf)
-#define KW_COLOP_PF(X) X(128, 16) X(256, 16) X(256, 8) X(512, 16) X(512, 8) X(192, 12) X(384, 12)
+// (N, R1, CTAs per SM) of the persistent L2-prefetching variant (minb = kColopPf - CTAs per SM)
+#define KW_COLOP_PF(X) X(128, 16, 3) X(256, 16, 3) X(256, 16, 2) X(256, 8, 3) X(512, 16, 2) X(512, 8, 3) X(192, 12, 3) X(384, 12, 2)
 
 void init_colop_attributes(int optin) {
 #define KW_SET(NN, RR, MB) set_max_smem((const void*)k_colop<NN, RR, MB>, optin);
     KW_COLOP_VARIANTS(KW_SET)
 #undef KW_SET
-#define KW_SET(NN, RR) set_max_smem((const void*)k_colop_pf<NN, RR>, optin);
+#define KW_SET(NN, RR, MB) set_max_smem((const void*)k_colop_pf<NN, RR, MB>, optin);
     KW_COLOP_PF(KW_SET)
 #undef KW_SET
 #define KW_SET(n) set_max_smem((const void*)k_colop_fanin<n>, optin);
@@ -418,14 +426,14 @@ int colop_variants(int n, ColopVariant* out, int max) {
     if (n == NN && k < max) out[k++] = ColopVariant{RR, MB};
     KW_COLOP_VARIANTS(KW_ADD)
 #undef KW_ADD
-#define KW_ADD(NN, RR) \
-    if (n == NN && k < max) out[k++] = ColopVariant{RR, kColopPf};
+#define KW_ADD(NN, RR, MB) \
+    if (n == NN && k < max) out[k++] = ColopVariant{RR, kColopPf - MB};
     KW_COLOP_PF(KW_ADD)
 #undef KW_ADD
     return k;
 }
 
-template <int N, int R1>
+template <int N, int R1, int MB>
 static void launch_colop_pf(cudaStream_t st, const SimDev* d_sims, const int* d_t, const BlockWork* map, int nmap,
                             const ColJob& job) {
     static int sms = 0;
@@ -436,13 +444,13 @@ static void launch_colop_pf(cudaStream_t st, const SimDev* d_sims, const int* d_
     }
     const size_t smem = colop_park_bytes(job, R1);
     int per_sm = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void*)k_colop_pf<N, R1>, 256, smem) != cudaSuccess ||
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void*)k_colop_pf<N, R1, MB>, 256, smem) != cudaSuccess ||
         per_sm < 1) {
         cudaGetLastError();
         per_sm = 1;
     }
     const int grid = nmap < per_sm * sms ? nmap : per_sm * sms;
-    launch_pdl(k_colop_pf<N, R1>, grid, 256, smem, st, d_sims, d_t, map, nmap, job);
+    launch_pdl(k_colop_pf<N, R1, MB>, grid, 256, smem, st, d_sims, d_t, map, nmap, job);
 }
 
 // shared memory of the TMA-fed operator pass: `ns` stages, the parked product (several outputs),
@@ -491,10 +499,10 @@ void launch_colop(cudaStream_t st, const SimDev* d_sims, const int* d_t, const B
         else if (n == 128) launch_colop_tma<128>(st, d_sims, d_t, map, nmap, job, err);
         return;
     }
-    if (v.minb == kColopPf && !job.fanin) {
-#define KW_CASE(NN, RR)                                                      \
-    if (n == NN && v.r1 == RR) {                                             \
-        launch_colop_pf<NN, RR>(st, d_sims, d_t, map, nmap, job);            \
+    if (v.minb <= kColopPf && !job.fanin) {
+#define KW_CASE(NN, RR, MB)                                                  \
+    if (n == NN && v.r1 == RR && v.minb == kColopPf - MB) {                  \
+        launch_colop_pf<NN, RR, MB>(st, d_sims, d_t, map, nmap, job);        \
         return;                                                              \
     }
         KW_COLOP_PF(KW_CASE)

@@ -22,10 +22,11 @@ pytestmark = pytest.mark.gpu
 # (shape, operator-axis length): 3D passes run along A, 2D along B
 SHAPES = [((256, 24, 32), 256), ((128, 24, 32), 128), ((192, 16, 24), 192), ((512, 64), 512)]
 # (r1, minb); minb -1 is the TMA-fed warp-specialised kernel (3D passes along A of 128 and 256),
-# minb -2 the persistent kernel that prefetches the next tile into registers
-VARIANTS = {16: [], 256: [(16, 3), (16, 2), (8, 3), (8, 4), (16, -2), (8, -2), (16, -1)],
-            128: [(16, 3), (16, 2), (8, 3), (8, 4), (16, -2), (16, -1)],
-            192: [(12, 3), (12, 2), (12, 4), (12, -2)], 512: [(16, 0), (16, 2), (8, 2), (8, 3), (8, 4), (16, -2), (8, -2)]}
+# minb -10 - m the persistent kernel with m CTAs per SM that prefetches its next tile into L2
+VARIANTS = {16: [], 256: [(16, 3), (16, 2), (8, 3), (8, 4), (16, -13), (16, -12), (8, -13), (16, -1)],
+            128: [(16, 3), (16, 2), (8, 3), (8, 4), (16, -13), (16, -1)],
+            192: [(12, 3), (12, 2), (12, 4), (12, -13)],
+            512: [(16, 0), (16, 2), (8, 2), (8, 3), (8, 4), (16, -12), (8, -13)]}
 
 
 def _run(b):
