@@ -72,6 +72,18 @@ void* Context::cache_take(size_t rounded) {
 
 void Context::cache_put(void* p, size_t rounded) {
     std::lock_guard<std::mutex> lock(cache_mu);
+    if (!cache_cap) {   // a quarter of the device's memory
+        size_t free_b = 0, total_b = 0;
+        if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) {
+            cudaGetLastError();
+            total_b = 0;
+        }
+        cache_cap = total_b ? total_b / 4 : (size_t)1 << 30;
+    }
+    if (cached_bytes + rounded > cache_cap) {   // over the cap: give the block back
+        cudaFree(p);
+        return;
+    }
     cache.emplace(rounded, p);
     cached_bytes += rounded;
 }

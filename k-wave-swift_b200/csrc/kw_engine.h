@@ -24,11 +24,13 @@ struct Context {
     int fail(int code, const std::string& msg) { err = msg; return code; }
 
     // Device blocks of destroyed simulations, kept for the next create on this context (keyed by
-    // their rounded size; a create of the same problem finds every block it needs). A failed
-    // cudaMalloc releases the cache and tries once more. kw_context_destroy frees it.
+    // their rounded size; a create of the same problem finds every block it needs), up to a
+    // quarter of the device's memory. A failed cudaMalloc releases the cache and tries once more.
+    // kw_context_destroy frees it.
     std::mutex cache_mu;
     std::multimap<size_t, void*> cache;
     size_t cached_bytes = 0;
+    size_t cache_cap = 0;   // at most this much is kept (a quarter of device memory)
     static size_t round_block(size_t bytes) {
         return bytes >= (1u << 20) ? (bytes + (2u << 20) - 1) & ~(size_t)((2u << 20) - 1) : (bytes + 511) & ~(size_t)511;
     }
