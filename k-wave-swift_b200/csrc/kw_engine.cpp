@@ -106,26 +106,70 @@ Context::~Context() {
     }
 }
 
+// device -> host copy into a caller's (pageable) buffer, staged through the context's pinned
+// buffers when it is large: the DMA of chunk k + 1 runs while the host threads copy chunk k out
+// of the other buffer. Returns when the data are in `dst`.
+void Engine::download_host(void* dst, const void* src, size_t bytes) {
+    constexpr size_t kSub = 1u << 20;
+    Context& c = *ctx_;
+    std::unique_lock<std::mutex> lock(c.stage_mu);
+    if (bytes < 2 * kSub || !stage_ready_locked()) {
+        lock.unlock();
+        check(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, st()), "output copy");
+        check(cudaStreamSynchronize(st()), "output copy");
+        return;
+    }
+    const char* s = static_cast<const char*>(src);
+    char* d = static_cast<char*>(dst);
+    const size_t nchunk = (bytes + Context::kStageBytes - 1) / Context::kStageBytes;
+    auto host_copy = [&](size_t k) {   // chunk k from its buffer to the caller's
+        const int b = (int)(k & 1);
+        check(cudaEventSynchronize(c.stage_ev[b]), "stage wait");
+        const size_t off = k * Context::kStageBytes, len = std::min(Context::kStageBytes, bytes - off);
+        const char* buf = static_cast<const char*>(c.stage[b]);
+        parallel_for((long long)((len + kSub - 1) / kSub), [&](long long q) {
+            const size_t lo = (size_t)q * kSub, n = std::min(kSub, len - lo);
+            std::memcpy(d + off + lo, buf + lo, n);
+        }, 2);
+    };
+    for (size_t k = 0; k < nchunk; ++k) {
+        const int b = (int)(k & 1);
+        const size_t off = k * Context::kStageBytes, len = std::min(Context::kStageBytes, bytes - off);
+        check(cudaEventSynchronize(c.stage_ev[b]), "stage wait");   // its previous copy is finished
+        check(cudaMemcpyAsync(c.stage[b], s + off, len, cudaMemcpyDeviceToHost, st()), "output copy");
+        check(cudaEventRecord(c.stage_ev[b], st()), "stage event");
+        if (k > 0) host_copy(k - 1);
+    }
+    host_copy(nchunk - 1);
+}
+
+// the two pinned staging buffers and their events, allocated on first use (false: no pinned memory)
+bool Engine::stage_ready_locked() {
+    Context& c = *ctx_;
+    if (c.stage[0] && c.stage[1]) return true;
+    if (c.stage_failed) return false;
+    bool ok = true;
+    for (int b = 0; b < 2 && ok; ++b)
+        ok = cudaHostAlloc(&c.stage[b], Context::kStageBytes, cudaHostAllocDefault) == cudaSuccess &&
+             cudaEventCreateWithFlags(&c.stage_ev[b], cudaEventDisableTiming) == cudaSuccess;
+    if (!ok) {   // plain copies from then on
+        cudaGetLastError();
+        for (int b = 0; b < 2; ++b) {
+            if (c.stage[b]) cudaFreeHost(c.stage[b]);
+            if (c.stage_ev[b]) cudaEventDestroy(c.stage_ev[b]);
+            c.stage[b] = nullptr;
+            c.stage_ev[b] = nullptr;
+        }
+        c.stage_failed = true;
+    }
+    return ok;
+}
+
 void Engine::upload_host(void* dst, const void* src, size_t bytes) {
     constexpr size_t kSub = 1u << 20;   // one host thread copies 1 MiB pieces of a chunk
     Context& c = *ctx_;
     std::unique_lock<std::mutex> lock(c.stage_mu);
-    if (bytes >= 2 * kSub && !c.stage[0]) {
-        bool ok = true;
-        for (int b = 0; b < 2 && ok; ++b)
-            ok = cudaHostAlloc(&c.stage[b], Context::kStageBytes, cudaHostAllocDefault) == cudaSuccess &&
-                 cudaEventCreateWithFlags(&c.stage_ev[b], cudaEventDisableTiming) == cudaSuccess;
-        if (!ok) {   // no pinned memory: plain copies from then on
-            cudaGetLastError();
-            for (int b = 0; b < 2; ++b) {
-                if (c.stage[b]) cudaFreeHost(c.stage[b]);
-                if (c.stage_ev[b]) cudaEventDestroy(c.stage_ev[b]);
-                c.stage[b] = nullptr;
-                c.stage_ev[b] = nullptr;
-            }
-        }
-    }
-    if (bytes < 2 * kSub || !c.stage[0] || !c.stage[1]) {
+    if (bytes < 2 * kSub || !stage_ready_locked()) {
         lock.unlock();
         check(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, st()), "upload");
         return;
@@ -1348,19 +1392,15 @@ void Engine::get_output(int i, int f, float* dst, size_t count) {
     if (count != n) throw err(KW_ERR_INVALID, "output buffer size mismatch");
     const SensorDev& sn = h.dev.sensor;
     const size_t np = (size_t)h.npts;
-    auto d2h = [&](const float* src, float* d, size_t cnt) {
-        check(cudaMemcpyAsync(d, src, cnt * sizeof(float), cudaMemcpyDeviceToHost, st()), "output copy");
-    };
+    auto d2h = [&](const float* src, float* d, size_t cnt) { download_host(d, src, cnt * sizeof(float)); };
     auto series = [&](const float* dev) {   // [T][np] on the device -> [np][T] row-major
         std::vector<float> tmp((size_t)T * np);
         d2h(dev, tmp.data(), tmp.size());
-        check(cudaStreamSynchronize(st()), "sync");
         transpose_series(tmp.data(), dst, (size_t)T, np);
     };
     auto rms = [&](const float* ss) {
         std::vector<float> tmp(np);
         d2h(ss, tmp.data(), np);
-        check(cudaStreamSynchronize(st()), "sync");
         for (size_t q = 0; q < np; ++q) dst[q] = std::sqrt(tmp[q] / (float)T);
     };
     switch (f) {

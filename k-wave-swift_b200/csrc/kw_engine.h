@@ -44,6 +44,7 @@ struct Context {
     std::mutex stage_mu;
     void* stage[2] = {nullptr, nullptr};
     cudaEvent_t stage_ev[2] = {nullptr, nullptr};
+    bool stage_failed = false;   // no pinned memory could be had: plain copies
 
     ~Context();
 };
@@ -176,6 +177,8 @@ private:
     // host -> device copy of a caller's (pageable) buffer, staged through the context's pinned
     // buffers when it is large
     void upload_host(void* dst, const void* src, size_t bytes);
+    void download_host(void* dst, const void* src, size_t bytes);   // synchronous, staged when large
+    bool stage_ready_locked();   // with Context::stage_mu held
     void check(cudaError_t e, const char* what);
     cudaStream_t st() const { return st_override_ ? st_override_ : ctx_->stream; }
 
