@@ -44,6 +44,17 @@ bool Engine::fuse_rows() const {
     const char* e = std::getenv("KW_FUSE_ROWS");
     return e && e[0] == '1';
 }
+// Traversal order of the tile maps. A pass reads what the previous one wrote, and the last part
+// written (up to ~100 MB at 256^3) is still in L2 when the next kernel starts; CTAs are started
+// in map order, so a pass over the same plane-major layout that walks its tiles the other way
+// round starts on those lines. The R2C and the inverse pass along B walk forwards, the forward
+// pass along B and the C2R backwards (the operator pass along A reads every plane in each tile
+// and breaks the chain). KW_MAP_ORDER=0: every map forwards.
+static bool alternate_order() {
+    const char* e = std::getenv("KW_MAP_ORDER");
+    return !(e && e[0] == '0');
+}
+
 // bulk L2 prefetch of the C2R epilogue's field rows (k_rowr_c2r); KW_C2R_PREFETCH=0 turns it off
 static bool c2r_prefetch() {
     const char* e = std::getenv("KW_C2R_PREFETCH");
@@ -59,8 +70,8 @@ static int col_class(const SimHost& h, int axis) {
 // lines_per_row rows (a coupled C2R epilogue stages every component of a row in the same CTA);
 // lines_per_row = -1 / -2: tiles of r2c_rows(M) / c2r_rows(M) rows for the register-resident R2C /
 // C2R kernels.
-const Engine::Map& Engine::map_rows(int lines_per_row, int ncomp, int sim_only, int sclass) {
-    auto key = std::make_tuple(0, lines_per_row, ncomp, sim_only, sclass);
+const Engine::Map& Engine::map_rows(int lines_per_row, int ncomp, int sim_only, int sclass, bool reverse) {
+    auto key = std::make_tuple(reverse ? 20 : 0, lines_per_row, ncomp, sim_only, sclass);
     auto it = maps_.find(key);
     if (it != maps_.end()) return it->second;
     std::vector<BlockWork> v;
@@ -75,6 +86,7 @@ const Engine::Map& Engine::map_rows(int lines_per_row, int ncomp, int sim_only, 
         for (int c = 0; c < ncomp; ++c)
             for (int tI = 0; tI < tiles; ++tI) v.push_back(BlockWork{s, c, tI});
     }
+    if (reverse) std::reverse(v.begin(), v.end());
     Map m;
     m.d = upload(v);
     m.n = (int)v.size();
@@ -83,8 +95,8 @@ const Engine::Map& Engine::map_rows(int lines_per_row, int ncomp, int sim_only, 
 
 // Column-pass tiles: col_lines(n) (col_lines_op(n) for an operator pass) contiguous columns, or
 // for the register-plan lengths colr_lines(n) (colop_lines(n)) columns of one plane.
-const Engine::Map& Engine::map_cols(int axis, int ncomp, int sim_only, bool op, int sclass, int tw_op) {
-    auto key = std::make_tuple(1 + axis + (op ? 2 : 0), tw_op, ncomp, sim_only, sclass);
+const Engine::Map& Engine::map_cols(int axis, int ncomp, int sim_only, bool op, int sclass, int tw_op, bool reverse) {
+    auto key = std::make_tuple(1 + axis + (op ? 2 : 0) + (reverse ? 20 : 0), tw_op, ncomp, sim_only, sclass);
     auto it = maps_.find(key);
     if (it != maps_.end()) return it->second;
     std::vector<BlockWork> v;
@@ -106,6 +118,7 @@ const Engine::Map& Engine::map_cols(int axis, int ncomp, int sim_only, bool op, 
         for (int c = 0; c < ncomp; ++c)
             for (int tI = 0; tI < tiles; ++tI) v.push_back(BlockWork{s, c, tI});
     }
+    if (reverse) std::reverse(v.begin(), v.end());
     Map m;
     m.d = upload(v);
     m.n = (int)v.size();
@@ -246,7 +259,7 @@ void Engine::issue_job(const SpecJob& job, int sim_only) {
             cj.gate = job.gate;
             cj.tile_elems = te;
             if (mode == COL_INV) cj.spec_in = job.spec_out, cj.fanout = 0;
-            const Map& m = map_cols(axis, ncomp_map, sim_only, op, sc);
+            const Map& m = map_cols(axis, ncomp_map, sim_only, op, sc, 0, mode == COL_FWD && alternate_order());
             const double bytes = sum_sims(in_class, bytes_of);
             const long long tiles = sc ? (op ? 4 : 2) : (op ? 5 : 3);
             const size_t smem = (size_t)(tiles * te * sizeof(float2));
@@ -330,7 +343,7 @@ void Engine::issue_job(const SpecJob& job, int sim_only) {
         cj.prefetch = c2r_prefetch() ? 1 : 0;
         cj.fwd = job.fwd_spec >= 0 && reg && dim_ >= 2;
         cj.fwd_spec = job.fwd_spec;
-        const Map& m = map_rows(reg ? -2 : ncta, job.coupled ? 1 : job.nout, sim_only, sc);
+        const Map& m = map_rows(reg ? -2 : ncta, job.coupled ? 1 : job.nout, sim_only, sc, alternate_order());
         const double bytes = sum_sims(in_class, [&](const SimHost& h) {
             int no = job.coupled ? (open_comps(h, 1) ? job.nout : 0) : open_comps(h, job.nout);
             if (job.epi == EPI_EOS_ABS && no) no = h.dev.absorb == 3 ? 2 : 1;
