@@ -189,7 +189,8 @@ private:
     void smooth_field(int s, float* field);
     const Map& map_rows(int lines_per_row, int ncomp, int sim_only, int sclass, bool reverse = false);
     // tw > 0: tiles of tw columns (the register operator pass of the chosen variant)
-    const Map& map_cols(int axis, int ncomp, int sim_only, bool op, int sclass, int tw = 0, bool reverse = false);
+    // order: 0 forwards, 1 backwards, 2 / 3 column-chunk-major forwards / backwards (kw_jobs.cpp)
+    const Map& map_cols(int axis, int ncomp, int sim_only, bool op, int sclass, int tw = 0, int order = 0);
     const Map& map_elems(int sim_only);
     const Map& map_planes(int ncomp, int sim_only);
     void issue_job(const SpecJob& job, int sim_only);

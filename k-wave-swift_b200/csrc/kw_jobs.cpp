@@ -50,10 +50,14 @@ bool Engine::fuse_rows() const {
 // round starts on those lines. The R2C and the inverse pass along B walk forwards, the forward
 // pass along B and the C2R backwards (the operator pass along A reads every plane in each tile
 // and breaks the chain). KW_MAP_ORDER=0: every map forwards.
-static bool alternate_order() {
+// KW_MAP_ORDER=2: the column passes walk column-chunk-major instead (forward pass along B
+// forwards, operator pass backwards, inverse pass along B forwards), so the column-to-column
+// transitions start on the resident lines rather than the row-to-column ones.
+static int map_order_policy() {
     const char* e = std::getenv("KW_MAP_ORDER");
-    return !(e && e[0] == '0');
+    return e ? std::atoi(e) : 1;
 }
+static bool alternate_order() { return map_order_policy() != 0; }
 
 // bulk L2 prefetch of the C2R epilogue's field rows (k_rowr_c2r); KW_C2R_PREFETCH=0 turns it off
 static bool c2r_prefetch() {
@@ -95,8 +99,8 @@ const Engine::Map& Engine::map_rows(int lines_per_row, int ncomp, int sim_only, 
 
 // Column-pass tiles: col_lines(n) (col_lines_op(n) for an operator pass) contiguous columns, or
 // for the register-plan lengths colr_lines(n) (colop_lines(n)) columns of one plane.
-const Engine::Map& Engine::map_cols(int axis, int ncomp, int sim_only, bool op, int sclass, int tw_op, bool reverse) {
-    auto key = std::make_tuple(1 + axis + (op ? 2 : 0) + (reverse ? 20 : 0), tw_op, ncomp, sim_only, sclass);
+const Engine::Map& Engine::map_cols(int axis, int ncomp, int sim_only, bool op, int sclass, int tw_op, int order) {
+    auto key = std::make_tuple(1 + axis + (op ? 2 : 0) + 20 * order, tw_op, ncomp, sim_only, sclass);
     auto it = maps_.find(key);
     if (it != maps_.end()) return it->second;
     std::vector<BlockWork> v;
@@ -106,19 +110,33 @@ const Engine::Map& Engine::map_cols(int axis, int ncomp, int sim_only, bool op, 
         const int n = axis == 0 ? h.A : h.B;
         const int inner = axis == 0 ? h.B * h.Cp : h.Cp;
         const int outer = axis == 0 ? 1 : h.A;
-        int tiles;
+        int tiles, tw;
         const bool reg = op ? has_colop(sclass) : (has_colp(sclass) || (has_colop(sclass) && !(cola_policy() & 4)));
         if (sclass && reg) {   // register-plan kernels: columns of one plane
-            const int tw = op ? (tw_op > 0 ? tw_op : colop_lines(n)) : colr_lines(n);
+            tw = op ? (tw_op > 0 ? tw_op : colop_lines(n)) : colr_lines(n);
             tiles = outer * ((inner + tw - 1) / tw);
         } else {
-            const int tw = op ? col_lines_op(n) : col_lines(n);
+            tw = op ? col_lines_op(n) : col_lines(n);
             tiles = outer * ((inner + tw - 1) / tw);
         }
+        // tile order within a component: plane-major (as numbered), or for order 2 / 3 and the
+        // register-plan kernels column-chunk-major (all planes / rows of one chunk of spectrum
+        // bins together, chunks by their first bin)
+        std::vector<int> seq(tiles);
+        for (int tI = 0; tI < tiles; ++tI) seq[tI] = tI;
+        if (order >= 2 && sclass && reg) {
+            const int nch = (inner + tw - 1) / tw;
+            auto rank = [&](int tI) -> long long {
+                if (axis == 1) return (long long)(tI % nch) * outer + tI / nch;   // (chunk, plane)
+                const int c0 = tI * tw;                                          // (bin, row of B)
+                return (long long)(c0 % h.Cp) * h.B + c0 / h.Cp;
+            };
+            std::stable_sort(seq.begin(), seq.end(), [&](int x, int y) { return rank(x) < rank(y); });
+        }
         for (int c = 0; c < ncomp; ++c)
-            for (int tI = 0; tI < tiles; ++tI) v.push_back(BlockWork{s, c, tI});
+            for (int tI : seq) v.push_back(BlockWork{s, c, tI});
     }
-    if (reverse) std::reverse(v.begin(), v.end());
+    if (order == 1 || order == 3) std::reverse(v.begin(), v.end());
     Map m;
     m.d = upload(v);
     m.n = (int)v.size();
@@ -259,7 +277,9 @@ void Engine::issue_job(const SpecJob& job, int sim_only) {
             cj.gate = job.gate;
             cj.tile_elems = te;
             if (mode == COL_INV) cj.spec_in = job.spec_out, cj.fanout = 0;
-            const Map& m = map_cols(axis, ncomp_map, sim_only, op, sc, 0, mode == COL_FWD && alternate_order());
+            const int pol = map_order_policy();
+            const int ord = pol == 2 ? (op ? 3 : 2) : (mode == COL_FWD && pol != 0 ? 1 : 0);
+            const Map& m = map_cols(axis, ncomp_map, sim_only, op, sc, 0, ord);
             const double bytes = sum_sims(in_class, bytes_of);
             const long long tiles = sc ? (op ? 4 : 2) : (op ? 5 : 3);
             const size_t smem = (size_t)(tiles * te * sizeof(float2));
@@ -281,7 +301,7 @@ void Engine::issue_job(const SpecJob& job, int sim_only) {
                     tune_colop(sc, axis, ncomp_map, sim_only, cj, key, tma_ok);
                 } else {
                     const ColopVariant v = colop_choice(sc, key, tma_ok);
-                    const Map& mv = map_cols(axis, ncomp_map, sim_only, op, sc, colop_tile(sc, v.r1));
+                    const Map& mv = map_cols(axis, ncomp_map, sim_only, op, sc, colop_tile(sc, v.r1), ord);
                     timed(std::string(label) + job.name, bytes,
                           [&] { launch_colop(st(), d_sims_, d_t_, mv.d, mv.n, cj, sc, v, d_flag_ + 1); });
                 }
