@@ -5,7 +5,7 @@
 // per CTA) and a launch bound of resident CTAs per SM. Which is fastest depends on the length, the
 // number of outputs, the tile count and the GPU. At the end of kw_sim_create / kw_batch_create the
 // engine issues one time step in tune mode: every launch is skipped except the operator passes,
-// whose variants are each timed with CUDA events (one warm-up launch, then three) on the job's own
+// whose variants are each timed with CUDA events (two warm-up launches, then ten) on the job's own
 // tile map, and the fastest is kept for that key. The spectra the passes overwrite are scratch
 // between jobs, so timing them before the first step changes no result.
 //
@@ -132,6 +132,9 @@ private:
     }
 };
 
+// launches per candidate: untimed, then timed back to back (the mean is kept)
+constexpr int kTuneWarm = 2, kTuneReps = 10;
+
 bool autotune_enabled() {
     const char* e = std::getenv("KW_AUTOTUNE");
     return !(e && e[0] == '0');
@@ -201,15 +204,15 @@ void Engine::tune_colop(int n, int axis, int ncomp_map, int sim_only, const ColJ
     double best_us = 1e300;
     for (int k = 0; k < nc; ++k) {
         const Map& m = map_cols(axis, ncomp_map, sim_only, true, n, colop_tile(n, cands[k].r1));
-        launch_colop(st(), d_sims_, d_t_, m.d, m.n, cj, n, cands[k], d_flag_ + 1);   // warm-up
+        for (int r = 0; r < kTuneWarm; ++r) launch_colop(st(), d_sims_, d_t_, m.d, m.n, cj, n, cands[k], d_flag_ + 1);
         check(cudaEventRecord(a, st()), "event");
-        for (int r = 0; r < 3; ++r) launch_colop(st(), d_sims_, d_t_, m.d, m.n, cj, n, cands[k], d_flag_ + 1);
+        for (int r = 0; r < kTuneReps; ++r) launch_colop(st(), d_sims_, d_t_, m.d, m.n, cj, n, cands[k], d_flag_ + 1);
         check(cudaEventRecord(b, st()), "event");
         check(cudaEventSynchronize(b), "tune sync");
         check(cudaGetLastError(), "tune launch");
         float ms = 0;
         cudaEventElapsedTime(&ms, a, b);
-        const double us = 1e3 * ms / 3.0;
+        const double us = 1e3 * ms / kTuneReps;
         if (us < best_us) {
             best_us = us;
             best = k;
