@@ -81,16 +81,24 @@ private:
         for (const char* c = p.name; *c; ++c) s += std::isalnum((unsigned char)*c) ? *c : '_';
         return s;
     }
-    static std::string resolve_path() {
+    // $KW_TUNE_CACHE (read on every lookup: tests change it), else the per-GPU default, resolved
+    // once per process (it queries the device properties and creates the directory)
+    std::string resolve_path() {
         if (const char* e = std::getenv("KW_TUNE_CACHE")) return e;
-        if (const char* h = std::getenv("HOME")) {
-            const std::string dir = std::string(h) + "/.cache/kwave_b200";
-            mkdir((std::string(h) + "/.cache").c_str(), 0755);
-            mkdir(dir.c_str(), 0755);
-            return dir + "/tune_" + gpu_tag() + ".json";
+        if (!default_resolved_) {
+            default_resolved_ = true;
+            if (const char* h = std::getenv("HOME")) {
+                const std::string dir = std::string(h) + "/.cache/kwave_b200";
+                mkdir((std::string(h) + "/.cache").c_str(), 0755);
+                mkdir(dir.c_str(), 0755);
+                default_path_ = dir + "/tune_" + gpu_tag() + ".json";
+            }
         }
-        return "";
+        return default_path_;
     }
+    bool default_resolved_ = false;
+    std::string default_path_;
+    std::string gpu_name_;
     // (re)load when the cache file in effect changed (KW_TUNE_CACHE set or changed in the process)
     void load_locked() {
         const std::string want = resolve_path();
@@ -113,7 +121,8 @@ private:
     void save_locked() {
         if (path_.empty()) return;
         std::ostringstream o;
-        o << "{\n \"kernel\": \"k_colop\",\n \"gpu\": \"" << gpu_tag() << "\",\n \"choices\": {\n";
+        if (gpu_name_.empty()) gpu_name_ = gpu_tag();
+        o << "{\n \"kernel\": \"k_colop\",\n \"gpu\": \"" << gpu_name_ << "\",\n \"choices\": {\n";
         size_t i = 0;
         for (const auto& kv : map_) {
             char buf[96];
