@@ -269,12 +269,9 @@ void launch_tick(cudaStream_t st, int* d_t) { launch_pdl(k_tick, 1, 1, 0, st, d_
 
 // Opt-in (KW_PDL=1): on a B200 the 256^3 step, captured as a CUDA graph, took 1.67 ms with the
 // attribute on every pass kernel against 1.46 ms without it (the per-launch times did not change).
-bool pdl_enabled() {
-    static const bool on = [] {
-        const char* e = std::getenv("KW_PDL");
-        return e && e[0] == '1';
-    }();
-    return on;
+bool pdl_enabled() {   // read on every launch (a test switches it between simulations)
+    const char* e = std::getenv("KW_PDL");
+    return e && e[0] == '1';
 }
 
 void launch_check_finite(cudaStream_t st, const SimDev* d_sims, const int* d_t, const BlockWork* map, int nblocks) {
