@@ -59,6 +59,26 @@ static int map_order_policy() {
 }
 static bool alternate_order() { return map_order_policy() != 0; }
 
+// The register R2C and the one-component C2R kernels also prefetch into L2 the rows of the CTA one
+// resident wave on (the SM count times the resident CTAs per SM of the kernel). Measured at 256^3:
+// R2C 3-5 % and the velocity C2R 5 % faster, while the coupled density and power-law C2R, which
+// already prefetch their epilogues' fields, got 4-11 % slower with it, so those do not.
+// KW_ROW_AHEAD=0 turns it off.
+static int row_ahead(int per_sm) {
+    const char* e = std::getenv("KW_ROW_AHEAD");
+    if (e && e[0] == '0') return 0;
+    static int sms = 0;
+    if (!sms) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) {
+            cudaGetLastError();
+            sms = 1;
+        }
+    }
+    return sms * per_sm;
+}
+
 // bulk L2 prefetch of the C2R epilogue's field rows (k_rowr_c2r); KW_C2R_PREFETCH=0 turns it off
 static bool c2r_prefetch() {
     const char* e = std::getenv("KW_C2R_PREFETCH");
@@ -242,6 +262,7 @@ void Engine::issue_job(const SpecJob& job, int sim_only) {
         te = round4(te);
         rj.tile_elems = te;
         const bool reg = rowr_class(sc) && !rj.apply_op;
+        rj.ahead = reg ? row_ahead(4) : 0;   // 64 registers: four CTAs per SM
         const Map& m = map_rows(reg ? -1 : 0, comps_in, sim_only, sc);
         const double bytes = sum_sims(in_class, [&](const SimHost& h) { return open_comps(h, comps_in) * ((double)h.N * 4 + spec_bytes(h)); });
         const size_t smem = (size_t)(has_fixed_kernel(sc) ? 2 : 3) * te * sizeof(float2);
@@ -361,6 +382,7 @@ void Engine::issue_job(const SpecJob& job, int sim_only) {
         cj.tile_elems = te;
         const bool reg = rowr_class(sc);
         cj.prefetch = c2r_prefetch() ? 1 : 0;
+        cj.ahead = reg && ncta == 1 ? row_ahead(3) : 0;   // three CTAs per SM (the 128-point epilogues)
         cj.fwd = job.fwd_spec >= 0 && reg && dim_ >= 2;
         cj.fwd_spec = job.fwd_spec;
         const Map& m = map_rows(reg ? -2 : ncta, job.coupled ? 1 : job.nout, sim_only, sc, alternate_order());

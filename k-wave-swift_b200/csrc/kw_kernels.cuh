@@ -27,6 +27,7 @@ struct RowR2CJob {
     OpSpec op[kMaxComp];
     int gate;
     long long tile_elems;  // float2 elements of one staged tile (max over the launch's simulations)
+    int ahead;             // register rows: > 0, prefetch into L2 the input rows of the CTA this many entries on
 };
 
 struct ColJob {
@@ -52,6 +53,7 @@ struct RowC2RJob {
     long long tile_elems;
     int tape;              // the density / source / absorption epilogues also fill the adjoint tape
     int prefetch;          // register row kernels: bulk-prefetch the CTA's rows of the epilogue's fields into L2
+    int ahead;             // > 0: also the spectrum rows of the CTA this many map entries on (the next wave)
     int fwd;               // register row kernels: also run the forward R2C of the epilogue's output
     int fwd_spec;          // ... into spec[fwd_spec + o] (velocity: o = component; density: 0 = rho0 div u, 1 = rho_sum)
 };

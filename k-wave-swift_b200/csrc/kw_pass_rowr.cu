@@ -87,6 +87,17 @@ __global__ void __launch_bounds__(256) k_rowr_r2c(const SimDev* __restrict__ sim
     const int t = threadIdx.x % T, l = threadIdx.x / T;
     const int row = bw.tile * TW + l;
     const bool ok = row < S.A * S.B;
+    if (job.ahead > 0 && threadIdx.x == 0 && blockIdx.x + job.ahead < nmap) {
+        // the input rows of the CTA one resident wave on, into L2 (contiguous: its TW rows)
+        const BlockWork nb = map[blockIdx.x + job.ahead];
+        const SimDev& S2 = sims[nb.sim];
+        const long long r0 = (long long)nb.tile * TW;
+        const long long nrows = min((long long)TW, (long long)S2.A * S2.B - r0);
+        const float* f = field_ptr(S2, job.in_field, nb.comp);
+        if (f && nrows > 0)
+            asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(f + r0 * 2 * M),
+                         "r"((unsigned)(nrows * 2 * M * sizeof(float))) : "memory");
+    }
     const float2* in = reinterpret_cast<const float2*>(field_ptr(S, job.in_field, bw.comp) + (long long)row * (2 * M));
     float2 v[R1];
 #pragma unroll
@@ -160,6 +171,17 @@ __global__ void __launch_bounds__(256, rowr_minb<M, EPI, TAPE, VAR>()) k_rowr_c2
         auto pf64 = [&](const double* f) {   // FP64 accumulators
             if (f) asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(f + r0 * 2 * M), "r"(2 * bytes) : "memory");
         };
+        // the spectrum rows of the CTA one resident wave on (all its components)
+        if (job.ahead > 0 && blockIdx.x + job.ahead < nmap) {
+            const BlockWork nb = map[blockIdx.x + job.ahead];
+            const SimDev& S2 = sims[nb.sim];
+            const long long q0 = (long long)nb.tile * TW;
+            const long long nq = min((long long)TW, (long long)S2.A * S2.B - q0);
+            const int c0n = job.ncomp == 1 ? nb.comp : 0;
+            for (int cc = 0; cc < job.ncomp && nq > 0; ++cc)
+                asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(S2.spec[job.spec_in + c0n + cc] + q0 * S2.Cp),
+                             "r"((unsigned)(nq * S2.Cp * sizeof(float2))) : "memory");
+        }
         // the coupled components after the first are transformed after it: their spectrum rows too
         for (int cc = 1; cc < ncomp; ++cc) {
             const float2* X0 = S.spec[job.spec_in + comp0 + cc] + r0 * S.Cp;
