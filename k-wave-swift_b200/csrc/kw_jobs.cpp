@@ -79,6 +79,13 @@ static int row_ahead(int per_sm) {
     return sms * per_sm;
 }
 
+// KW_COLP_AHEAD=n: the TMA-fed in-place column pass also prefetches into L2 (one tensor prefetch)
+// the tile n of its tiles on, beyond its two-stage ring; 0 (default): none
+static int colp_ahead() {
+    const char* e = std::getenv("KW_COLP_AHEAD");
+    return e ? std::max(0, std::atoi(e)) : 0;
+}
+
 // bulk L2 prefetch of the C2R epilogue's field rows (k_rowr_c2r); KW_C2R_PREFETCH=0 turns it off
 static bool c2r_prefetch() {
     const char* e = std::getenv("KW_C2R_PREFETCH");
@@ -297,6 +304,7 @@ void Engine::issue_job(const SpecJob& job, int sim_only) {
             for (int c = 0; c < kMaxComp; ++c) cj.op[c] = job.op[c];
             cj.gate = job.gate;
             cj.tile_elems = te;
+            cj.tma_ahead = colp_ahead();
             if (mode == COL_INV) cj.spec_in = job.spec_out, cj.fanout = 0;
             const int pol = map_order_policy();
             const int ord = pol == 2 ? (op ? 3 : 2) : (mode == COL_FWD && pol != 0 ? 1 : 0);

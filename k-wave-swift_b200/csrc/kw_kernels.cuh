@@ -41,6 +41,7 @@ struct ColJob {
     OpSpec op[kMaxComp];
     int gate;
     long long tile_elems;
+    int tma_ahead;         // TMA column pass: > 0, also prefetch into L2 the tile this many of its tiles on
 };
 
 struct RowC2RJob {

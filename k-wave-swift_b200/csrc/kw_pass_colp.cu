@@ -85,6 +85,19 @@ __global__ void __launch_bounds__(288, ColpCfg<N>::MINB) k_colp(const SimDev* __
                 const CUtensorMap* tm = S.tmaps + tmap_spec(job.spec_in + comp_in, job.layout_axis);
                 if (axisA) tma_load_2d(st, tm, c0, 0, full + s);
                 else tma_load_3d(st, tm, c0, 0, o, full + s);
+                // the tile job.tma_ahead of this CTA's tiles on, into L2 (beyond the ring's reach)
+                const int pidx = idx + job.tma_ahead * gridDim.x;
+                if (job.tma_ahead > 0 && pidx < nmap) {
+                    const BlockWork pw = map[pidx];
+                    const SimDev& P2 = sims[pw.sim];
+                    const int pinner = axisA ? P2.B * P2.Cp : P2.Cp;
+                    const int pnch = (pinner + TW - 1) / TW;
+                    const int po = pw.tile / pnch;
+                    const int pc0 = (pw.tile - po * pnch) * TW;
+                    const CUtensorMap* ptm = P2.tmaps + tmap_spec(job.spec_in + (job.fanout ? 0 : pw.comp), job.layout_axis);
+                    if (axisA) tma_prefetch_2d(ptm, pc0, 0);
+                    else tma_prefetch_3d(ptm, pc0, 0, po);
+                }
             }
             ++k;
         }
